@@ -1,0 +1,351 @@
+"""Benchmark of the explicit-dynamics hot path: bond-updates/s per Velocity Verlet step.
+
+Workload (default): OSBMaterial dynamic fracture block of 400 x 200 x 100 points (8.0M
+points, ~0.96B directed bonds) at dx = 5e-4 m, horizon 3.015 dx, E = 70 GPa, nu = 0.25,
+rho = 2700 kg/m^3, Gc = 100 J/m^2, 5 % of the bond pairs broken at random (seeded),
++-1 m/s velocity conditions on the outermost point layer of both y faces, FP32-compensated
+bond arithmetic with FP64 integration. One step = one Velocity Verlet step of the whole body.
+
+Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+Under torchrun every rank runs its own body (replicas: specimens do not interact); the
+time is the maximum over ranks.
+"""
+import argparse
+import ctypes as C
+import json
+import math
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+for p in (os.path.join(ROOT, "peridynamics.jl_b200"),):
+    if p not in sys.path:
+        sys.path.insert(0, p)
+
+METRIC = "bond-updates/s per VV step"
+UNIT = "bond-updates/s"
+
+CONFIGS = {
+    # name: (nx, ny, nz, dx, material, random broken fraction, bc velocity)
+    "osb8m": (400, 200, 100, 5e-4, "OSB", 0.05, 1.0),
+    "osb1m": (200, 100, 50, 1e-3, "OSB", 0.0, 0.6),
+    "bb1m": (200, 100, 50, 1e-3, "BB", 0.0, 0.6),
+    "c1m": (200, 100, 50, 1e-3, "C", 0.0, 0.6),
+}
+# algorithmic bytes (FP32-compensated form): per directed bond nbr 4 + xi 12 + L 4 + 1/8 bit;
+# per point 140 (u, v FP64 read+write, own u, b_ext/BC, parameter id, damage) + 8 for OSB
+# (m, theta) + 72 for CMat (F, P K^-1)
+B_BOND = {"fp32": 20.125, "fp64": 36.125}
+B_POINT = {"fp32": 140.0, "fp64": 184.0}
+B_POINT_EXTRA = {"BB": 0.0, "OSB": 8.0, "C": 72.0}
+
+
+def load_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def make_body(cfg, jitter_seed=None):
+    import pdcuda as pd
+    nx, ny, nz, dx, mat, frac, vbc = CONFIGS[cfg]
+    lx, ly, lz = nx * dx, ny * dx, nz * dx
+    pos, vol = pd.uniform_box(lx, ly, lz, dx)
+    material = {"OSB": pd.OSBMaterial, "BB": pd.BBMaterial,
+                "C": lambda: pd.CMaterial(model=pd.NeoHooke())}[mat]()
+    body = pd.Body(material, pos, vol)
+    kw = dict(horizon=3.015 * dx, rho=2700.0, E=70e9, Gc=100.0)
+    if mat != "BB":
+        kw["nu"] = 0.25
+    pd.material(body, **kw)
+    y = body._pos[:, 1]
+    pd.point_set(body, "ymin", np.nonzero(y < y.min() + 0.5 * dx)[0])
+    pd.point_set(body, "ymax", np.nonzero(y > y.max() - 0.5 * dx)[0])
+    pd.velocity_bc(lambda t: -vbc, body, "ymin", "y")
+    pd.velocity_bc(lambda t: vbc, body, "ymax", "y")
+    return body, frac
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_{index}.csv")
+
+    def __enter__(self):
+        try:
+            os.makedirs(os.path.dirname(self.path), exist_ok=True)
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index),
+                 "--query-gpu=index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+                 "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
+                 "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.f.close()
+
+    def summary(self):
+        try:
+            rows = [r.split(",") for r in open(self.path).read().strip().splitlines()]
+            sm = [float(r[1]) for r in rows]
+            mx = float(rows[0][2])
+            reasons = set()
+            names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+            for r in rows:
+                for k, nm in enumerate(names):
+                    if r[5 + k].strip() == "Active":
+                        reasons.add(nm)
+            return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                    "samples": len(sm)}
+        except Exception as e:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "error": str(e)}
+
+
+def cpu_baseline(cfg, threads, budget_s=20.0):
+    """The FP64 oracle (CPU restatement of the reference, OpenMP) on a sub-block of the same
+    lattice, spacing and parameters: bond-updates/s over whole Velocity Verlet steps."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    nx, ny, nz, dx, mat, frac, vbc = CONFIGS[cfg]
+    sx, sy, sz = min(nx, 64), min(ny, 64), min(nz, 40)
+    g = lambda n: (np.arange(n) - (n - 1) / 2) * dx
+    X = np.array(np.meshgrid(g(sx), g(sy), g(sz), indexing="ij")).reshape(3, -1).T
+    X = np.ascontiguousarray(X[np.lexsort((X[:, 0], X[:, 1], X[:, 2]))])
+    V = np.full(len(X), dx ** 3)
+    om = {"OSB": O.OSB, "BB": O.BB, "C": O.CMAT}[mat]
+    kw = {} if mat == "BB" else {"nu": 0.25}
+    p = O.point_params(om, 3.015 * dx, 2700.0, E=70e9, Gc=100.0, **kw)
+    O.set_threads(threads)
+    b = O.OracleBody(om, X, V, [p], cmodel=O.NEOHOOKE)
+    dt = b.stable_timestep(0.7)
+    b.v[:, 1] = np.where(X[:, 1] > 0, vbc, -vbc)
+    b.force_density(0.0, dt)
+    steps, t0 = 0, time.perf_counter()
+    while True:
+        b.run_vv(steps + 1, 1, dt)
+        steps += 1
+        el = time.perf_counter() - t0
+        if el > budget_s or steps >= 50:
+            break
+    O.set_threads(1)
+    return {"value": b.n_bonds * steps / el, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"{sx}x{sy}x{sz} sub-block ({len(X)} points, {b.n_bonds} bonds) of the same "
+                      f"lattice and parameters, {steps} FP64 VV steps in {el:.1f} s"}
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    vals = []
+    for _ in range(max(args.warmup, 0)):
+        pass
+    budget = 20.0 / max(args.steps, 1)
+    t = time.perf_counter()
+    res = None
+    for _ in range(args.steps):
+        res = cpu_baseline(args.config, threads, budget_s=max(budget, 2.0))
+        vals.append(res["value"])
+    el = time.perf_counter() - t
+    v = float(np.median(vals))
+    nx, ny, nz, dx, mat, frac, vbc = CONFIGS[args.config]
+    line = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "impl": "reference",
+            "config": {"workload": args.config, "points": nx * ny * nz, "material": mat},
+            "cpu_baseline": dict(res, value=v),
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "note": "Julia is not installed: the reference arm is the CPU restatement of the "
+                    "reference (oracle/, FP64, OpenMP on all host threads)", "wall_s": el}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default="osb8m", choices=list(CONFIGS))
+    ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
+    ap.add_argument("--fp64-steps", type=int, default=-1, help="steps of the FP64 comparison (0 = skip)")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--graph", type=int, default=0)
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import torch
+        import torch.distributed as tdist
+        torch.cuda.set_device(local)
+        import datetime
+        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        dist = tdist
+
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        if dist:
+            dist.barrier()
+            dist.destroy_process_group()
+        return
+
+    import pdcuda as pd
+    nx, ny, nz, dx, mat, frac, vbc = CONFIGS[args.config]
+
+    def barrier():
+        if dist:
+            import torch
+            dist.barrier()
+            torch.cuda.synchronize()
+
+    def max_over_ranks(x):
+        if not dist:
+            return x
+        import torch
+        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def build(prec):
+        body, frac_ = make_body(args.config)
+        dev = pd.DeviceBody(body, precision=prec, device=local)
+        if frac_ > 0:
+            dev.break_random_pairs(frac_, 0x5EED + rank)
+        dt = dev.stable_timestep(0.7)
+        dev.force(0.0, dt)
+        return body, dev, dt
+
+    body, dev, dt = build(args.precision)
+    n_pts, n_bonds, sym = dev.info()
+    group, block = dev.autotune()
+    dev.set_graph(args.graph)
+    step = 1
+    dev.run(step, args.warmup, dt)
+    step += args.warmup
+
+    peak, peak_kind = load_peaks()
+    launches0 = dev.launch_count()
+    barrier()
+    with ClockSampler(local) as clk:
+        ms_total, ms_a, ms_b, ms_int = dev.run_timed(step, args.steps, dt)
+    step += args.steps
+    launches = dev.launch_count() - launches0
+    barrier()
+    ms_max = max_over_ranks(ms_total)
+    value = n_bonds * args.steps * world / (ms_max / 1e3)
+    clocks = clk.summary()
+
+    # roofline of the dominant kernel (per launch, algorithmic bytes)
+    prec = args.precision
+    n_launch = args.steps
+    per_kernel = {"phase_a": ms_a / n_launch, "phase_b": ms_b / n_launch}
+    dom = max(per_kernel, key=per_kernel.get) if mat != "BB" else "phase_a"
+    dom_ms = per_kernel[dom]
+    # bytes a launch of one force phase must move: every bond once (nbr, geometry, state bit)
+    # and its per-point reads / writes
+    if prec == "fp32":
+        pt_bytes = {"phase_a": 32 + 8 + 16 + 4 + 4, "phase_b": 32 + 8 + 16 + 12 + 4}[dom]
+    else:
+        pt_bytes = {"phase_a": 64 + 8 + 32 + 4 + 4, "phase_b": 64 + 8 + 32 + 24 + 4}[dom]
+    alg_bytes = n_bonds * B_BOND[prec] + n_pts * pt_bytes
+    achieved = alg_bytes / (dom_ms / 1e3) / 1e9
+    step_bytes = n_bonds * B_BOND[prec] + n_pts * (B_POINT[prec] + B_POINT_EXTRA[mat])
+    step_ms = ms_max / args.steps
+    step_achieved = step_bytes / (step_ms / 1e3) / 1e9
+
+    # FP64 comparison on the same workload
+    fp64 = None
+    f64_steps = args.fp64_steps if args.fp64_steps >= 0 else max(args.steps // 4, 10)
+    if prec == "fp32" and f64_steps > 0:
+        dev.close()
+        _, d64, dt64 = build("fp64")
+        d64.autotune()
+        d64.run(1, 3, dt64)
+        barrier()
+        t64 = d64.run_timed(4, f64_steps, dt64)[0]
+        barrier()
+        t64 = max_over_ranks(t64)
+        fp64 = n_bonds * f64_steps * world / (t64 / 1e3)
+        d64.close()
+        _, dev, dt = build(prec)
+        dev.set_graph(args.graph)
+
+    # end to end through the public API with host buffers: upload the state, run, read back
+    h_u = np.ascontiguousarray(np.zeros((n_pts, 3)))
+    h_v = np.ascontiguousarray(np.zeros((n_pts, 3)))
+    h_v[:, 1] = 0.0
+    barrier()
+    t0 = time.perf_counter()
+    dev.set_state(displacement=h_u, velocity=h_v)
+    dev.run(1, args.steps, dt)
+    out_u = dev.field("displacement")
+    out_d = dev.field("damage")
+    e2e_s = time.perf_counter() - t0
+    e2e_s = max_over_ranks(e2e_s)
+    h2d = (h_u.nbytes + h_v.nbytes) / args.steps
+    d2h = (out_u.nbytes + out_d.nbytes) / args.steps
+    e2e = n_bonds * args.steps * world / e2e_s
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu = cpu_baseline(args.config, os.cpu_count() or 1)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32" if prec == "fp32" else "f64",
+            "data": "synthetic",
+            "config": {"workload": f"{args.config}: {mat} {nx}x{ny}x{nz} points, dx={dx}, "
+                                   f"horizon 3.015dx, {frac:.0%} pairs broken, VV step",
+                       "points": n_pts, "bonds": n_bonds, "precision": prec,
+                       "mapping": {"group": group, "block": block}, "symmetric_pairs": bool(sym),
+                       "l2": "inputs larger than L2 (bond arrays of ~19 GB)",
+                       "parallelism": f"replicas x{world}"},
+            "roofline": {"bound": "hbm", "kernel": f"{mat.lower()} force {dom}",
+                         "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": None, "peak_kind": peak_kind,
+                         "alg_bytes_per_launch": alg_bytes, "ms_per_launch": dom_ms},
+            "roofline_step": {"achieved": step_achieved, "peak": peak, "frac": step_achieved / peak,
+                              "alg_bytes_per_step": step_bytes,
+                              "ms": {"phase_a": ms_a / n_launch, "phase_b": ms_b / n_launch,
+                                     "integrate": ms_int / n_launch}},
+            "fp64_value": fp64, "fp32_over_fp64": (value / fp64) if fp64 else None,
+            "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "gpu_launches": launches, "clocks": clocks, "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    dev.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,254 @@
+/*
+ * pdcuda.h -- C ABI of libpdcuda, the B200 (sm_100a) explicit-dynamics engine behind
+ * Peridynamics.jl's Body / material! / velocity_bc! / VelocityVerlet / Job / submit surface.
+ *
+ * The library replaces the per-chunk calls that the reference's threads data handler makes
+ * on one BodyChunk (src/core/threads_body_data_handler.jl, src/discretization/body_chunk.jl)
+ * with one device-resident body. Every entry point below names the reference function it
+ * replaces (file:line inside Peridynamics.jl).
+ *
+ * Conventions
+ *  - Plain C types only. Arrays are host pointers, valid for the duration of the call; the
+ *    library copies them into device memory it owns. Point vectors use the reference's
+ *    3 x N column-major layout (x, y, z of point 0, then point 1, ...). Point tensors are
+ *    9 x N column-major 3x3 matrices. Indices are 0-based.
+ *  - Every function returns a pd_status. PD_OK is 0. On error, pd_last_error() returns a
+ *    message for the calling thread.
+ *  - Calls on one handle must be serialised by the caller (one host thread per handle).
+ *    Handles are independent.
+ */
+#ifndef PDCUDA_H
+#define PDCUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int32_t pd_status;
+#define PD_OK 0
+#define PD_ERR_ARG 1      /* invalid argument (reference: ArgumentError) */
+#define PD_ERR_CUDA 2     /* CUDA runtime error */
+#define PD_ERR_NAN 3      /* NaN in the internal force density (reference: NaNError) */
+#define PD_ERR_TIMEOUT 4  /* a bounded device wait gave up */
+#define PD_ERR_OOM 5      /* device allocation failed */
+#define PD_ERR_UNSUPPORTED 6
+
+/* material families (src/physics/bond_based.jl, ordinary_state_based.jl, correspondence.jl) */
+#define PD_MAT_BB 0
+#define PD_MAT_OSB 1
+#define PD_MAT_CMAT 2
+
+/* correspondence constitutive models (src/physics/constitutive_models.jl) */
+#define PD_CM_SVK 0
+#define PD_CM_NEOHOOKE 1
+#define PD_CM_NEOHOOKE_PENALTY 2
+
+/* influence functions (src/discretization/kernels.jl:10-52) */
+#define PD_KERNEL_CONST_ONE 0
+#define PD_KERNEL_LINEAR 1
+#define PD_KERNEL_CUBIC_BSPLINE 2
+
+/* arithmetic of the bond loops */
+#define PD_PREC_FP64 0        /* FP64 everywhere; positions kept incrementally as the reference does */
+#define PD_PREC_FP32_KAHAN 1  /* FP32 bond math on xi + (u_j - u_i), compensated sums, FP64 integration */
+
+/* storage fields (src/time_solvers/velocity_verlet.jl:342-352, bond_system.jl:408-412,
+ * correspondence.jl:173-181) */
+#define PD_FIELD_POSITION 0       /* double[3n] */
+#define PD_FIELD_DISPLACEMENT 1   /* double[3n] */
+#define PD_FIELD_VELOCITY 2       /* double[3n] */
+#define PD_FIELD_VELOCITY_HALF 3  /* double[3n] */
+#define PD_FIELD_ACCELERATION 4   /* double[3n] */
+#define PD_FIELD_B_INT 5          /* double[3n] */
+#define PD_FIELD_B_EXT 6          /* double[3n] */
+#define PD_FIELD_DAMAGE 7         /* double[n] */
+#define PD_FIELD_N_ACTIVE_BONDS 8 /* int64[n] */
+#define PD_FIELD_BOND_ACTIVE 9    /* uint8[n_bonds] */
+#define PD_FIELD_DEFGRAD 10       /* double[9n] (CMaterial) */
+#define PD_FIELD_CAUCHY_STRESS 11 /* double[9n] (CMaterial) */
+
+/* boundary-condition targets (velocity_bc! writes velocity_half, forcedensity_bc! b_ext:
+ * src/physics/boundary_conditions.jl:422-435, 559-575) */
+#define PD_BC_VELOCITY_HALF 0
+#define PD_BC_B_EXT 1
+/* boundary-condition value kinds */
+#define PD_BC_KIND_TIME 0        /* f(t): one value per step, tabulated by the host */
+#define PD_BC_KIND_POINT_TIME 1  /* f(p, t): one value per point of the set per step */
+#define PD_BC_KIND_DATA 2        /* DataBC: one constant value per point of the set */
+
+/* StandardPointParameters (src/core/parameters.jl:107-125); CPointParameters
+ * (src/physics/correspondence.jl:148-161) without the Hooke tensor. */
+typedef struct {
+    double delta, rho, E, nu, G, K, lambda, mu, Gc, epsilon_c, bc;
+} pd_point_params;
+
+/* One body chunk with its bond system (src/discretization/bond_system.jl:44-65). */
+typedef struct {
+    int64_t n_points;
+    const double *position;        /* [3n] reference positions */
+    const double *volume;          /* [n] */
+    int64_t n_bonds;
+    const int64_t *bond_offsets;   /* [n+1]: bonds of point i are [off[i], off[i+1]) */
+    const int32_t *neighbors;      /* [n_bonds], 0-based */
+    const double *bond_length;     /* [n_bonds] or NULL (then |X_j - X_i|) */
+    const uint8_t *fail_permit;    /* [n_bonds] or NULL (then all 1) */
+    const uint16_t *param_id;      /* [n] or NULL (then all 0) */
+    int32_t n_params;
+    const pd_point_params *params; /* [n_params] */
+    int32_t material;              /* PD_MAT_* */
+    int32_t kernel;                /* PD_KERNEL_* (OSB, CMat) */
+    int32_t cmodel;                /* PD_CM_* (CMat) */
+    int32_t precision;             /* PD_PREC_* */
+    int32_t multi_params;          /* 1: ParameterHandler semantics of the reference
+                                      (bond-averaged parameters, bond_based.jl:163-180,
+                                      ordinary_state_based.jl:151-174) */
+    double zem_cs;                 /* ZEMSilling Cs (zem_stabilization.jl:16-21), default 0.5 */
+    double maxdmg;                 /* CMaterial maxdmg (correspondence.jl:123-128), default 0.85 */
+    int32_t device;                /* CUDA device ordinal */
+} pd_body_desc;
+
+/* One boundary condition on one point set and one dimension. */
+typedef struct {
+    int32_t field;        /* PD_BC_VELOCITY_HALF / PD_BC_B_EXT */
+    int32_t dim;          /* 0, 1, 2 */
+    int32_t kind;         /* PD_BC_KIND_* */
+    int32_t n_points;
+    const int32_t *points;/* [n_points] */
+    const double *data;   /* PD_BC_KIND_DATA: [n_points] values, else NULL */
+} pd_bc_desc;
+
+typedef struct pd_handle pd_handle;
+
+/* Message of the last failed call on this thread (empty if none). */
+const char *pd_last_error(void);
+
+/* Library version, e.g. "0.1.0". */
+const char *pd_version(void);
+
+/* Neighbour search: replaces find_bonds / find_bonds! / filter_bonds! and the
+ * duplicate-point check (src/discretization/bond_system.jl:96-165). Runs on the device.
+ * Bond i->j exists for j != i with |X_j - X_i|^2 <= delta_i^2; bonds of a point are ordered
+ * by ascending j. fail_permit of a bond is fp_point[i] & fp_point[j]. n_filters filter-mode
+ * pre-cracks (precrack!(...; update_dmg=false), predefined_cracks.jl:106-112) are given as
+ * point masks filter_a/filter_b of n_filters x n bytes. Call first with capacity 0 to get
+ * *n_bonds, then with arrays of that capacity. */
+pd_status pd_find_bonds(int64_t n, const double *position, const double *delta,
+                        const uint8_t *fp_point, int32_t n_filters, const uint8_t *filter_a,
+                        const uint8_t *filter_b, int64_t capacity, int64_t *bond_offsets,
+                        int32_t *neighbors, double *bond_length, uint8_t *fail_permit,
+                        int64_t *n_bonds, int32_t device);
+
+/* Creates the device body: replaces BodyChunk construction with its storage
+ * (src/discretization/body_chunk.jl:41-52, src/core/storages.jl) for one chunk holding all
+ * points. All fields start as the reference initialises them (zeros, all bonds active,
+ * n_active_bonds = n_neighbors). */
+pd_status pd_create(const pd_body_desc *desc, pd_handle **out);
+
+/* pd_create with the bonds found on the device by the neighbour search of pd_find_bonds
+ * (desc->bond_offsets, neighbors, bond_length and fail_permit are ignored): the horizon of a
+ * point is the delta of its parameter set, fp_point (n bytes, may be NULL = all 1) is the
+ * failure permission per point (failure_permit!, fracture.jl:38-42) and the n_filters
+ * filter-mode pre-cracks are point masks as in pd_find_bonds. */
+pd_status pd_create_search(const pd_body_desc *desc, const uint8_t *fp_point, int32_t n_filters,
+                           const uint8_t *filter_a, const uint8_t *filter_b, pd_handle **out);
+
+/* Frees all device memory of the handle. */
+pd_status pd_destroy(pd_handle *h);
+
+/* Overwrites point fields (any pointer may be NULL = keep): replaces the initial-condition
+ * and pre-crack setup of a chunk (apply_initial_conditions!, initial_conditions.jl:86-94;
+ * break_bonds! + calc_damage!, bond_system.jl:249-267, 338-343). bond_active is one byte
+ * per bond; n_active_bonds is recomputed from it. position NULL keeps the current one. */
+pd_status pd_set_state(pd_handle *h, const double *position, const double *displacement,
+                       const double *velocity, const double *velocity_half,
+                       const double *acceleration, const double *b_ext,
+                       const uint8_t *bond_active);
+
+/* Damage-mode pre-crack: replaces break_bonds! + calc_damage! of apply_precracks!
+ * (bond_system.jl:249-267, predefined_cracks.jl:31-60). Bonds joining a point of set a
+ * with a point of set b become inactive. set_a / set_b: n bytes, nonzero = member. */
+pd_status pd_break_bonds(pd_handle *h, const uint8_t *set_a, const uint8_t *set_b);
+
+/* Initial damage of synthetic workloads (no counterpart in the reference, which has no API
+ * for random initial damage): each unordered pair {i, j} is broken with probability
+ * `fraction`, decided by a hash of (min(i,j), max(i,j), seed), so both directions agree. */
+pd_status pd_break_random_pairs(pd_handle *h, double fraction, uint64_t seed);
+
+/* Copies one storage field to host memory of `bytes` bytes (export_results,
+ * threads_body_data_handler.jl:197-212). */
+pd_status pd_get_field(pd_handle *h, int32_t field, void *out, size_t bytes);
+
+/* Installs the boundary conditions of the chunk (ConditionHandler,
+ * src/discretization/condition_handler.jl:1-36). Replaces any previous set. */
+pd_status pd_set_bcs(pd_handle *h, int32_t n_bcs, const pd_bc_desc *bcs);
+
+/* Values of the time-dependent boundary conditions for steps first_step ..
+ * first_step + n_steps - 1: the host evaluates each f(t) (apply_bc!,
+ * boundary_conditions.jl:37-51, 91-108) at t = step * dt. `values` holds, step after step,
+ * one value per PD_BC_KIND_TIME condition and n_points values per PD_BC_KIND_POINT_TIME
+ * condition, in the order of pd_set_bcs. NaN / Inf values leave the field unchanged. */
+pd_status pd_set_bc_values(pd_handle *h, int64_t first_step, int64_t n_steps,
+                           const double *values, int64_t n_values);
+
+/* CFL time step: replaces calc_stable_timestep / calc_timestep_point
+ * (velocity_verlet.jl:132-163, bond_system.jl:269-277). dt_per_param (may be NULL) receives
+ * the minimum per parameter set times the safety factor (one body per set in an ensemble). */
+pd_status pd_stable_timestep(pd_handle *h, double safety_factor, double *dt,
+                             double *dt_per_param);
+
+/* Integration step per parameter set (ensemble of bodies with their own CFL steps).
+ * pd_run_vv with dt <= 0 uses these. */
+pd_status pd_set_param_timesteps(pd_handle *h, const double *dt_per_param);
+
+/* One force evaluation at the current positions: replaces calc_force_density!(chunk, t, dt)
+ * (bond_system.jl:279-297) with calc_failure!, calc_damage! and force_density_point! for
+ * every point, followed by check_for_nans (nans.jl:10-18). Used by initialize!
+ * (core/data_handler.jl:1-4) and the Newton-Krylov matrix-free products. */
+pd_status pd_force(pd_handle *h, double t, double dt);
+
+/* n_steps Velocity Verlet steps first_step .. first_step + n_steps - 1 at t = step * dt:
+ * replaces solve! / verlet_timestep! (velocity_verlet.jl:165-237: update_vel_half!,
+ * apply_boundary_conditions!, update_disp_and_pos!, calc_force_density!,
+ * update_acc_and_vel!). On NaN in the force density it stops with PD_ERR_NAN and leaves the
+ * state as the reference does when it throws NaNError; pd_nan_step reports the step. */
+pd_status pd_run_vv(pd_handle *h, int64_t first_step, int64_t n_steps, double dt);
+
+/* Step at which the last PD_ERR_NAN was raised (NaNError.step). */
+pd_status pd_nan_step(pd_handle *h, int64_t *step);
+
+/* pd_run_vv with CUDA events on the handle's stream around every kernel (no graph):
+ * elapsed milliseconds of the whole run, of the first force kernel (BB: the force kernel;
+ * OSB / CMat: phase A), of the second force kernel (OSB / CMat phase B) and of the
+ * integration kernels, summed over the steps. Same effect on the state as pd_run_vv. */
+pd_status pd_run_vv_timed(pd_handle *h, int64_t first_step, int64_t n_steps, double dt,
+                          double *ms_total, double *ms_phase_a, double *ms_phase_b,
+                          double *ms_integrate);
+
+/* Chooses the point-to-lane mapping (points per thread / warp) and block size of the force
+ * kernels by timing each candidate on this body. Leaves the state unchanged. */
+pd_status pd_autotune(pd_handle *h, int32_t *group_out, int32_t *block_out);
+
+/* Forces a mapping: group lanes per point in {1, 2, 4, 8, 16, 32}, or 0 for the FP64
+ * serial-order mapping (one lane per point summing in the reference's order: bit-identical
+ * to a serial CPU evaluation); block size 64, 128 or 256. */
+pd_status pd_set_mapping(pd_handle *h, int32_t group, int32_t block);
+
+/* Enables CUDA-graph capture of blocks of `steps_per_graph` steps (0 disables). */
+pd_status pd_set_graph(pd_handle *h, int32_t steps_per_graph);
+
+/* Sizes: points, bonds, and 1 if the fast symmetric-pair bond mode is active. */
+pd_status pd_info(pd_handle *h, int64_t *n_points, int64_t *n_bonds, int32_t *symmetric);
+
+/* Number of kernel launches issued by the handle since creation. */
+pd_status pd_launch_count(pd_handle *h, int64_t *count);
+
+/* The cudaStream_t of the handle, as an opaque pointer. */
+pd_status pd_stream(pd_handle *h, void **stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PDCUDA_H */

@@ -1,0 +1,1105 @@
+// pd_api.cu -- C ABI of libpdcuda: handle lifecycle, uploads, boundary conditions, the
+// Velocity Verlet step loop (eager or CUDA-graph captured), exports and the autotuner.
+#include <algorithm>
+#include <cmath>
+#include <cstddef>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "pdcuda.h"
+#include "pd_common.cuh"
+#include "pd_launch.h"
+#include "pd_bonds.h"
+
+using namespace pd;
+
+static thread_local std::string g_err;
+
+static pd_status fail(pd_status code, const std::string& msg) {
+  g_err = msg;
+  return code;
+}
+
+#define PD_CUDA(x)                                                                            \
+  do {                                                                                        \
+    cudaError_t e_ = (x);                                                                     \
+    if (e_ != cudaSuccess)                                                                    \
+      return fail(e_ == cudaErrorMemoryAllocation ? PD_ERR_OOM : PD_ERR_CUDA,                 \
+                  std::string(#x) + ": " + cudaGetErrorString(e_));                           \
+  } while (0)
+
+#define PD_TRY(x)                  \
+  do {                             \
+    pd_status s_ = (x);            \
+    if (s_ != PD_OK) return s_;    \
+  } while (0)
+
+struct GraphKey {
+  int steps = 0, group = 0, block = 0, exact = 0, bcpts = 0;
+  double dt = 0;
+  long long version = -1;
+  bool operator==(const GraphKey& o) const {
+    return steps == o.steps && group == o.group && block == o.block && exact == o.exact &&
+           bcpts == o.bcpts && dt == o.dt && version == o.version;
+  }
+};
+
+struct pd_handle {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  long long n = 0, nb = 0;
+  int material = 0, kernel = 1, cmodel = 0, precision = 0, multi = 0;
+  double cs = 0.5, maxdmg = 0.85;
+  std::vector<DevParam> hp;
+  std::vector<unsigned> hmeta;
+  std::vector<void*> allocs;
+  DevBody d{};
+  IntDev g{};
+  BCDev bc{};
+  DevParam* dparams = nullptr;
+  int* rev = nullptr;
+  int* flags = nullptr;
+  LaunchCfg cfg{8, 256, false};
+  bool damage_valid = false;
+  bool has_bext_state = false;
+  // boundary conditions (host side)
+  std::vector<BCInfo> bcinfo;
+  std::vector<int> bcn;
+  long long per_step = 0;
+  bool needs_table = false;
+  double* table = nullptr;
+  long long table_cap = 0;
+  std::vector<unsigned char> bext_pt;  // points with b_ext conditions
+  long long version = 0;
+  // graphs
+  int graph_steps = 0;
+  cudaGraphExec_t gexec = nullptr;
+  int graph_nodes = 0;
+  GraphKey gkey;
+  long long launches = 0;
+  long long nan_step = -1;
+};
+
+template <class T>
+static pd_status dalloc(pd_handle* h, T** p, size_t count) {
+  void* q = nullptr;
+  if (count == 0) count = 1;
+  cudaError_t e = cudaMalloc(&q, sizeof(T) * count);
+  if (e != cudaSuccess)
+    return fail(e == cudaErrorMemoryAllocation ? PD_ERR_OOM : PD_ERR_CUDA,
+                std::string("cudaMalloc of ") + std::to_string(sizeof(T) * count) + " bytes: " +
+                    cudaGetErrorString(e));
+  h->allocs.push_back(q);
+  *p = (T*)q;
+  return PD_OK;
+}
+
+static void dfree(pd_handle* h, void* p) {
+  if (!p) return;
+  auto it = std::find(h->allocs.begin(), h->allocs.end(), p);
+  if (it != h->allocs.end()) h->allocs.erase(it);
+  cudaFree(p);
+}
+
+static pd_status set_ctrl(pd_handle* h, size_t off, const void* src, size_t bytes) {
+  PD_CUDA(cudaMemcpyAsync(reinterpret_cast<char*>(h->d.ctrl) + off, src, bytes,
+                          cudaMemcpyHostToDevice, h->stream));
+  return PD_OK;
+}
+
+static pd_status upload_meta(pd_handle* h) {
+  PD_CUDA(cudaMemcpyAsync(h->d.meta, h->hmeta.data(), sizeof(unsigned) * h->n,
+                          cudaMemcpyHostToDevice, h->stream));
+  return PD_OK;
+}
+
+static pd_status upload_params(pd_handle* h) {
+  PD_CUDA(cudaMemcpyAsync(h->dparams, h->hp.data(), sizeof(DevParam) * h->hp.size(),
+                          cudaMemcpyHostToDevice, h->stream));
+  PD_CUDA(cudaStreamSynchronize(h->stream));
+  return PD_OK;
+}
+
+static void destroy_graph(pd_handle* h) {
+  if (h->gexec) cudaGraphExecDestroy(h->gexec);
+  h->gexec = nullptr;
+  h->gkey = GraphKey();
+}
+
+extern "C" const char* pd_last_error(void) { return g_err.c_str(); }
+extern "C" const char* pd_version(void) { return "0.1.0"; }
+
+static DevParam make_param(const pd_point_params& p, double cs) {
+  DevParam q{};
+  q.delta = p.delta; q.rho = p.rho; q.bc = p.bc; q.epsc = p.epsilon_c; q.G = p.G; q.K = p.K;
+  q.lambda = p.lambda; q.mu = p.mu;
+  q.beta = cs * p.bc / p.delta;
+  q.dt = 0; q.dth = 0;
+  q.deltaf = (float)p.delta; q.bcf = (float)p.bc; q.epscf = (float)p.epsilon_c;
+  q.Gf = (float)p.G; q.Kf = (float)p.K; q.lambdaf = (float)p.lambda; q.muf = (float)p.mu;
+  q.betaf = (float)q.beta;
+  q.inv_delta = (float)(1.0 / p.delta);
+  q.vscale = (float)(1.0 / (p.delta * p.delta * p.delta));
+  return q;
+}
+
+static pd_status validate_desc(const pd_body_desc* desc, bool need_bonds) {
+  if (!desc) return fail(PD_ERR_ARG, "desc is NULL");
+  if (desc->n_points < 0) return fail(PD_ERR_ARG, "n_points < 0");
+  if (desc->n_points > 0x7fffffffLL) return fail(PD_ERR_ARG, "n_points exceeds 2^31 - 1");
+  if (desc->n_points > 0 && (!desc->position || !desc->volume))
+    return fail(PD_ERR_ARG, "position and volume are required");
+  if (desc->n_params < 1 || desc->n_params > 65535 || !desc->params)
+    return fail(PD_ERR_ARG, "1 <= n_params <= 65535 parameter sets are required");
+  if (desc->material < PD_MAT_BB || desc->material > PD_MAT_CMAT)
+    return fail(PD_ERR_ARG, "unknown material");
+  if (desc->precision != PD_PREC_FP64 && desc->precision != PD_PREC_FP32_KAHAN)
+    return fail(PD_ERR_ARG, "unknown precision");
+  if (desc->kernel < PD_KERNEL_CONST_ONE || desc->kernel > PD_KERNEL_CUBIC_BSPLINE)
+    return fail(PD_ERR_ARG, "unknown kernel");
+  if (desc->cmodel < PD_CM_SVK || desc->cmodel > PD_CM_NEOHOOKE_PENALTY)
+    return fail(PD_ERR_ARG, "unknown constitutive model");
+  for (int k = 0; k < desc->n_params; k++) {
+    const pd_point_params& p = desc->params[k];
+    if (!(p.delta > 0)) return fail(PD_ERR_ARG, "`horizon` should be larger than zero!");
+    if (!(p.rho > 0)) return fail(PD_ERR_ARG, "`rho` should be larger than zero!");
+  }
+  const long long n = desc->n_points;
+  if (desc->param_id)
+    for (long long i = 0; i < n; i++)
+      if (desc->param_id[i] >= desc->n_params) return fail(PD_ERR_ARG, "param_id out of range");
+  for (long long i = 0; i < n; i++)
+    if (!(desc->volume[i] > 0) && desc->volume[i] != 0)
+      return fail(PD_ERR_ARG, "volume must be finite and >= 0");
+  if (need_bonds) {
+    if (desc->n_bonds < 0) return fail(PD_ERR_ARG, "n_bonds < 0");
+    if (desc->n_bonds > 0x7fffffffLL) return fail(PD_ERR_ARG, "n_bonds exceeds 2^31 - 1");
+    if (!desc->bond_offsets) return fail(PD_ERR_ARG, "bond_offsets is NULL");
+    if (desc->n_bonds > 0 && !desc->neighbors) return fail(PD_ERR_ARG, "neighbors is NULL");
+    if (desc->bond_offsets[0] != 0 || desc->bond_offsets[n] != desc->n_bonds)
+      return fail(PD_ERR_ARG, "bond_offsets must start at 0 and end at n_bonds");
+    for (long long i = 0; i < n; i++)
+      if (desc->bond_offsets[i + 1] < desc->bond_offsets[i])
+        return fail(PD_ERR_ARG, "bond_offsets must be non-decreasing");
+    for (long long b = 0; b < desc->n_bonds; b++)
+      if (desc->neighbors[b] < 0 || desc->neighbors[b] >= n)
+        return fail(PD_ERR_ARG, "neighbor index out of range");
+  }
+  return PD_OK;
+}
+
+// symmetric-pair mode of the state-based materials: every bond has a reverse, both directions
+// share one state and one critical stretch. Otherwise the reverse index is kept.
+static pd_status setup_symmetry(pd_handle* h) {
+  if (h->material == PD_MAT_BB || h->nb == 0) { h->d.sym = 1; return PD_OK; }
+  int hf[4] = {0, 0, 0, 0};
+  if (!h->rev) PD_TRY(dalloc(h, &h->rev, h->nb));
+  PD_CUDA(cudaMemsetAsync(h->flags, 0, sizeof(int) * 4, h->stream));
+  launch_reverse(h->d, h->rev, h->flags, h->stream);
+  launch_check_sym(h->d, h->rev, h->flags, h->stream);
+  PD_CUDA(cudaMemcpyAsync(hf, h->flags, sizeof(hf), cudaMemcpyDeviceToHost, h->stream));
+  PD_CUDA(cudaStreamSynchronize(h->stream));
+  if (hf[0])
+    return fail(PD_ERR_UNSUPPORTED,
+                "bond lists are not symmetric (a bond i->j without j->i): the gather form of the "
+                "state-based materials needs symmetric bond lists (equal horizons)");
+  h->d.sym = (hf[1] == 0 && hf[2] == 0) ? 1 : 0;
+  h->d.rev = h->rev;
+  return PD_OK;
+}
+
+static pd_status finish_create(pd_handle* h, const pd_body_desc* desc, const double* dL,
+                               const unsigned char* dfp) {
+  const long long n = h->n, nb = h->nb;
+  // bond geometry
+  if (h->precision == PD_PREC_FP64) {
+    double* len = nullptr;
+    PD_TRY(dalloc(h, &len, nb));
+    h->d.len64 = len;
+    launch_build_len64(h->d, dL, dfp, len, h->stream);
+  } else {
+    float4* geo = nullptr;
+    PD_TRY(dalloc(h, &geo, nb));
+    h->d.geo = geo;
+    launch_build_geo(h->d, dL, dfp, geo, h->stream);
+  }
+  PD_CUDA(cudaGetLastError());
+  // bond_active: all bonds active
+  unsigned* bits = nullptr;
+  const long long nw = (nb + 31) / 32;
+  PD_TRY(dalloc(h, &bits, nw + 1));
+  PD_CUDA(cudaMemsetAsync(bits, 0xff, sizeof(unsigned) * (nw + 1), h->stream));
+  h->d.bits = bits;
+  // point state
+  PD_TRY(dalloc(h, &h->d.n_active, n));
+  PD_TRY(dalloc(h, &h->g.vh, 3 * n));
+  PD_TRY(dalloc(h, &h->g.v, 3 * n));
+  PD_TRY(dalloc(h, &h->g.a, 3 * n));
+  PD_TRY(dalloc(h, &h->g.bext, 3 * n));
+  PD_CUDA(cudaMemsetAsync(h->g.vh, 0, sizeof(double) * 3 * n, h->stream));
+  PD_CUDA(cudaMemsetAsync(h->g.v, 0, sizeof(double) * 3 * n, h->stream));
+  PD_CUDA(cudaMemsetAsync(h->g.a, 0, sizeof(double) * 3 * n, h->stream));
+  PD_CUDA(cudaMemsetAsync(h->g.bext, 0, sizeof(double) * 3 * n, h->stream));
+  if (h->precision == PD_PREC_FP64) {
+    PD_TRY(dalloc(h, &h->g.u, 3 * n));
+    PD_TRY(dalloc(h, &h->d.b64, 3 * n));
+    PD_CUDA(cudaMemsetAsync(h->g.u, 0, sizeof(double) * 3 * n, h->stream));
+    PD_CUDA(cudaMemsetAsync(h->d.b64, 0, sizeof(double) * 3 * n, h->stream));
+    h->g.fp32 = 0;
+  } else {
+    PD_TRY(dalloc(h, &h->d.b32, 3 * n));
+    PD_CUDA(cudaMemsetAsync(h->d.b32, 0, sizeof(float) * 3 * n, h->stream));
+    h->g.fp32 = 1;
+  }
+  if (h->material == PD_MAT_OSB) {
+    if (h->precision == PD_PREC_FP64) PD_TRY(dalloc(h, &h->d.coef64, n));
+    else PD_TRY(dalloc(h, &h->d.coef32, n));
+  } else if (h->material == PD_MAT_CMAT) {
+    if (h->precision == PD_PREC_FP64) {
+      PD_TRY(dalloc(h, &h->d.F64, 9 * n));
+      PD_TRY(dalloc(h, &h->d.PK64, 9 * n));
+      PD_CUDA(cudaMemsetAsync(h->d.F64, 0, sizeof(double) * 9 * n, h->stream));
+    } else {
+      PD_TRY(dalloc(h, &h->d.H32, 9 * n));
+      PD_TRY(dalloc(h, &h->d.cst32, 3 * n));
+      PD_CUDA(cudaMemsetAsync(h->d.H32, 0, sizeof(float) * 9 * n, h->stream));
+    }
+  }
+  launch_count_active(h->d, h->stream);
+  PD_CUDA(cudaGetLastError());
+  PD_TRY(setup_symmetry(h));
+  PD_CUDA(cudaStreamSynchronize(h->stream));
+  (void)desc;
+  return PD_OK;
+}
+
+static pd_status begin_create(const pd_body_desc* desc, pd_handle** out, pd_handle** hp) {
+  if (!out) return fail(PD_ERR_ARG, "out is NULL");
+  *out = nullptr;
+  PD_CUDA(cudaSetDevice(desc->device));
+  pd_handle* h = new pd_handle();
+  *hp = h;
+  h->device = desc->device;
+  h->n = desc->n_points;
+  h->material = desc->material;
+  h->kernel = desc->kernel;
+  h->cmodel = desc->cmodel;
+  h->precision = desc->precision;
+  h->cs = desc->zem_cs;
+  h->maxdmg = desc->maxdmg;
+  h->multi = desc->multi_params ? 1 : 0;
+  PD_CUDA(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+  for (int k = 0; k < desc->n_params; k++) h->hp.push_back(make_param(desc->params[k], h->cs));
+  PD_TRY(dalloc(h, &h->dparams, h->hp.size()));
+  PD_TRY(upload_params(h));
+  PD_TRY(dalloc(h, &h->d.ctrl, 1));
+  PD_CUDA(cudaMemsetAsync(h->d.ctrl, 0, sizeof(Ctrl), h->stream));
+  PD_TRY(dalloc(h, &h->flags, 4));
+  const long long n = h->n;
+  h->hmeta.assign(n, 0u);
+  for (long long i = 0; i < n; i++) h->hmeta[i] = desc->param_id ? desc->param_id[i] : 0u;
+  PD_TRY(dalloc(h, &h->d.meta, n));
+  PD_TRY(upload_meta(h));
+  // reference positions and volumes
+  std::vector<double4> X0(n > 0 ? n : 1), cur(n > 0 ? n : 1);
+  for (long long i = 0; i < n; i++) {
+    X0[i] = make_double4(desc->position[3 * i], desc->position[3 * i + 1], desc->position[3 * i + 2],
+                         desc->volume[i]);
+    cur[i] = h->precision == PD_PREC_FP64 ? X0[i] : make_double4(0, 0, 0, desc->volume[i]);
+  }
+  double4 *dX0 = nullptr, *dcur = nullptr;
+  PD_TRY(dalloc(h, &dX0, n));
+  PD_TRY(dalloc(h, &dcur, n));
+  PD_CUDA(cudaMemcpy(dX0, X0.data(), sizeof(double4) * n, cudaMemcpyHostToDevice));
+  PD_CUDA(cudaMemcpy(dcur, cur.data(), sizeof(double4) * n, cudaMemcpyHostToDevice));
+  h->d.X0 = dX0;
+  h->d.cur = dcur;
+  h->d.n = n;
+  h->d.params = h->dparams;
+  h->d.material = h->material;
+  h->d.kernel = h->kernel;
+  h->d.cmodel = h->cmodel;
+  h->d.multi = h->multi;
+  h->d.maxdmg = h->maxdmg;
+  h->d.cs = h->cs;
+  h->d.sym = 1;
+  h->cfg.group = h->precision == PD_PREC_FP64 ? 1 : 8;
+  h->cfg.block = 256;
+  h->cfg.exact = false;
+  return PD_OK;
+}
+
+extern "C" pd_status pd_create(const pd_body_desc* desc, pd_handle** out) {
+  PD_TRY(validate_desc(desc, true));
+  pd_handle* h = nullptr;
+  pd_status st = begin_create(desc, out, &h);
+  if (st != PD_OK) { if (h) pd_destroy(h); return st; }
+  h->nb = desc->n_bonds;
+  h->d.nb = h->nb;
+  const long long n = h->n, nb = h->nb;
+  long long* doff = nullptr;
+  int* dnbr = nullptr;
+  double* dL = nullptr;
+  unsigned char* dfp = nullptr;
+  st = dalloc(h, &doff, n + 1);
+  if (st == PD_OK) st = dalloc(h, &dnbr, nb);
+  if (st == PD_OK && desc->bond_length) st = dalloc(h, &dL, nb);
+  if (st == PD_OK && desc->fail_permit) st = dalloc(h, &dfp, nb);
+  if (st != PD_OK) { pd_destroy(h); return st; }
+  cudaError_t e = cudaMemcpy(doff, desc->bond_offsets, sizeof(long long) * (n + 1), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess && nb) e = cudaMemcpy(dnbr, desc->neighbors, sizeof(int) * nb, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess && dL) e = cudaMemcpy(dL, desc->bond_length, sizeof(double) * nb, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess && dfp) e = cudaMemcpy(dfp, desc->fail_permit, nb, cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) { pd_destroy(h); return fail(PD_ERR_CUDA, cudaGetErrorString(e)); }
+  h->d.off = doff;
+  h->d.nbr = dnbr;
+  st = finish_create(h, desc, dL, dfp);
+  if (dL) dfree(h, dL);
+  if (dfp) dfree(h, dfp);
+  if (st != PD_OK) { std::string m = g_err; pd_destroy(h); return fail(st, m); }
+  *out = h;
+  return PD_OK;
+}
+
+// device search; fills the cell grid from the host positions
+static pd_status search_grid(long long n, const double* position, const double* delta, double lo[3],
+                             double& hcell, long long nc[3]) {
+  double dmax = 0;
+  for (long long i = 0; i < n; i++) dmax = std::max(dmax, delta[i]);
+  if (!(dmax > 0)) return fail(PD_ERR_ARG, "horizons must be > 0");
+  hcell = dmax;
+  long double ncell = 1;
+  for (int k = 0; k < 3; k++) {
+    double a = INFINITY, b = -INFINITY;
+    for (long long i = 0; i < n; i++) { a = std::min(a, position[3 * i + k]); b = std::max(b, position[3 * i + k]); }
+    if (n == 0) { a = 0; b = 0; }
+    lo[k] = a;
+    nc[k] = (long long)std::floor((b - a) / dmax) + 1;
+    if (nc[k] < 1) nc[k] = 1;
+    ncell *= nc[k];
+  }
+  if (ncell > 256.0L * 1024 * 1024)
+    return fail(PD_ERR_ARG, "the bounding box holds more than 2^28 horizon-sized cells");
+  return PD_OK;
+}
+
+static pd_status pack_masks(long long n, int32_t nf, const uint8_t* fa, const uint8_t* fb,
+                            std::vector<unsigned short>& m) {
+  if (nf < 0 || nf > 8) return fail(PD_ERR_ARG, "at most 8 filter-mode pre-cracks are supported");
+  m.assign(n, 0);
+  for (int k = 0; k < nf; k++)
+    for (long long i = 0; i < n; i++) {
+      if (fa[(size_t)k * n + i] && fb[(size_t)k * n + i])
+        return fail(PD_ERR_ARG, "pre-crack point sets intersect");
+      m[i] |= (unsigned short)((fa[(size_t)k * n + i] ? 1u : 0u) << (2 * k));
+      m[i] |= (unsigned short)((fb[(size_t)k * n + i] ? 1u : 0u) << (2 * k + 1));
+    }
+  return PD_OK;
+}
+
+extern "C" pd_status pd_find_bonds(int64_t n, const double* position, const double* delta,
+                                   const uint8_t* fp_point, int32_t n_filters, const uint8_t* filter_a,
+                                   const uint8_t* filter_b, int64_t capacity, int64_t* bond_offsets,
+                                   int32_t* neighbors, double* bond_length, uint8_t* fail_permit,
+                                   int64_t* n_bonds, int32_t device) {
+  if (n < 0 || !n_bonds || (n > 0 && (!position || !delta)))
+    return fail(PD_ERR_ARG, "invalid arguments");
+  PD_CUDA(cudaSetDevice(device));
+  double lo[3], hc;
+  long long nc[3];
+  PD_TRY(search_grid(n, position, delta, lo, hc, nc));
+  std::vector<unsigned short> mask;
+  if (n_filters > 0) PD_TRY(pack_masks(n, n_filters, filter_a, filter_b, mask));
+  cudaStream_t s;
+  PD_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+  double *dX = nullptr, *dd = nullptr, *dL = nullptr;
+  unsigned short* dm = nullptr;
+  long long* doff = nullptr;
+  int* dnbr = nullptr;
+  unsigned char *dfp = nullptr, *dfpb = nullptr;
+  long long nb = 0;
+  int dup = 0;
+  pd_status st = PD_OK;
+  cudaError_t e = cudaSuccess;
+  auto ok = [&](cudaError_t x) { if (e == cudaSuccess) e = x; return e == cudaSuccess; };
+  ok(cudaMalloc(&dX, sizeof(double) * 3 * (n ? n : 1)));
+  ok(cudaMalloc(&dd, sizeof(double) * (n ? n : 1)));
+  ok(cudaMalloc(&doff, sizeof(long long) * (n + 1)));
+  if (n_filters > 0) ok(cudaMalloc(&dm, sizeof(unsigned short) * (n ? n : 1)));
+  if (e == cudaSuccess) {
+    ok(cudaMemcpy(dX, position, sizeof(double) * 3 * n, cudaMemcpyHostToDevice));
+    ok(cudaMemcpy(dd, delta, sizeof(double) * n, cudaMemcpyHostToDevice));
+    if (dm) ok(cudaMemcpy(dm, mask.data(), sizeof(unsigned short) * n, cudaMemcpyHostToDevice));
+  }
+  if (e == cudaSuccess) ok(device_find_bonds_grid(n, dX, dd, dm, lo, hc, nc, doff, &dnbr, &nb, &dup, s));
+  if (e == cudaSuccess && dup) st = fail(PD_ERR_ARG, "point duplicate found!");
+  if (e == cudaSuccess && st == PD_OK) {
+    *n_bonds = nb;
+    if (capacity >= nb && bond_offsets && (nb == 0 || (neighbors && bond_length && fail_permit))) {
+      ok(cudaMalloc(&dL, sizeof(double) * (nb ? nb : 1)));
+      ok(cudaMalloc(&dfp, n ? n : 1));
+      ok(cudaMalloc(&dfpb, nb ? nb : 1));
+      if (e == cudaSuccess) {
+        std::vector<unsigned char> fp(n, 1);
+        if (fp_point) std::copy(fp_point, fp_point + n, fp.begin());
+        ok(cudaMemcpy(dfp, fp.data(), n, cudaMemcpyHostToDevice));
+        if (nb) launch_bond_props(n, dX, dfp, doff, dnbr, dL, dfpb, s);
+        ok(cudaStreamSynchronize(s));
+        ok(cudaMemcpy(bond_offsets, doff, sizeof(long long) * (n + 1), cudaMemcpyDeviceToHost));
+        if (nb) {
+          ok(cudaMemcpy(neighbors, dnbr, sizeof(int) * nb, cudaMemcpyDeviceToHost));
+          ok(cudaMemcpy(bond_length, dL, sizeof(double) * nb, cudaMemcpyDeviceToHost));
+          ok(cudaMemcpy(fail_permit, dfpb, nb, cudaMemcpyDeviceToHost));
+        }
+      }
+    }
+  }
+  cudaFree(dX); cudaFree(dd); cudaFree(dm); cudaFree(doff); cudaFree(dnbr); cudaFree(dL);
+  cudaFree(dfp); cudaFree(dfpb);
+  cudaStreamDestroy(s);
+  if (e != cudaSuccess) return fail(PD_ERR_CUDA, std::string("pd_find_bonds: ") + cudaGetErrorString(e));
+  return st;
+}
+
+extern "C" pd_status pd_create_search(const pd_body_desc* desc, const uint8_t* fp_point,
+                                      int32_t n_filters, const uint8_t* filter_a,
+                                      const uint8_t* filter_b, pd_handle** out) {
+  PD_TRY(validate_desc(desc, false));
+  const long long n = desc->n_points;
+  std::vector<double> delta(n);
+  for (long long i = 0; i < n; i++) delta[i] = desc->params[desc->param_id ? desc->param_id[i] : 0].delta;
+  double lo[3], hc;
+  long long nc[3];
+  PD_TRY(search_grid(n, desc->position, delta.data(), lo, hc, nc));
+  std::vector<unsigned short> mask;
+  if (n_filters > 0) PD_TRY(pack_masks(n, n_filters, filter_a, filter_b, mask));
+  pd_handle* h = nullptr;
+  pd_status st = begin_create(desc, out, &h);
+  if (st != PD_OK) { if (h) pd_destroy(h); return st; }
+  double *dX = nullptr, *dd = nullptr;
+  unsigned short* dm = nullptr;
+  long long* doff = nullptr;
+  unsigned char *dfp = nullptr, *dfpb = nullptr;
+  std::vector<double> X(desc->position, desc->position + 3 * n);
+  st = dalloc(h, &dX, 3 * n);
+  if (st == PD_OK) st = dalloc(h, &dd, n);
+  if (st == PD_OK) st = dalloc(h, &doff, n + 1);
+  if (st == PD_OK && n_filters > 0) st = dalloc(h, &dm, n);
+  if (st == PD_OK) st = dalloc(h, &dfp, n);
+  if (st != PD_OK) { std::string m = g_err; pd_destroy(h); return fail(st, m); }
+  std::vector<unsigned char> fp(n, 1);
+  if (fp_point) std::copy(fp_point, fp_point + n, fp.begin());
+  cudaError_t e = cudaMemcpy(dX, X.data(), sizeof(double) * 3 * n, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(dd, delta.data(), sizeof(double) * n, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess && dm) e = cudaMemcpy(dm, mask.data(), sizeof(unsigned short) * n, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(dfp, fp.data(), n, cudaMemcpyHostToDevice);
+  int* dnbr = nullptr;
+  long long nb = 0;
+  int dup = 0;
+  if (e == cudaSuccess) e = device_find_bonds_grid(n, dX, dd, dm, lo, hc, nc, doff, &dnbr, &nb, &dup, h->stream);
+  if (e != cudaSuccess) { pd_destroy(h); return fail(PD_ERR_CUDA, cudaGetErrorString(e)); }
+  if (dup) { pd_destroy(h); return fail(PD_ERR_ARG, "point duplicate found!"); }
+  h->allocs.push_back(dnbr);
+  h->nb = nb;
+  h->d.nb = nb;
+  h->d.off = doff;
+  h->d.nbr = dnbr;
+  double* dL = nullptr;
+  st = dalloc(h, &dL, nb);
+  if (st == PD_OK) st = dalloc(h, &dfpb, nb);
+  if (st != PD_OK) { std::string m = g_err; pd_destroy(h); return fail(st, m); }
+  if (nb) launch_bond_props(n, dX, dfp, doff, dnbr, dL, dfpb, h->stream);
+  st = finish_create(h, desc, dL, dfpb);
+  dfree(h, dL); dfree(h, dfpb); dfree(h, dX); dfree(h, dd); dfree(h, dm); dfree(h, dfp);
+  if (st != PD_OK) { std::string m = g_err; pd_destroy(h); return fail(st, m); }
+  *out = h;
+  return PD_OK;
+}
+
+extern "C" pd_status pd_destroy(pd_handle* h) {
+  if (!h) return PD_OK;
+  cudaSetDevice(h->device);
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  destroy_graph(h);
+  for (void* p : h->allocs) cudaFree(p);
+  h->allocs.clear();
+  if (h->stream) cudaStreamDestroy(h->stream);
+  delete h;
+  return PD_OK;
+}
+
+static pd_status clear_error(pd_handle* h) {
+  const int z = 0;
+  PD_TRY(set_ctrl(h, offsetof(Ctrl, err), &z, sizeof(int)));
+  h->nan_step = -1;
+  return PD_OK;
+}
+
+extern "C" pd_status pd_set_state(pd_handle* h, const double* position, const double* displacement,
+                                  const double* velocity, const double* velocity_half,
+                                  const double* acceleration, const double* b_ext,
+                                  const uint8_t* bond_active) {
+  if (!h) return fail(PD_ERR_ARG, "handle is NULL");
+  PD_CUDA(cudaSetDevice(h->device));
+  PD_CUDA(cudaStreamSynchronize(h->stream));
+  const long long n = h->n, nb = h->nb;
+  if (n == 0) return PD_OK;
+  std::vector<double4> cur(n);
+  PD_CUDA(cudaMemcpy(cur.data(), h->d.cur, sizeof(double4) * n, cudaMemcpyDeviceToHost));
+  std::vector<double4> X0(n);
+  PD_CUDA(cudaMemcpy(X0.data(), h->d.X0, sizeof(double4) * n, cudaMemcpyDeviceToHost));
+  bool cur_changed = false;
+  if (h->precision == PD_PREC_FP64) {
+    if (position) {
+      for (long long i = 0; i < n; i++) { cur[i].x = position[3 * i]; cur[i].y = position[3 * i + 1]; cur[i].z = position[3 * i + 2]; }
+      cur_changed = true;
+    }
+    if (displacement) PD_CUDA(cudaMemcpy(h->g.u, displacement, sizeof(double) * 3 * n, cudaMemcpyHostToDevice));
+  } else {
+    if (displacement) {
+      for (long long i = 0; i < n; i++) { cur[i].x = displacement[3 * i]; cur[i].y = displacement[3 * i + 1]; cur[i].z = displacement[3 * i + 2]; }
+      cur_changed = true;
+    } else if (position) {
+      for (long long i = 0; i < n; i++) {
+        cur[i].x = position[3 * i] - X0[i].x; cur[i].y = position[3 * i + 1] - X0[i].y; cur[i].z = position[3 * i + 2] - X0[i].z;
+      }
+      cur_changed = true;
+    }
+  }
+  if (cur_changed) PD_CUDA(cudaMemcpy(h->d.cur, cur.data(), sizeof(double4) * n, cudaMemcpyHostToDevice));
+  if (velocity) PD_CUDA(cudaMemcpy(h->g.v, velocity, sizeof(double) * 3 * n, cudaMemcpyHostToDevice));
+  if (velocity_half) PD_CUDA(cudaMemcpy(h->g.vh, velocity_half, sizeof(double) * 3 * n, cudaMemcpyHostToDevice));
+  if (acceleration) PD_CUDA(cudaMemcpy(h->g.a, acceleration, sizeof(double) * 3 * n, cudaMemcpyHostToDevice));
+  if (b_ext) {
+    PD_CUDA(cudaMemcpy(h->g.bext, b_ext, sizeof(double) * 3 * n, cudaMemcpyHostToDevice));
+    for (long long i = 0; i < n; i++) {
+      const bool nz = b_ext[3 * i] != 0 || b_ext[3 * i + 1] != 0 || b_ext[3 * i + 2] != 0 ||
+                      std::signbit(b_ext[3 * i]) || std::signbit(b_ext[3 * i + 1]) || std::signbit(b_ext[3 * i + 2]);
+      const bool bc = !h->bext_pt.empty() && h->bext_pt[i];
+      if (nz || bc) h->hmeta[i] |= META_HAS_BEXT; else h->hmeta[i] &= ~META_HAS_BEXT;
+    }
+    PD_TRY(upload_meta(h));
+  }
+  if (bond_active && nb > 0) {
+    unsigned char* tmp = nullptr;
+    PD_CUDA(cudaMalloc(&tmp, nb));
+    cudaError_t e = cudaMemcpy(tmp, bond_active, nb, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) {
+      launch_pack_bits(tmp, h->d.bits, nb, h->stream);
+      e = cudaStreamSynchronize(h->stream);
+    }
+    cudaFree(tmp);
+    if (e != cudaSuccess) return fail(PD_ERR_CUDA, cudaGetErrorString(e));
+    launch_count_active(h->d, h->stream);
+    h->damage_valid = true;
+    PD_TRY(setup_symmetry(h));
+    destroy_graph(h);
+  }
+  PD_TRY(clear_error(h));
+  PD_CUDA(cudaStreamSynchronize(h->stream));
+  return PD_OK;
+}
+
+extern "C" pd_status pd_get_field(pd_handle* h, int32_t field, void* out, size_t bytes) {
+  if (!h || !out) return fail(PD_ERR_ARG, "handle or output is NULL");
+  PD_CUDA(cudaSetDevice(h->device));
+  PD_CUDA(cudaStreamSynchronize(h->stream));
+  const long long n = h->n, nb = h->nb;
+  size_t need = 0;
+  switch (field) {
+    case PD_FIELD_POSITION: case PD_FIELD_DISPLACEMENT: case PD_FIELD_VELOCITY:
+    case PD_FIELD_VELOCITY_HALF: case PD_FIELD_ACCELERATION: case PD_FIELD_B_INT:
+    case PD_FIELD_B_EXT: need = sizeof(double) * 3 * n; break;
+    case PD_FIELD_DAMAGE: need = sizeof(double) * n; break;
+    case PD_FIELD_N_ACTIVE_BONDS: need = sizeof(int64_t) * n; break;
+    case PD_FIELD_BOND_ACTIVE: need = nb; break;
+    case PD_FIELD_DEFGRAD: case PD_FIELD_CAUCHY_STRESS:
+      if (h->material != PD_MAT_CMAT) return fail(PD_ERR_ARG, "field only exists for CMaterial");
+      need = sizeof(double) * 9 * n; break;
+    default: return fail(PD_ERR_ARG, "unknown field");
+  }
+  if (bytes != need) return fail(PD_ERR_ARG, "output size is " + std::to_string(bytes) + " bytes, need " + std::to_string(need));
+  if (n == 0) return PD_OK;
+  auto copy = [&](const void* src) -> pd_status {
+    PD_CUDA(cudaMemcpy(out, src, need, cudaMemcpyDeviceToHost));
+    return PD_OK;
+  };
+  void* tmp = nullptr;
+  pd_status st = PD_OK;
+  switch (field) {
+    case PD_FIELD_POSITION: case PD_FIELD_DISPLACEMENT:
+      PD_CUDA(cudaMalloc(&tmp, need));
+      launch_export_position(h->d, h->g, (double*)tmp, field == PD_FIELD_POSITION ? 0 : 1, h->stream);
+      PD_CUDA(cudaStreamSynchronize(h->stream));
+      st = copy(tmp);
+      break;
+    case PD_FIELD_VELOCITY: st = copy(h->g.v); break;
+    case PD_FIELD_VELOCITY_HALF: st = copy(h->g.vh); break;
+    case PD_FIELD_ACCELERATION: st = copy(h->g.a); break;
+    case PD_FIELD_B_EXT: st = copy(h->g.bext); break;
+    case PD_FIELD_B_INT:
+      if (h->precision == PD_PREC_FP64) st = copy(h->d.b64);
+      else {
+        std::vector<float> f(3 * n);
+        PD_CUDA(cudaMemcpy(f.data(), h->d.b32, sizeof(float) * 3 * n, cudaMemcpyDeviceToHost));
+        double* o = (double*)out;
+        for (long long k = 0; k < 3 * n; k++) o[k] = f[k];
+      }
+      break;
+    case PD_FIELD_DAMAGE:
+      PD_CUDA(cudaMalloc(&tmp, need));
+      launch_export_damage(h->d, h->damage_valid ? 1 : 0, (double*)tmp, h->stream);
+      PD_CUDA(cudaStreamSynchronize(h->stream));
+      st = copy(tmp);
+      break;
+    case PD_FIELD_N_ACTIVE_BONDS: {
+      std::vector<int> na(n);
+      PD_CUDA(cudaMemcpy(na.data(), h->d.n_active, sizeof(int) * n, cudaMemcpyDeviceToHost));
+      int64_t* o = (int64_t*)out;
+      for (long long i = 0; i < n; i++) o[i] = na[i];
+      break;
+    }
+    case PD_FIELD_BOND_ACTIVE:
+      if (nb == 0) break;
+      PD_CUDA(cudaMalloc(&tmp, need));
+      launch_export_bond_active(h->d, (unsigned char*)tmp, h->stream);
+      PD_CUDA(cudaStreamSynchronize(h->stream));
+      st = copy(tmp);
+      break;
+    case PD_FIELD_DEFGRAD:
+      if (h->precision == PD_PREC_FP64) st = copy(h->d.F64);
+      else {
+        std::vector<float> f(9 * n);
+        PD_CUDA(cudaMemcpy(f.data(), h->d.H32, sizeof(float) * 9 * n, cudaMemcpyDeviceToHost));
+        double* o = (double*)out;
+        for (long long i = 0; i < n; i++)
+          for (int k = 0; k < 9; k++) o[9 * i + k] = (double)f[9 * i + k] + ((k % 4) == 0 ? 1.0 : 0.0);
+      }
+      break;
+    case PD_FIELD_CAUCHY_STRESS:
+      PD_CUDA(cudaMalloc(&tmp, need));
+      launch_cauchy64(h->d, h->d.F64, h->precision == PD_PREC_FP64 ? 0 : 1, (double*)tmp, h->stream);
+      PD_CUDA(cudaStreamSynchronize(h->stream));
+      st = copy(tmp);
+      break;
+  }
+  if (tmp) cudaFree(tmp);
+  PD_CUDA(cudaGetLastError());
+  return st;
+}
+
+extern "C" pd_status pd_set_bcs(pd_handle* h, int32_t n_bcs, const pd_bc_desc* bcs) {
+  if (!h) return fail(PD_ERR_ARG, "handle is NULL");
+  if (n_bcs < 0 || (n_bcs > 0 && !bcs)) return fail(PD_ERR_ARG, "invalid boundary conditions");
+  PD_CUDA(cudaSetDevice(h->device));
+  const long long n = h->n;
+  std::vector<BCInfo> info(n_bcs);
+  std::vector<std::vector<BCEntry>> per_point(n);
+  std::vector<double> data;
+  long long col = 0;
+  h->needs_table = false;
+  h->bext_pt.assign(n, 0);
+  for (int k = 0; k < n_bcs; k++) {
+    const pd_bc_desc& b = bcs[k];
+    if (b.field != PD_BC_VELOCITY_HALF && b.field != PD_BC_B_EXT) return fail(PD_ERR_ARG, "unknown boundary condition field");
+    if (b.dim < 0 || b.dim > 2) return fail(PD_ERR_ARG, "dimension must be 0, 1 or 2");
+    if (b.kind < PD_BC_KIND_TIME || b.kind > PD_BC_KIND_DATA) return fail(PD_ERR_ARG, "unknown boundary condition kind");
+    if (b.n_points < 0 || (b.n_points > 0 && !b.points)) return fail(PD_ERR_ARG, "boundary condition point list missing");
+    if (b.kind == PD_BC_KIND_DATA && b.n_points > 0 && !b.data) return fail(PD_ERR_ARG, "DataBC values missing");
+    info[k].field = b.field;
+    info[k].dim = b.dim;
+    info[k].kind = b.kind;
+    if (b.kind == PD_BC_KIND_TIME) { info[k].col = (int)col; col += 1; h->needs_table = true; }
+    else if (b.kind == PD_BC_KIND_POINT_TIME) { info[k].col = (int)col; col += b.n_points; h->needs_table = true; }
+    else { info[k].col = (int)data.size(); data.insert(data.end(), b.data, b.data + b.n_points); }
+    for (int q = 0; q < b.n_points; q++) {
+      const int p = b.points[q];
+      if (p < 0 || p >= n) return fail(PD_ERR_ARG, "boundary condition point out of range");
+      per_point[p].push_back(BCEntry{k, q});
+      if (b.field == PD_BC_B_EXT) h->bext_pt[p] = 1;
+    }
+  }
+  std::vector<int> pts, eoff(1, 0);
+  std::vector<BCEntry> ent;
+  for (long long i = 0; i < n; i++) {
+    h->hmeta[i] &= ~META_HAS_BC;
+    if (per_point[i].empty()) continue;
+    pts.push_back((int)i);
+    for (auto& e : per_point[i]) ent.push_back(e);
+    eoff.push_back((int)ent.size());
+    h->hmeta[i] |= META_HAS_BC;
+    if (h->bext_pt[i]) h->hmeta[i] |= META_HAS_BEXT;
+  }
+  PD_TRY(upload_meta(h));
+  PD_CUDA(cudaStreamSynchronize(h->stream));
+  // free the previous lists
+  dfree(h, (void*)h->bc.point); dfree(h, (void*)h->bc.entry_off); dfree(h, (void*)h->bc.entry);
+  dfree(h, (void*)h->bc.info); dfree(h, (void*)h->bc.data);
+  h->bc = BCDev{};
+  h->bc.table = h->table;
+  int *dp = nullptr, *de = nullptr;
+  BCEntry* den = nullptr;
+  BCInfo* di = nullptr;
+  double* dd = nullptr;
+  PD_TRY(dalloc(h, &dp, pts.size()));
+  PD_TRY(dalloc(h, &de, eoff.size()));
+  PD_TRY(dalloc(h, &den, ent.size()));
+  PD_TRY(dalloc(h, &di, info.size()));
+  PD_TRY(dalloc(h, &dd, data.size()));
+  if (!pts.empty()) PD_CUDA(cudaMemcpy(dp, pts.data(), sizeof(int) * pts.size(), cudaMemcpyHostToDevice));
+  PD_CUDA(cudaMemcpy(de, eoff.data(), sizeof(int) * eoff.size(), cudaMemcpyHostToDevice));
+  if (!ent.empty()) PD_CUDA(cudaMemcpy(den, ent.data(), sizeof(BCEntry) * ent.size(), cudaMemcpyHostToDevice));
+  if (!info.empty()) PD_CUDA(cudaMemcpy(di, info.data(), sizeof(BCInfo) * info.size(), cudaMemcpyHostToDevice));
+  if (!data.empty()) PD_CUDA(cudaMemcpy(dd, data.data(), sizeof(double) * data.size(), cudaMemcpyHostToDevice));
+  h->bc.n_points = (int)pts.size();
+  h->bc.point = dp;
+  h->bc.entry_off = de;
+  h->bc.entry = den;
+  h->bc.info = di;
+  h->bc.data = dd;
+  h->bc.per_step = col;
+  h->per_step = col;
+  h->bcinfo = info;
+  const long long zero = 0;
+  PD_TRY(set_ctrl(h, offsetof(Ctrl, table_n), &zero, sizeof(long long)));
+  PD_CUDA(cudaStreamSynchronize(h->stream));
+  h->version++;
+  destroy_graph(h);
+  return PD_OK;
+}
+
+extern "C" pd_status pd_set_bc_values(pd_handle* h, int64_t first_step, int64_t n_steps,
+                                      const double* values, int64_t n_values) {
+  if (!h) return fail(PD_ERR_ARG, "handle is NULL");
+  if (n_steps < 0) return fail(PD_ERR_ARG, "n_steps < 0");
+  if (n_values != n_steps * h->per_step)
+    return fail(PD_ERR_ARG, "expected " + std::to_string(n_steps * h->per_step) + " values");
+  PD_CUDA(cudaSetDevice(h->device));
+  if (n_values > h->table_cap) {
+    PD_CUDA(cudaStreamSynchronize(h->stream));
+    dfree(h, h->table);
+    h->table = nullptr;
+    PD_TRY(dalloc(h, &h->table, n_values));
+    h->table_cap = n_values;
+    h->bc.table = h->table;
+    h->version++;
+  }
+  if (n_values > 0)
+    PD_CUDA(cudaMemcpyAsync(h->table, values, sizeof(double) * n_values, cudaMemcpyHostToDevice, h->stream));
+  long long v[2] = {first_step, n_steps};
+  PD_TRY(set_ctrl(h, offsetof(Ctrl, table_first), v, sizeof(v)));
+  PD_CUDA(cudaStreamSynchronize(h->stream));
+  return PD_OK;
+}
+
+extern "C" pd_status pd_stable_timestep(pd_handle* h, double safety_factor, double* dt,
+                                        double* dt_per_param) {
+  if (!h || !dt) return fail(PD_ERR_ARG, "handle or dt is NULL");
+  PD_CUDA(cudaSetDevice(h->device));
+  const long long n = h->n;
+  double* tmp = nullptr;
+  std::vector<double> dtp(n);
+  if (n > 0) {
+    PD_CUDA(cudaMalloc(&tmp, sizeof(double) * n));
+    launch_timestep(h->d, tmp, h->stream);
+    cudaError_t e = cudaStreamSynchronize(h->stream);
+    if (e == cudaSuccess) e = cudaMemcpy(dtp.data(), tmp, sizeof(double) * n, cudaMemcpyDeviceToHost);
+    cudaFree(tmp);
+    if (e != cudaSuccess) return fail(PD_ERR_CUDA, cudaGetErrorString(e));
+  }
+  double m = INFINITY;
+  std::vector<double> mp(h->hp.size(), INFINITY);
+  for (long long i = 0; i < n; i++) {
+    m = std::min(m, dtp[i]);
+    const unsigned p = h->hmeta[i] & META_PID_MASK;
+    mp[p] = std::min(mp[p], dtp[i]);
+  }
+  *dt = m * safety_factor;
+  if (dt_per_param)
+    for (size_t k = 0; k < mp.size(); k++) dt_per_param[k] = mp[k] * safety_factor;
+  return PD_OK;
+}
+
+extern "C" pd_status pd_set_param_timesteps(pd_handle* h, const double* dtp) {
+  if (!h || !dtp) return fail(PD_ERR_ARG, "handle or dt_per_param is NULL");
+  PD_CUDA(cudaSetDevice(h->device));
+  for (size_t k = 0; k < h->hp.size(); k++) { h->hp[k].dt = dtp[k]; h->hp[k].dth = 0.5 * dtp[k]; }
+  PD_TRY(upload_params(h));
+  destroy_graph(h);
+  return PD_OK;
+}
+
+static int launch_force(pd_handle* h, int kstep, int phase) {
+  const int k = h->precision == PD_PREC_FP64 ? launch_force64(h->d, h->cfg, kstep, phase, h->stream)
+                                             : launch_force32(h->d, h->cfg, kstep, phase, h->stream);
+  h->launches += k;
+  return k;
+}
+
+static pd_status check_err(pd_handle* h) {
+  Ctrl c;
+  PD_CUDA(cudaMemcpyAsync(&c, h->d.ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, h->stream));
+  PD_CUDA(cudaStreamSynchronize(h->stream));
+  if (c.err == 1) {
+    h->nan_step = c.err_step;
+    return fail(PD_ERR_NAN, "NaN values detected in force density field! step: " + std::to_string(c.err_step));
+  }
+  if (c.err == 2)
+    return fail(PD_ERR_ARG, "boundary condition values missing for step " + std::to_string(c.err_step) +
+                                " (call pd_set_bc_values)");
+  return PD_OK;
+}
+
+extern "C" pd_status pd_force(pd_handle* h, double t, double dt) {
+  if (!h) return fail(PD_ERR_ARG, "handle is NULL");
+  PD_CUDA(cudaSetDevice(h->device));
+  PD_TRY(clear_error(h));
+  const long long step = (t > 0 && dt > 0) ? (long long)std::floor(t / dt) : 0;
+  PD_TRY(set_ctrl(h, offsetof(Ctrl, base), &step, sizeof(long long)));
+  launch_force(h, 0, 0);
+  PD_CUDA(cudaGetLastError());
+  h->damage_valid = true;
+  return check_err(h);
+}
+
+// one block of steps [kstep0, kstep0 + steps) as eager launches; timing events optional
+static void issue_steps(pd_handle* h, int steps, double dto, std::vector<cudaEvent_t>* ev) {
+  int e = 0;
+  auto rec = [&]() { if (ev) cudaEventRecord((*ev)[e++], h->stream); };
+  for (int k = 0; k < steps; k++) {
+    rec();
+    launch_kick_drift(h->d, h->g, k == 0 ? 0 : 1, dto, k, h->stream);
+    h->launches++;
+    if (h->bc.n_points > 0) { launch_bc(h->d, h->g, h->bc, dto, k, h->stream); h->launches++; }
+    rec();
+    launch_force(h, k, 1);
+    rec();
+    launch_force(h, k, 2);
+    rec();
+  }
+  rec();
+  launch_finish(h->d, h->g, dto, h->stream);
+  h->launches++;
+  rec();
+}
+
+static pd_status run_block_graph(pd_handle* h, int steps, double dto) {
+  GraphKey key;
+  key.steps = steps; key.group = h->cfg.group; key.block = h->cfg.block; key.exact = h->cfg.exact;
+  key.bcpts = h->bc.n_points; key.dt = dto; key.version = h->version;
+  if (!(h->gexec && key == h->gkey)) {
+    destroy_graph(h);
+    cudaGraph_t graph;
+    long long before = h->launches;
+    PD_CUDA(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+    issue_steps(h, steps, dto, nullptr);
+    cudaError_t e = cudaStreamEndCapture(h->stream, &graph);
+    if (e != cudaSuccess) return fail(PD_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+    h->graph_nodes = (int)(h->launches - before);
+    h->launches = before;
+    e = cudaGraphInstantiate(&h->gexec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) { h->gexec = nullptr; return fail(PD_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e)); }
+    h->gkey = key;
+  }
+  PD_CUDA(cudaGraphLaunch(h->gexec, h->stream));
+  h->launches += h->graph_nodes;
+  return PD_OK;
+}
+
+static pd_status run_vv(pd_handle* h, int64_t first_step, int64_t n_steps, double dt,
+                        std::vector<cudaEvent_t>* ev) {
+  if (!h) return fail(PD_ERR_ARG, "handle is NULL");
+  if (n_steps < 0) return fail(PD_ERR_ARG, "n_steps < 0");
+  if (n_steps == 0) return PD_OK;
+  PD_CUDA(cudaSetDevice(h->device));
+  double dto = dt > 0 ? dt : -1.0;
+  if (dto < 0)
+    for (auto& p : h->hp)
+      if (!(p.dt > 0)) return fail(PD_ERR_ARG, "dt <= 0 and no per-parameter time steps set");
+  if (h->needs_table) {
+    Ctrl c;
+    PD_CUDA(cudaMemcpy(&c, h->d.ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost));
+    if (c.table_first > first_step || c.table_first + c.table_n < first_step + n_steps)
+      return fail(PD_ERR_ARG, "boundary condition values do not cover steps " + std::to_string(first_step) +
+                                  ".." + std::to_string(first_step + n_steps - 1));
+  }
+  PD_TRY(clear_error(h));
+  int64_t done = 0;
+  const int K = h->graph_steps;
+  while (done < n_steps) {
+    const long long base = first_step + done;
+    int steps = (int)std::min<int64_t>(n_steps - done, (K > 0 && !ev) ? K : (int64_t)(1 << 30));
+    PD_TRY(set_ctrl(h, offsetof(Ctrl, base), &base, sizeof(long long)));
+    if (K > 0 && steps == K && !ev) {
+      PD_TRY(run_block_graph(h, steps, dto));
+    } else {
+      issue_steps(h, steps, dto, ev);
+      PD_CUDA(cudaGetLastError());
+    }
+    done += steps;
+    if (ev) break;
+  }
+  h->damage_valid = true;
+  return check_err(h);
+}
+
+extern "C" pd_status pd_run_vv(pd_handle* h, int64_t first_step, int64_t n_steps, double dt) {
+  return run_vv(h, first_step, n_steps, dt, nullptr);
+}
+
+extern "C" pd_status pd_run_vv_timed(pd_handle* h, int64_t first_step, int64_t n_steps, double dt,
+                                     double* ms_total, double* ms_phase_a, double* ms_phase_b,
+                                     double* ms_integrate) {
+  if (!h) return fail(PD_ERR_ARG, "handle is NULL");
+  if (n_steps <= 0) return fail(PD_ERR_ARG, "n_steps must be > 0");
+  if (n_steps > (1 << 20)) return fail(PD_ERR_ARG, "at most 2^20 timed steps per call");
+  PD_CUDA(cudaSetDevice(h->device));
+  const size_t nev = (size_t)4 * n_steps + 2;
+  std::vector<cudaEvent_t> ev(nev);
+  for (auto& e : ev) PD_CUDA(cudaEventCreate(&e));
+  pd_status st = run_vv(h, first_step, n_steps, dt, &ev);
+  if (st == PD_OK || st == PD_ERR_NAN) {
+    PD_CUDA(cudaStreamSynchronize(h->stream));
+    double ta = 0, tb = 0, ti = 0;
+    float x;
+    for (int64_t k = 0; k < n_steps; k++) {
+      cudaEventElapsedTime(&x, ev[4 * k], ev[4 * k + 1]); ti += x;
+      cudaEventElapsedTime(&x, ev[4 * k + 1], ev[4 * k + 2]); ta += x;
+      cudaEventElapsedTime(&x, ev[4 * k + 2], ev[4 * k + 3]); tb += x;
+    }
+    cudaEventElapsedTime(&x, ev[nev - 2], ev[nev - 1]); ti += x;
+    cudaEventElapsedTime(&x, ev[0], ev[nev - 1]);
+    if (ms_total) *ms_total = x;
+    if (ms_phase_a) *ms_phase_a = ta;
+    if (ms_phase_b) *ms_phase_b = tb;
+    if (ms_integrate) *ms_integrate = ti;
+  }
+  for (auto& e : ev) cudaEventDestroy(e);
+  return st;
+}
+
+extern "C" pd_status pd_nan_step(pd_handle* h, int64_t* step) {
+  if (!h || !step) return fail(PD_ERR_ARG, "handle or step is NULL");
+  *step = h->nan_step;
+  return PD_OK;
+}
+
+extern "C" pd_status pd_set_mapping(pd_handle* h, int32_t group, int32_t block) {
+  if (!h) return fail(PD_ERR_ARG, "handle is NULL");
+  if (block != 64 && block != 128 && block != 256) return fail(PD_ERR_ARG, "block must be 64, 128 or 256");
+  if (group == 0) {
+    if (h->precision != PD_PREC_FP64) return fail(PD_ERR_ARG, "the serial-order mapping (group 0) is FP64 only");
+    h->cfg.exact = true;
+    h->cfg.group = 1;
+  } else {
+    if (group != 1 && group != 2 && group != 4 && group != 8 && group != 16 && group != 32)
+      return fail(PD_ERR_ARG, "group must be 0, 1, 2, 4, 8, 16 or 32");
+    h->cfg.exact = false;
+    h->cfg.group = group;
+  }
+  h->cfg.block = block;
+  destroy_graph(h);
+  return PD_OK;
+}
+
+extern "C" pd_status pd_autotune(pd_handle* h, int32_t* group_out, int32_t* block_out) {
+  if (!h) return fail(PD_ERR_ARG, "handle is NULL");
+  PD_CUDA(cudaSetDevice(h->device));
+  const LaunchCfg keep = h->cfg;
+  cudaEvent_t e0, e1;
+  PD_CUDA(cudaEventCreate(&e0));
+  PD_CUDA(cudaEventCreate(&e1));
+  float best = INFINITY;
+  LaunchCfg bestc = keep;
+  const int groups[] = {1, 2, 4, 8, 16, 32};
+  const int blocks[] = {128, 256};
+  // force evaluations are idempotent at fixed positions: bonds that broke stay broken and
+  // every output is recomputed
+  for (int G : groups)
+    for (int B : blocks) {
+      h->cfg.group = G; h->cfg.block = B; h->cfg.exact = false;
+      launch_force(h, 0, 0);
+      cudaEventRecord(e0, h->stream);
+      for (int r = 0; r < 3; r++) launch_force(h, 0, 0);
+      cudaEventRecord(e1, h->stream);
+      cudaError_t e = cudaEventSynchronize(e1);
+      if (e != cudaSuccess) { cudaEventDestroy(e0); cudaEventDestroy(e1); return fail(PD_ERR_CUDA, cudaGetErrorString(e)); }
+      float ms;
+      cudaEventElapsedTime(&ms, e0, e1);
+      if (ms < best) { best = ms; bestc = h->cfg; }
+    }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  h->cfg = bestc;
+  destroy_graph(h);
+  if (group_out) *group_out = bestc.group;
+  if (block_out) *block_out = bestc.block;
+  return check_err(h);
+}
+
+extern "C" pd_status pd_set_graph(pd_handle* h, int32_t steps_per_graph) {
+  if (!h) return fail(PD_ERR_ARG, "handle is NULL");
+  if (steps_per_graph < 0 || steps_per_graph > 4096) return fail(PD_ERR_ARG, "0 <= steps_per_graph <= 4096");
+  h->graph_steps = steps_per_graph;
+  destroy_graph(h);
+  return PD_OK;
+}
+
+extern "C" pd_status pd_info(pd_handle* h, int64_t* n_points, int64_t* n_bonds, int32_t* symmetric) {
+  if (!h) return fail(PD_ERR_ARG, "handle is NULL");
+  if (n_points) *n_points = h->n;
+  if (n_bonds) *n_bonds = h->nb;
+  if (symmetric) *symmetric = h->d.sym;
+  return PD_OK;
+}
+
+extern "C" pd_status pd_launch_count(pd_handle* h, int64_t* count) {
+  if (!h || !count) return fail(PD_ERR_ARG, "handle or count is NULL");
+  *count = h->launches;
+  return PD_OK;
+}
+
+extern "C" pd_status pd_stream(pd_handle* h, void** stream) {
+  if (!h || !stream) return fail(PD_ERR_ARG, "handle or stream is NULL");
+  *stream = (void*)h->stream;
+  return PD_OK;
+}
+
+extern "C" pd_status pd_break_bonds(pd_handle* h, const uint8_t* set_a, const uint8_t* set_b) {
+  if (!h || (h->n > 0 && (!set_a || !set_b))) return fail(PD_ERR_ARG, "handle or point sets are NULL");
+  PD_CUDA(cudaSetDevice(h->device));
+  const long long n = h->n;
+  if (n == 0) return PD_OK;
+  for (long long i = 0; i < n; i++)
+    if (set_a[i] && set_b[i]) return fail(PD_ERR_ARG, "point sets intersect");
+  unsigned char* tmp = nullptr;
+  PD_CUDA(cudaMalloc(&tmp, 2 * n));
+  cudaError_t e = cudaMemcpy(tmp, set_a, n, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(tmp + n, set_b, n, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) {
+    launch_break_sets(h->d, tmp, tmp + n, h->stream);
+    launch_count_active(h->d, h->stream);
+    e = cudaStreamSynchronize(h->stream);
+  }
+  cudaFree(tmp);
+  if (e != cudaSuccess) return fail(PD_ERR_CUDA, cudaGetErrorString(e));
+  h->damage_valid = true;
+  destroy_graph(h);
+  return PD_OK;
+}
+
+extern "C" pd_status pd_break_random_pairs(pd_handle* h, double fraction, uint64_t seed) {
+  if (!h) return fail(PD_ERR_ARG, "handle is NULL");
+  if (!(fraction >= 0 && fraction <= 1)) return fail(PD_ERR_ARG, "fraction must be in [0, 1]");
+  PD_CUDA(cudaSetDevice(h->device));
+  if (h->n == 0) return PD_OK;
+  launch_break_random(h->d, fraction, (unsigned long long)seed, h->stream);
+  launch_count_active(h->d, h->stream);
+  PD_CUDA(cudaStreamSynchronize(h->stream));
+  h->damage_valid = true;
+  PD_TRY(setup_symmetry(h));
+  destroy_graph(h);
+  return PD_OK;
+}

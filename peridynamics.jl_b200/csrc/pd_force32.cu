@@ -1,0 +1,487 @@
+// pd_force32.cu -- FP32-compensated force-density kernels (the fast path).
+//
+// Per bond, in FP32:
+//   du  = (float)(u_j - u_i)           difference of the FP64 displacements, then rounded
+//   eta = xi + du                       deformed bond vector from the stored FP32 offset xi
+//   l   = |eta|
+//   e   = l - L = (2 xi.du + du.du) / (l + L)   (no cancellation at stretches ~1e-4)
+// Per-point sums use Neumaier-compensated FP32 accumulation and a fixed-order compensated
+// reduction over the G lanes of a point, so results are deterministic.
+//
+// The state-based materials run in gather form (phase A per point, phase B per point reading
+// the phase-A state of the neighbours) instead of the reference's scatter b_j -= p V_i.
+// With symmetric bond lists and symmetric bond states one bit per bond serves both
+// directions; otherwise the reverse-bond index gives the state of bond j -> i.
+//
+// Correspondence in FP32 uses the displacement gradient H = F - I (so that F - I does not
+// cancel) and a horizon-scaled shape tensor K' = K / delta^5 (the unscaled det K underflows
+// FP32 for millimetre lattices). The stress formulas are the reference's, rewritten in
+// terms of E = (H + H^T + H^T H) / 2 without cancelling subtractions.
+#include "pd_common.cuh"
+#include "pd_launch.h"
+
+namespace pd {
+
+__device__ __forceinline__ double4 ld4(const double4* p) {
+  const double2* q = reinterpret_cast<const double2*>(p);
+  double2 a = __ldg(q), b = __ldg(q + 1);
+  return make_double4(a.x, a.y, b.x, b.y);
+}
+
+struct BondF {
+  float gx, gy, gz, L;
+  float dux, duy, duz;
+  float ex, ey, ez, l, e;
+  bool fp;
+};
+
+__device__ __forceinline__ void bond32(const float4 g, const double4& ui, const double4& uj,
+                                       BondF& B) {
+  B.gx = g.x; B.gy = g.y; B.gz = g.z;
+  B.L = fabsf(g.w);
+  B.fp = g.w > 0.f;
+  B.dux = (float)(uj.x - ui.x);
+  B.duy = (float)(uj.y - ui.y);
+  B.duz = (float)(uj.z - ui.z);
+  B.ex = g.x + B.dux; B.ey = g.y + B.duy; B.ez = g.z + B.duz;
+  B.l = sqrtf(B.ex * B.ex + B.ey * B.ey + B.ez * B.ez);
+  const float xd = g.x * B.dux + g.y * B.duy + g.z * B.duz;
+  const float dd = B.dux * B.dux + B.duy * B.duy + B.duz * B.duz;
+  B.e = (2.f * xd + dd) / (B.l + B.L);
+}
+
+__device__ __forceinline__ void flag_nan32(const DevBody& d, int kstep, float x, float y, float z) {
+  if (isnan(x) || isnan(y) || isnan(z)) {
+    long long step = d.ctrl->base + kstep;
+    if (atomicExch(&d.ctrl->err, 1) == 0) d.ctrl->err_step = step;
+    else atomicMin(&d.ctrl->err_step, step);
+  }
+}
+
+#define PD_POINT_LOOP(G)                                                                     \
+  constexpr int PPW = 32 / (G);                                                              \
+  const int lane = threadIdx.x & 31;                                                         \
+  const int sub = lane / (G), gl = lane % (G);                                               \
+  const long long warp0 = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;           \
+  const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;                         \
+  for (long long w = warp0; w * PPW < d.n; w += nwarps)
+
+// failure test of CriticalStretch (bond_system.jl:309-327): eps > eps_c with permission
+__device__ __forceinline__ bool fail_test32(const DevBody& d, long long b, const BondF& B,
+                                            float epsc) {
+  bool act = bond_bit_live(d.bits, b);
+  if (act && B.e / B.L > epsc && B.fp) {
+    clear_bit(d.bits, b);
+    act = false;
+  }
+  return act;
+}
+
+// -------------------------------------------------------------------------------------------
+// BB (bond_based.jl:125-180): one sweep, failure then the pairwise force
+// -------------------------------------------------------------------------------------------
+template <int G, bool MULTI>
+__global__ void __launch_bounds__(256) k_bb32(DevBody d, int kstep) {
+  if (d.ctrl->err) return;
+  PD_POINT_LOOP(G) {
+    const long long i = w * PPW + sub;
+    const bool valid = i < d.n;
+    KSum bx, by, bz;
+    int na = 0;
+    if (valid) {
+      const double4 ui = ld4(d.cur + i);
+      const DevParam& P = d.params[d.meta[i] & META_PID_MASK];
+      const float epsc = P.epscf, bci = P.bcf;
+      const long long b0 = d.off[i], b1 = d.off[i + 1];
+      for (long long b = b0 + gl; b < b1; b += G) {
+        const int j = __ldg(d.nbr + b);
+        const float4 g = __ldg(d.geo + b);
+        const double4 uj = ld4(d.cur + j);
+        BondF B;
+        bond32(g, ui, uj, B);
+        const bool act = fail_test32(d, b, B, epsc);
+        na += act;
+        if (act) {
+          float bc = bci;
+          if (MULTI) bc = 0.5f * (bci + d.params[d.meta[j] & META_PID_MASK].bcf);
+          const float s = bc * (B.e / B.L) * (float)uj.w / B.l;
+          bx.add(s * B.ex); by.add(s * B.ey); bz.add(s * B.ez);
+        }
+      }
+    }
+    if (G > 1) { group_reduce<G>(bx); group_reduce<G>(by); group_reduce<G>(bz); na = group_sum<G>(na); }
+    if (valid && gl == 0) {
+      const float x = bx.value(), y = by.value(), z = bz.value();
+      d.b32[3 * i] = x; d.b32[3 * i + 1] = y; d.b32[3 * i + 2] = z;
+      d.n_active[i] = na;
+      flag_nan32(d, kstep, x, y, z);
+    }
+  }
+}
+
+// -------------------------------------------------------------------------------------------
+// OSB phase A (ordinary_state_based.jl:107-126, 176-204): failure, weighted volume m,
+// dilatation theta, and c1 = 15 G / m, c2 = theta (3 K / m - c1 / 3) (:135-136)
+// -------------------------------------------------------------------------------------------
+template <int G>
+__global__ void __launch_bounds__(256) k_osb_a32(DevBody d, int kstep) {
+  if (d.ctrl->err) return;
+  PD_POINT_LOOP(G) {
+    const long long i = w * PPW + sub;
+    const bool valid = i < d.n;
+    KSum m, th;
+    int na = 0;
+    const DevParam& P = d.params[valid ? (d.meta[i] & META_PID_MASK) : 0];
+    if (valid) {
+      const double4 ui = ld4(d.cur + i);
+      const float epsc = P.epscf, delta = P.deltaf;
+      const long long b0 = d.off[i], b1 = d.off[i + 1];
+      for (long long b = b0 + gl; b < b1; b += G) {
+        const int j = __ldg(d.nbr + b);
+        const float4 g = __ldg(d.geo + b);
+        const double4 uj = ld4(d.cur + j);
+        BondF B;
+        bond32(g, ui, uj, B);
+        const bool act = fail_test32(d, b, B, epsc);
+        na += act;
+        if (act) {
+          const float om = omega_of_f(d.kernel, delta, B.L) * (float)uj.w;
+          m.add(om * (B.gx * B.gx + B.gy * B.gy + B.gz * B.gz));
+          th.add(om * B.L * B.e);
+        }
+      }
+    }
+    if (G > 1) { group_reduce<G>(m); group_reduce<G>(th); na = group_sum<G>(na); }
+    if (valid && gl == 0) {
+      const float wv = m.value();
+      float c1 = 0.f, c2 = 0.f, dil = 0.f;
+      if (wv != 0.f) {
+        dil = 3.f / wv * th.value();
+        c1 = 15.f * P.Gf / wv;
+        c2 = dil * (3.f * P.Kf / wv - c1 / 3.f);
+      }
+      d.coef32[i] = make_float4(c1, c2, wv, dil);
+      d.n_active[i] = na;
+    }
+  }
+}
+
+template <bool MULTI>
+__device__ __forceinline__ float osb_s32(const float4& co, const DevParam& Po, const DevParam& Pq,
+                                         float om, float L, float e) {
+  float c1 = co.x, c2 = co.y;
+  if (MULTI) {
+    if (co.z == 0.f) return 0.f;
+    c1 = 15.f * (Po.Gf + Pq.Gf) / (2.f * co.z);
+    c2 = co.w * (3.f * (Po.Kf + Pq.Kf) / (2.f * co.z) - c1 / 3.f);
+  }
+  return om * (c2 * L + c1 * e);
+}
+
+// -------------------------------------------------------------------------------------------
+// OSB phase B (ordinary_state_based.jl:128-174): b_i = sum_j (s_ij + s_ji) V_j eta / l
+// -------------------------------------------------------------------------------------------
+template <int G, bool MULTI>
+__global__ void __launch_bounds__(256) k_osb_b32(DevBody d, int kstep) {
+  if (d.ctrl->err) return;
+  PD_POINT_LOOP(G) {
+    const long long i = w * PPW + sub;
+    const bool valid = i < d.n;
+    KSum bx, by, bz;
+    if (valid) {
+      const double4 ui = ld4(d.cur + i);
+      const DevParam& Pi = d.params[d.meta[i] & META_PID_MASK];
+      const float4 ci = d.coef32[i];
+      const long long b0 = d.off[i], b1 = d.off[i + 1];
+      for (long long b = b0 + gl; b < b1; b += G) {
+        const int j = __ldg(d.nbr + b);
+        const float4 g = __ldg(d.geo + b);
+        const double4 uj = ld4(d.cur + j);
+        const float4 cj = __ldg(d.coef32 + j);
+        BondF B;
+        bond32(g, ui, uj, B);
+        const bool ai = bond_bit(d.bits, b);
+        const bool aj = d.sym ? ai : bond_bit(d.bits, __ldg(d.rev + b));
+        if (!(ai || aj)) continue;
+        float oi, oj;
+        const DevParam* Pj = &Pi;
+        if (MULTI) Pj = &d.params[d.meta[j] & META_PID_MASK];
+        oi = ai ? omega_of_f(d.kernel, Pi.deltaf, B.L) : 0.f;
+        oj = aj ? (MULTI ? omega_of_f(d.kernel, Pj->deltaf, B.L) : omega_of_f(d.kernel, Pi.deltaf, B.L)) : 0.f;
+        const float si = osb_s32<MULTI>(ci, Pi, *Pj, oi, B.L, B.e);
+        const float sj = osb_s32<MULTI>(cj, *Pj, Pi, oj, B.L, B.e);
+        const float f = (si + sj) * (float)uj.w / B.l;
+        bx.add(f * B.ex); by.add(f * B.ey); bz.add(f * B.ez);
+      }
+    }
+    if (G > 1) { group_reduce<G>(bx); group_reduce<G>(by); group_reduce<G>(bz); }
+    if (valid && gl == 0) {
+      const float x = bx.value(), y = by.value(), z = bz.value();
+      d.b32[3 * i] = x; d.b32[3 * i + 1] = y; d.b32[3 * i + 2] = z;
+      flag_nan32(d, kstep, x, y, z);
+    }
+  }
+}
+
+// ------------------------------------------------------------------------------------------
+// FP32 3x3 helpers (column-major) for the correspondence material
+// ------------------------------------------------------------------------------------------
+__device__ __forceinline__ void fcross(const float* a, const float* b, float* c) {
+  c[0] = a[1] * b[2] - a[2] * b[1];
+  c[1] = a[2] * b[0] - a[0] * b[2];
+  c[2] = a[0] * b[1] - a[1] * b[0];
+}
+__device__ __forceinline__ void finv3(const float* A, float* R) {
+  float x0[3] = {A[0], A[1], A[2]}, y0[3], y1[3], y2[3];
+  fcross(A + 3, A + 6, y0);
+  const float d = x0[0] * y0[0] + x0[1] * y0[1] + x0[2] * y0[2];
+  for (int k = 0; k < 3; k++) { x0[k] /= d; y0[k] /= d; }
+  fcross(A + 6, x0, y1);
+  fcross(x0, A + 3, y2);
+  for (int c = 0; c < 3; c++) { R[3 * c] = y0[c]; R[1 + 3 * c] = y1[c]; R[2 + 3 * c] = y2[c]; }
+}
+__device__ __forceinline__ void fmatmul(const float* A, const float* B, float* C) {
+  for (int r = 0; r < 3; r++)
+    for (int c = 0; c < 3; c++)
+      C[r + 3 * c] = A[r] * B[3 * c] + A[r + 3] * B[1 + 3 * c] + A[r + 6] * B[2 + 3 * c];
+}
+
+// P(F = I + H) of the reference's models, written without the cancelling F^T F - I
+__device__ void pk1_32(int cmodel, const DevParam& p, const float* H, float* P) {
+  float E[9], S[9], HS[9];
+  for (int r = 0; r < 3; r++)
+    for (int c = 0; c < 3; c++) {
+      const float hth = H[3 * r] * H[3 * c] + H[1 + 3 * r] * H[1 + 3 * c] + H[2 + 3 * r] * H[2 + 3 * c];
+      E[r + 3 * c] = 0.5f * (H[r + 3 * c] + H[c + 3 * r] + hth);
+    }
+  const float trE = E[0] + E[4] + E[8];
+  if (cmodel == CM_SVK) {
+    // S = lambda tr(E) I + 2 mu E
+    for (int k = 0; k < 9; k++) S[k] = 2.f * p.muf * E[k] + ((k % 4) == 0 ? p.lambdaf * trE : 0.f);
+  } else {
+    // J - 1 = tr H + (principal 2x2 minors of H) + det H
+    const float m2 = (H[0] * H[4] - H[3] * H[1]) + (H[0] * H[8] - H[6] * H[2]) + (H[4] * H[8] - H[7] * H[5]);
+    float dH;
+    {
+      float c[3];
+      fcross(H + 3, H + 6, c);
+      dH = H[0] * c[0] + H[1] * c[1] + H[2] * c[2];
+    }
+    const float jm1 = (H[0] + H[4] + H[8]) + m2 + dH;
+    const float J = 1.f + jm1;
+    float C[9], Ci[9], T[9];
+    for (int k = 0; k < 9; k++) C[k] = 2.f * E[k] + ((k % 4) == 0 ? 1.f : 0.f);
+    finv3(C, Ci);
+    if (cmodel == CM_NEOHOOKE) {
+      // S = mu (I - C^-1) + lambda ln J C^-1 = C^-1 (2 mu E + lambda ln J I)
+      const float lj = p.lambdaf * log1pf(jm1);
+      for (int k = 0; k < 9; k++) T[k] = 2.f * p.muf * E[k] + ((k % 4) == 0 ? lj : 0.f);
+    } else {
+      // NeoHookePenalty: S = C^-1 (2 G J^(-2/3) dev E + K/4 (J^2 - J^-2) I), P = 0 if J < eps
+      if (!(J >= 2.220446049250313e-16f)) {
+        for (int k = 0; k < 9; k++) P[k] = 0.f;
+        return;
+      }
+      const float jp = expf(-2.f / 3.f * log1pf(jm1));
+      const float iJ = 1.f / J;
+      const float vol = 0.25f * p.Kf * (jm1 * (J + 1.f) * iJ) * (J + iJ);
+      for (int k = 0; k < 9; k++)
+        T[k] = 2.f * p.Gf * jp * (E[k] - ((k % 4) == 0 ? trE / 3.f : 0.f)) + ((k % 4) == 0 ? vol : 0.f);
+    }
+    fmatmul(Ci, T, S);
+  }
+  // P = F S = S + H S
+  fmatmul(H, S, HS);
+  for (int k = 0; k < 9; k++) P[k] = S[k] + HS[k];
+}
+
+// -------------------------------------------------------------------------------------------
+// CMat phase A (correspondence.jl:193-224, 288-298; bond_system.jl:309-327)
+// -------------------------------------------------------------------------------------------
+template <int G>
+__global__ void __launch_bounds__(256) k_c_a32(DevBody d, int kstep) {
+  if (d.ctrl->err) return;
+  PD_POINT_LOOP(G) {
+    const long long i = w * PPW + sub;
+    const bool valid = i < d.n;
+    KSum K[6], Hs[9];
+    int na = 0;
+    unsigned meta = 0;
+    long long b0 = 0, b1 = 0;
+    const DevParam& P = d.params[valid ? (d.meta[i] & META_PID_MASK) : 0];
+    if (valid) {
+      meta = d.meta[i];
+      const double4 ui = ld4(d.cur + i);
+      const float epsc = P.epscf, id = P.inv_delta, vs = P.vscale;
+      b0 = d.off[i]; b1 = d.off[i + 1];
+      for (long long b = b0 + gl; b < b1; b += G) {
+        const int j = __ldg(d.nbr + b);
+        const float4 g = __ldg(d.geo + b);
+        const double4 uj = ld4(d.cur + j);
+        BondF B;
+        bond32(g, ui, uj, B);
+        const bool act = fail_test32(d, b, B, epsc);
+        na += act;
+        if (act) {
+          const float t = omega_of_f(d.kernel, P.deltaf, B.L) * (float)uj.w * vs;
+          const float X[3] = {B.gx * id, B.gy * id, B.gz * id};
+          const float U[3] = {B.dux * id, B.duy * id, B.duz * id};
+          K[0].add(t * X[0] * X[0]); K[1].add(t * X[1] * X[1]); K[2].add(t * X[2] * X[2]);
+          K[3].add(t * X[0] * X[1]); K[4].add(t * X[0] * X[2]); K[5].add(t * X[1] * X[2]);
+#pragma unroll
+          for (int c = 0; c < 3; c++)
+#pragma unroll
+            for (int r = 0; r < 3; r++) Hs[r + 3 * c].add(t * U[r] * X[c]);
+        }
+      }
+    }
+    if (G > 1) {
+#pragma unroll
+      for (int k = 0; k < 6; k++) group_reduce<G>(K[k]);
+#pragma unroll
+      for (int k = 0; k < 9; k++) group_reduce<G>(Hs[k]);
+      na = group_sum<G>(na);
+    }
+    bool killed = false;
+    if (valid && gl == 0) {
+      const float Km[9] = {K[0].value(), K[3].value(), K[4].value(),
+                           K[3].value(), K[1].value(), K[5].value(),
+                           K[4].value(), K[5].value(), K[2].value()};
+      float Kinv[9], Hm[9], H[9];
+      finv3(Km, Kinv);
+      for (int k = 0; k < 9; k++) Hm[k] = Hs[k].value();
+      fmatmul(Hm, Kinv, H);
+      bool hasnan = false;
+      for (int k = 0; k < 9; k++) { d.H32[9 * i + k] = H[k]; hasnan |= isnan(H[k]); }
+      const double damage = 1.0 - (double)na / (double)(b1 - b0);
+      killed = (meta & META_KILLED) || damage > d.maxdmg || hasnan;
+      float4* cs = d.cst32 + 3 * i;
+      if (killed) {
+        if (!(meta & META_KILLED)) d.meta[i] = meta | META_KILLED;
+        na = 0;
+        cs[0] = make_float4(0.f, 0.f, 0.f, 0.f);
+        cs[1] = make_float4(0.f, 0.f, 0.f, 0.f);
+        cs[2] = make_float4(0.f, 0.f, 0.f, 0.f);
+      } else {
+        float Pm[9], PK[9], A[9];
+        pk1_32(d.cmodel, P, H, Pm);
+        fmatmul(Pm, Kinv, PK);
+        const float id = P.inv_delta, id5 = id * id * id * id * id;
+        for (int k = 0; k < 9; k++) A[k] = PK[k] * id5 - P.betaf * H[k];
+        cs[0] = make_float4(A[0], A[1], A[2], A[3]);
+        cs[1] = make_float4(A[4], A[5], A[6], A[7]);
+        cs[2] = make_float4(A[8], P.betaf, 0.f, 0.f);
+      }
+      d.n_active[i] = na;
+    }
+    if (!d.sym) {
+      if (G > 1) killed = group_bcast<G>(killed);
+      if (valid && killed)
+        for (long long b = b0 + gl; b < b1; b += G) clear_bit(d.bits, b);
+    }
+  }
+}
+
+// -------------------------------------------------------------------------------------------
+// CMat phase B (correspondence.jl:226-251): with A = P K^-1 - beta H,
+//   t_ij = w (A_i xi + beta_i du), and j's term -t_ji = w (A_j xi + beta_j du)
+// -------------------------------------------------------------------------------------------
+template <int G>
+__global__ void __launch_bounds__(256) k_c_b32(DevBody d, int kstep) {
+  if (d.ctrl->err) return;
+  PD_POINT_LOOP(G) {
+    const long long i = w * PPW + sub;
+    const bool valid = i < d.n;
+    KSum bx, by, bz;
+    if (valid) {
+      const double4 ui = ld4(d.cur + i);
+      const DevParam& Pi = d.params[d.meta[i] & META_PID_MASK];
+      const float4 a0 = d.cst32[3 * i], a1 = d.cst32[3 * i + 1], a2 = d.cst32[3 * i + 2];
+      const float Ai[9] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w, a2.x};
+      const float bi = a2.y;
+      const long long b0 = d.off[i], b1 = d.off[i + 1];
+      for (long long b = b0 + gl; b < b1; b += G) {
+        const int j = __ldg(d.nbr + b);
+        const float4 g = __ldg(d.geo + b);
+        const double4 uj = ld4(d.cur + j);
+        const bool ai = bond_bit(d.bits, b);
+        const bool aj = d.sym ? ai : bond_bit(d.bits, __ldg(d.rev + b));
+        if (!(ai || aj)) continue;
+        const float4 c0 = __ldg(d.cst32 + 3 * (long long)j), c1 = __ldg(d.cst32 + 3 * (long long)j + 1),
+                     c2 = __ldg(d.cst32 + 3 * (long long)j + 2);
+        const float L = fabsf(g.w);
+        const float du[3] = {(float)(uj.x - ui.x), (float)(uj.y - ui.y), (float)(uj.z - ui.z)};
+        const float oi = ai ? omega_of_f(d.kernel, Pi.deltaf, L) : 0.f;
+        float oj = 0.f;
+        if (aj) {
+          float dj = Pi.deltaf;
+          if (d.multi) dj = d.params[d.meta[j] & META_PID_MASK].deltaf;
+          oj = omega_of_f(d.kernel, dj, L);
+        }
+        const float Aj[9] = {c0.x, c0.y, c0.z, c0.w, c1.x, c1.y, c1.z, c1.w, c2.x};
+        const float bj = c2.y;
+        const float V = (float)uj.w;
+        float t[3];
+#pragma unroll
+        for (int r = 0; r < 3; r++) {
+          const float ti = Ai[r] * g.x + Ai[r + 3] * g.y + Ai[r + 6] * g.z + bi * du[r];
+          const float tj = Aj[r] * g.x + Aj[r + 3] * g.y + Aj[r + 6] * g.z + bj * du[r];
+          t[r] = (oi * ti + oj * tj) * V;
+        }
+        bx.add(t[0]); by.add(t[1]); bz.add(t[2]);
+      }
+    }
+    if (G > 1) { group_reduce<G>(bx); group_reduce<G>(by); group_reduce<G>(bz); }
+    if (valid && gl == 0) {
+      const float x = bx.value(), y = by.value(), z = bz.value();
+      d.b32[3 * i] = x; d.b32[3 * i + 1] = y; d.b32[3 * i + 2] = z;
+      flag_nan32(d, kstep, x, y, z);
+    }
+  }
+}
+
+// ------------------------------------------------------------------------------------------
+#define PD_DISPATCH_G(G, CALL)                          \
+  switch (G) {                                          \
+    case 1: { constexpr int GG = 1; CALL; } break;      \
+    case 2: { constexpr int GG = 2; CALL; } break;      \
+    case 4: { constexpr int GG = 4; CALL; } break;      \
+    case 8: { constexpr int GG = 8; CALL; } break;      \
+    case 16: { constexpr int GG = 16; CALL; } break;    \
+    default: { constexpr int GG = 32; CALL; } break;    \
+  }
+
+static int grid_for32(long long n, int G, int block) {
+  long long warps = (n + (32 / G) - 1) / (32 / G);
+  long long blocks = (warps + block / 32 - 1) / (block / 32);
+  if (blocks < 1) blocks = 1;
+  if (blocks > 148LL * 64) blocks = 148LL * 64;
+  return (int)blocks;
+}
+
+int launch_force32(const DevBody& d, const LaunchCfg& c, int kstep, int phase, cudaStream_t s) {
+  const int G = c.group < 1 ? 1 : c.group;
+  const int grid = grid_for32(d.n, G, c.block);
+  const bool A = phase != 2, B = phase != 1;
+  int launches = 0;
+  if (d.material == MAT_BB) {
+    if (!A) return 0;
+    if (d.multi) { PD_DISPATCH_G(G, (k_bb32<GG, true><<<grid, c.block, 0, s>>>(d, kstep))); }
+    else { PD_DISPATCH_G(G, (k_bb32<GG, false><<<grid, c.block, 0, s>>>(d, kstep))); }
+    return 1;
+  }
+  if (d.material == MAT_OSB) {
+    if (A) { PD_DISPATCH_G(G, (k_osb_a32<GG><<<grid, c.block, 0, s>>>(d, kstep))); launches++; }
+    if (B) {
+      if (d.multi) { PD_DISPATCH_G(G, (k_osb_b32<GG, true><<<grid, c.block, 0, s>>>(d, kstep))); }
+      else { PD_DISPATCH_G(G, (k_osb_b32<GG, false><<<grid, c.block, 0, s>>>(d, kstep))); }
+      launches++;
+    }
+    return launches;
+  }
+  if (A) { PD_DISPATCH_G(G, (k_c_a32<GG><<<grid, c.block, 0, s>>>(d, kstep))); launches++; }
+  if (B) { PD_DISPATCH_G(G, (k_c_b32<GG><<<grid, c.block, 0, s>>>(d, kstep))); launches++; }
+  return launches;
+}
+
+}  // namespace pd

@@ -1,0 +1,573 @@
+// pd_force64.cu -- FP64 force-density kernels (the plain FP64 path).
+//
+// Compiled with -fmad=false: Julia rounds every product and sum separately, and these kernels
+// keep the reference's evaluation order, so with one lane per point (G = 1, "exact order")
+// the per-point results equal the serial CPU restatement bit for bit:
+//   - BB: one bond sweep (failure test, then the bond force) in bond order;
+//   - OSB / CMat: phase A per point (failure, damage, weighted volume and dilatation, or the
+//     deformation gradient and stress), phase B gathers the force density. The reference
+//     scatters b_j -= p V_i while it processes point i; phase B reproduces the order in which
+//     those scattered terms reach b_i in the serial loop: first the terms of neighbours j < i
+//     (ascending j), then the own bonds of i, then the terms of neighbours j > i.
+// With G > 1 lanes per point the same arithmetic is summed in a fixed butterfly order
+// (deterministic, not bit-identical to the serial order).
+#include "pd_common.cuh"
+#include "pd_launch.h"
+
+namespace pd {
+
+__device__ __forceinline__ double4 ld4(const double4* p) {
+  const double2* q = reinterpret_cast<const double2*>(p);
+  double2 a = __ldg(q), b = __ldg(q + 1);
+  return make_double4(a.x, a.y, b.x, b.y);
+}
+
+__device__ __forceinline__ double dot3(const double* a, const double* b) {
+  return (a[0] * b[0] + a[1] * b[1]) + a[2] * b[2];
+}
+__device__ __forceinline__ void cross3(const double* a, const double* b, double* c) {
+  c[0] = a[1] * b[2] - a[2] * b[1];
+  c[1] = a[2] * b[0] - a[0] * b[2];
+  c[2] = a[0] * b[1] - a[1] * b[0];
+}
+// StaticArrays 3x3 det / inv (column-major), as the CPU restatement
+__device__ __forceinline__ double det3(const double* A) {
+  double c[3];
+  cross3(A + 3, A + 6, c);
+  return dot3(A, c);
+}
+__device__ __forceinline__ void inv3(const double* A, double* R) {
+  double x0[3] = {A[0], A[1], A[2]};
+  double y0[3], y1[3], y2[3];
+  cross3(A + 3, A + 6, y0);
+  double d = dot3(x0, y0);
+  for (int k = 0; k < 3; k++) { x0[k] = x0[k] / d; y0[k] = y0[k] / d; }
+  cross3(A + 6, x0, y1);
+  cross3(x0, A + 3, y2);
+  for (int c = 0; c < 3; c++) { R[3 * c] = y0[c]; R[1 + 3 * c] = y1[c]; R[2 + 3 * c] = y2[c]; }
+}
+__device__ __forceinline__ void matmul3(const double* A, const double* B, double* C) {
+  for (int r = 0; r < 3; r++)
+    for (int c = 0; c < 3; c++)
+      C[r + 3 * c] = (A[r] * B[3 * c] + A[r + 3] * B[1 + 3 * c]) + A[r + 6] * B[2 + 3 * c];
+}
+__device__ __forceinline__ void matTmul3(const double* A, const double* B, double* C) {
+  for (int r = 0; r < 3; r++)
+    for (int c = 0; c < 3; c++)
+      C[r + 3 * c] = (A[3 * r] * B[3 * c] + A[1 + 3 * r] * B[1 + 3 * c]) + A[2 + 3 * r] * B[2 + 3 * c];
+}
+__device__ __forceinline__ void matmulT3(const double* A, const double* B, double* C) {
+  for (int r = 0; r < 3; r++)
+    for (int c = 0; c < 3; c++)
+      C[r + 3 * c] = (A[r] * B[c] + A[r + 3] * B[c + 3]) + A[r + 6] * B[c + 6];
+}
+__device__ __forceinline__ void matvec3(const double* A, const double* v, double* w) {
+  for (int r = 0; r < 3; r++) w[r] = (A[r] * v[0] + A[r + 3] * v[1]) + A[r + 6] * v[2];
+}
+
+// first_piola_kirchhoff (constitutive_models.jl:35-41, 169-176, 233-244)
+__device__ void pk1_64(int cmodel, const DevParam& p, const double* F, double* P) {
+  double C[9], S[9];
+  if (cmodel == CM_SVK) {
+    double E[9];
+    matTmul3(F, F, C);
+    for (int k = 0; k < 9; k++) E[k] = 0.5 * (C[k] - ((k % 4) == 0 ? 1.0 : 0.0));
+    double trE = (E[0] + E[4]) + E[8];
+    double a = p.lambda * trE, m2 = 2 * p.mu;
+    for (int k = 0; k < 9; k++) S[k] = (k % 4) == 0 ? m2 * E[k] + a : m2 * E[k];
+  } else if (cmodel == CM_NEOHOOKE) {
+    double J = det3(F), Ci[9];
+    matTmul3(F, F, C);
+    inv3(C, Ci);
+    double lj = p.lambda * log(J);
+    for (int k = 0; k < 9; k++) S[k] = p.mu * ((k % 4) == 0 ? -Ci[k] + 1.0 : -Ci[k]) + lj * Ci[k];
+  } else {
+    double J = det3(F);
+    if (J < 2.220446049250313e-16 || isnan(J)) {
+      for (int k = 0; k < 9; k++) P[k] = 0.0;
+      return;
+    }
+    double Ci[9];
+    matTmul3(F, F, C);
+    inv3(C, Ci);
+    double trC = (C[0] + C[4]) + C[8];
+    double a = 1.0 / 3.0 * trC;
+    double jp = pow(J, -2.0 / 3.0);
+    double ij = 1.0 / J;
+    double vol = p.K / 4 * (J * J - ij * ij);
+    for (int k = 0; k < 9; k++)
+      S[k] = p.G * ((k % 4) == 0 ? -(a * Ci[k]) + 1.0 : -(a * Ci[k])) * jp + vol * Ci[k];
+  }
+  matmul3(F, S, P);
+}
+
+__device__ __forceinline__ void flag_nan(const DevBody& d, int kstep, double x, double y, double z) {
+  if (isnan(x) || isnan(y) || isnan(z)) {
+    long long step = d.ctrl->base + kstep;
+    if (atomicExch(&d.ctrl->err, 1) == 0) d.ctrl->err_step = step;
+    else atomicMin(&d.ctrl->err_step, step);
+  }
+}
+
+// the warp-uniform loop over point groups: every lane of a warp runs the same number of
+// iterations so that the group shuffles see all lanes
+#define PD_POINT_LOOP(G)                                                                     \
+  constexpr int PPW = 32 / (G);                                                              \
+  const int lane = threadIdx.x & 31;                                                         \
+  const int sub = lane / (G), gl = lane % (G);                                               \
+  const long long warp0 = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;           \
+  const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;                         \
+  for (long long w = warp0; w * PPW < d.n; w += nwarps)
+
+// -------------------------------------------------------------------------------------------
+// BB: bond_based.jl:125-180 (calc_failure! storing the bond length, force_density_point!)
+// -------------------------------------------------------------------------------------------
+template <int G, bool MULTI>
+__global__ void __launch_bounds__(256) k_bb64(DevBody d, int kstep) {
+  if (d.ctrl->err) return;
+  PD_POINT_LOOP(G) {
+    const long long i = w * PPW + sub;
+    const bool valid = i < d.n;
+    double bx = 0.0, by = 0.0, bz = 0.0;
+    int na = 0;
+    if (valid) {
+      const double4 xi = ld4(d.cur + i);
+      const DevParam P = d.params[d.meta[i] & META_PID_MASK];
+      const long long b0 = d.off[i], b1 = d.off[i + 1];
+      for (long long b = b0 + gl; b < b1; b += G) {
+        const int j = __ldg(d.nbr + b);
+        const double Ls = __ldg(d.len64 + b);
+        const double L = fabs(Ls);
+        const double4 xj = ld4(d.cur + j);
+        const double dx = xj.x - xi.x, dy = xj.y - xi.y, dz = xj.z - xi.z;
+        const double l = sqrt((dx * dx + dy * dy) + dz * dz);
+        const double eps = (l - L) / L;
+        bool act = bond_bit_live(d.bits, b);
+        if (act && eps > P.epsc && Ls > 0) { act = false; clear_bit(d.bits, b); }
+        na += act;
+        const double om = act ? 1.0 : 0.0;
+        double s;
+        if (MULTI) {
+          const double bcj = d.params[d.meta[j] & META_PID_MASK].bc;
+          s = om * (P.bc + bcj) / 2 * eps * xj.w;
+        } else {
+          s = om * P.bc * eps * xj.w;
+        }
+        bx += s * dx / l;
+        by += s * dy / l;
+        bz += s * dz / l;
+      }
+    }
+    if (G > 1) {
+      bx = group_sum<G>(bx); by = group_sum<G>(by); bz = group_sum<G>(bz); na = group_sum<G>(na);
+    }
+    if (valid && gl == 0) {
+      d.b64[3 * i] = bx; d.b64[3 * i + 1] = by; d.b64[3 * i + 2] = bz;
+      d.n_active[i] = na;
+      flag_nan(d, kstep, bx, by, bz);
+    }
+  }
+}
+
+// -------------------------------------------------------------------------------------------
+// OSB phase A: calc_failure! (ordinary_state_based.jl:107-126), calc_damage!,
+// calc_weighted_volume (:176-189), calc_dilatation (:191-204), c1, c2 (:135-136)
+// -------------------------------------------------------------------------------------------
+template <int G, bool EXACT>
+__global__ void __launch_bounds__(256) k_osb_a64(DevBody d, int kstep) {
+  if (d.ctrl->err) return;
+  PD_POINT_LOOP(G) {
+    const long long i = w * PPW + sub;
+    const bool valid = i < d.n;
+    double wvol = 0.0, sdil = 0.0;
+    int na = 0;
+    const DevParam P = d.params[valid ? (d.meta[i] & META_PID_MASK) : 0];
+    long long b0 = 0, b1 = 0;
+    double4 xi = make_double4(0, 0, 0, 0), Xi = xi;
+    if (valid) {
+      xi = ld4(d.cur + i); Xi = ld4(d.X0 + i);
+      b0 = d.off[i]; b1 = d.off[i + 1];
+      for (long long b = b0 + gl; b < b1; b += G) {
+        const int j = __ldg(d.nbr + b);
+        const double Ls = __ldg(d.len64 + b);
+        const double L = fabs(Ls);
+        const double4 xj = ld4(d.cur + j), Xj = ld4(d.X0 + j);
+        const double dx = xj.x - xi.x, dy = xj.y - xi.y, dz = xj.z - xi.z;
+        const double l = sqrt((dx * dx + dy * dy) + dz * dz);
+        const double eps = (l - L) / L;
+        bool act = bond_bit_live(d.bits, b);
+        if (act && eps > P.epsc && Ls > 0) { act = false; clear_bit(d.bits, b); }
+        na += act;
+        const double DX = Xj.x - Xi.x, DY = Xj.y - Xi.y, DZ = Xj.z - Xi.z;
+        const double om = act ? omega_of(d.kernel, P.delta, L) : 0.0;
+        wvol += om * 1.0 * ((DX * DX + DY * DY) + DZ * DZ) * xj.w;
+        if (!EXACT) sdil += om * 1.0 * L * (l - L) * xj.w;
+      }
+    }
+    if (G > 1) {
+      wvol = group_sum<G>(wvol); sdil = group_sum<G>(sdil); na = group_sum<G>(na);
+    }
+    double dil = 0.0;
+    if (EXACT && valid && wvol != 0.0) {
+      // second sweep of the reference with c1 = 3 / wvol inside every term
+      const double c1d = 3.0 / wvol;
+      for (long long b = b0; b < b1; b++) {
+        const int j = __ldg(d.nbr + b);
+        const double Ls = __ldg(d.len64 + b);
+        const double L = fabs(Ls);
+        const double4 xj = ld4(d.cur + j);
+        const double dx = xj.x - xi.x, dy = xj.y - xi.y, dz = xj.z - xi.z;
+        const double l = sqrt((dx * dx + dy * dy) + dz * dz);
+        const double eps = (l - L) / L;
+        // the bit may have been cleared above; the decision is recomputed from the same eps
+        const bool act = bond_bit_live(d.bits, b) && !(eps > P.epsc && Ls > 0);
+        const double om = act ? omega_of(d.kernel, P.delta, L) : 0.0;
+        dil += om * 1.0 * c1d * L * (l - L) * xj.w;
+      }
+    } else if (!EXACT && wvol != 0.0) {
+      dil = 3.0 / wvol * sdil;
+    }
+    if (valid && gl == 0) {
+      double c1 = 0.0, c2 = 0.0;
+      if (wvol != 0.0) {
+        c1 = 15.0 * P.G / wvol;
+        c2 = dil * (3.0 * P.K / wvol - c1 / 3.0);
+      }
+      d.coef64[i] = make_double4(c1, c2, wvol, dil);
+      d.n_active[i] = na;
+    }
+  }
+}
+
+// p = omega beta (c2 L + c1 (l - L)) / l (ordinary_state_based.jl:144), coefficients of the
+// bond owner o with the partner q (ParameterHandler form :165-166 when MULTI)
+template <bool MULTI>
+__device__ __forceinline__ double osb_s64(const DevBody& d, const double4& co, const DevParam& Po,
+                                          const DevParam& Pq, double om, double L, double l) {
+  double c1, c2;
+  if (MULTI) {
+    c1 = 15.0 * (Po.G + Pq.G) / (2 * co.z);
+    c2 = co.w * (3.0 * (Po.K + Pq.K) / (2 * co.z) - c1 / 3.0);
+  } else {
+    c1 = co.x;
+    c2 = co.y;
+  }
+  return om * 1.0 * (c2 * L + c1 * (l - L)) / l;
+}
+
+// -------------------------------------------------------------------------------------------
+// OSB phase B: force_density_point! (ordinary_state_based.jl:128-174) in gather form
+// -------------------------------------------------------------------------------------------
+template <int G, bool EXACT, bool MULTI>
+__global__ void __launch_bounds__(256) k_osb_b64(DevBody d, int kstep) {
+  if (d.ctrl->err) return;
+  PD_POINT_LOOP(G) {
+    const long long i = w * PPW + sub;
+    const bool valid = i < d.n;
+    double bx = 0.0, by = 0.0, bz = 0.0;
+    if (valid) {
+      const double4 xi = ld4(d.cur + i);
+      const double Vi = xi.w;
+      (void)Vi;
+      const DevParam Pi = d.params[d.meta[i] & META_PID_MASK];
+      const double4 ci = d.coef64[i];
+      const bool own = ci.z != 0.0;
+      const long long b0 = d.off[i], b1 = d.off[i + 1];
+      // own term of bond b
+      auto own_term = [&](long long b) {
+        const int j = __ldg(d.nbr + b);
+        const double L = fabs(__ldg(d.len64 + b));
+        const double4 xj = ld4(d.cur + j);
+        const double dx = xj.x - xi.x, dy = xj.y - xi.y, dz = xj.z - xi.z;
+        const double l = sqrt((dx * dx + dy * dy) + dz * dz);
+        const bool act = bond_bit(d.bits, b);
+        const double om = act ? omega_of(d.kernel, Pi.delta, L) : 0.0;
+        const DevParam& Pj = MULTI ? d.params[d.meta[j] & META_PID_MASK] : Pi;
+        const double s = osb_s64<MULTI>(d, ci, Pi, Pj, om, L, l);
+        bx += s * dx * xj.w;
+        by += s * dy * xj.w;
+        bz += s * dz * xj.w;
+      };
+      // term that j's loop scatters into b_i through its bond j -> i
+      auto nbr_term = [&](long long b) {
+        const int j = __ldg(d.nbr + b);
+        const double4 cj = d.coef64[j];
+        if (cj.z == 0.0) return;  // j returned early (iszero(wvol))
+        const double L = fabs(__ldg(d.len64 + b));
+        const double4 xj = ld4(d.cur + j);
+        const double dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
+        const double l = sqrt((dx * dx + dy * dy) + dz * dz);
+        const bool act = d.sym ? bond_bit(d.bits, b) : bond_bit(d.bits, __ldg(d.rev + b));
+        const DevParam Pj = d.params[d.meta[j] & META_PID_MASK];
+        const double om = act ? omega_of(d.kernel, Pj.delta, L) : 0.0;
+        const double s = osb_s64<MULTI>(d, cj, Pj, Pi, om, L, l);
+        bx += -(s * dx) * xj.w;
+        by += -(s * dy) * xj.w;
+        bz += -(s * dz) * xj.w;
+      };
+      if (EXACT) {
+        long long split = b0;
+        while (split < b1 && __ldg(d.nbr + split) < i) split++;
+        for (long long b = b0; b < split; b++) nbr_term(b);
+        if (own)
+          for (long long b = b0; b < b1; b++) own_term(b);
+        for (long long b = split; b < b1; b++) nbr_term(b);
+      } else {
+        for (long long b = b0 + gl; b < b1; b += G) {
+          if (own) own_term(b);
+          nbr_term(b);
+        }
+      }
+    }
+    if (G > 1) { bx = group_sum<G>(bx); by = group_sum<G>(by); bz = group_sum<G>(bz); }
+    if (valid && gl == 0) {
+      d.b64[3 * i] = bx; d.b64[3 * i + 1] = by; d.b64[3 * i + 2] = bz;
+      flag_nan(d, kstep, bx, by, bz);
+    }
+  }
+}
+
+// -------------------------------------------------------------------------------------------
+// CMat phase A: calc_failure! (bond_system.jl:309-327), calc_damage!,
+// calc_deformation_gradient! (correspondence.jl:193-214), too_much_damage! (:288-298),
+// calc_first_piola_kirchhoff! (:216-224)
+// -------------------------------------------------------------------------------------------
+template <int G>
+__global__ void __launch_bounds__(256) k_c_a64(DevBody d, int kstep) {
+  if (d.ctrl->err) return;
+  PD_POINT_LOOP(G) {
+    const long long i = w * PPW + sub;
+    const bool valid = i < d.n;
+    double K[9], Ft[9];
+    for (int k = 0; k < 9; k++) { K[k] = 0.0; Ft[k] = 0.0; }
+    int na = 0;
+    unsigned meta = 0;
+    long long b0 = 0, b1 = 0;
+    DevParam P = d.params[0];
+    if (valid) {
+      meta = d.meta[i];
+      P = d.params[meta & META_PID_MASK];
+      const double4 xi = ld4(d.cur + i), Xi = ld4(d.X0 + i);
+      b0 = d.off[i]; b1 = d.off[i + 1];
+      for (long long b = b0 + gl; b < b1; b += G) {
+        const int j = __ldg(d.nbr + b);
+        const double Ls = __ldg(d.len64 + b);
+        const double L = fabs(Ls);
+        const double4 xj = ld4(d.cur + j), Xj = ld4(d.X0 + j);
+        const double dx[3] = {xj.x - xi.x, xj.y - xi.y, xj.z - xi.z};
+        const double l = sqrt(dot3(dx, dx));
+        const double eps = (l - L) / L;
+        bool act = bond_bit_live(d.bits, b);
+        if (act && eps > P.epsc && Ls > 0) { act = false; clear_bit(d.bits, b); }
+        na += act;
+        const double DX[3] = {Xj.x - Xi.x, Xj.y - Xi.y, Xj.z - Xi.z};
+        const double om = act ? omega_of(d.kernel, P.delta, L) : 0.0;
+        const double temp = om * xj.w;
+        for (int c = 0; c < 3; c++)
+          for (int r = 0; r < 3; r++) {
+            K[r + 3 * c] = K[r + 3 * c] + temp * (DX[r] * DX[c]);
+            Ft[r + 3 * c] = Ft[r + 3 * c] + temp * (dx[r] * DX[c]);
+          }
+      }
+    }
+    if (G > 1) {
+      for (int k = 0; k < 9; k++) { K[k] = group_sum<G>(K[k]); Ft[k] = group_sum<G>(Ft[k]); }
+      na = group_sum<G>(na);
+    }
+    bool killed = false;
+    if (valid && gl == 0) {
+      const long long nn = b1 - b0;
+      const double damage = 1.0 - (double)na / (double)nn;
+      double Kinv[9], F[9];
+      inv3(K, Kinv);
+      matmul3(Ft, Kinv, F);
+      bool hasnan = false;
+      for (int k = 0; k < 9; k++) { d.F64[9 * i + k] = F[k]; hasnan |= isnan(F[k]); }
+      killed = (meta & META_KILLED) || damage > d.maxdmg || hasnan;
+      if (killed) {
+        if (!(meta & META_KILLED)) d.meta[i] = meta | META_KILLED;
+        na = 0;
+      } else {
+        double Pm[9], PKinv[9];
+        pk1_64(d.cmodel, P, F, Pm);
+        matmul3(Pm, Kinv, PKinv);
+        for (int k = 0; k < 9; k++) d.PK64[9 * i + k] = PKinv[k];
+      }
+      d.n_active[i] = na;
+    }
+    // directed bond states: a killed point loses all its bonds (correspondence.jl:293)
+    if (!d.sym) {
+      if (G > 1) killed = group_bcast<G>(killed);
+      if (valid && killed)
+        for (long long b = b0 + gl; b < b1; b += G) clear_bit(d.bits, b);
+    }
+  }
+}
+
+// -------------------------------------------------------------------------------------------
+// CMat phase B: c_force_density!(::ZEMSilling) (correspondence.jl:226-251) in gather form
+// -------------------------------------------------------------------------------------------
+__device__ __forceinline__ void c_bond_t64(const double* F, const double* PK, double beta,
+                                           double om, const double* DX, const double* dx,
+                                           double* t) {
+  double FD[3], z[3], W[9], WD[3];
+  matvec3(F, DX, FD);
+  for (int k = 0; k < 3; k++) z[k] = dx[k] - FD[k];
+  const double ob = om * beta;
+  for (int k = 0; k < 9; k++) W[k] = om * PK[k];
+  matvec3(W, DX, WD);
+  for (int k = 0; k < 3; k++) t[k] = WD[k] + ob * z[k];
+}
+
+template <int G, bool EXACT>
+__global__ void __launch_bounds__(256) k_c_b64(DevBody d, int kstep) {
+  if (d.ctrl->err) return;
+  PD_POINT_LOOP(G) {
+    const long long i = w * PPW + sub;
+    const bool valid = i < d.n;
+    double bx = 0.0, by = 0.0, bz = 0.0;
+    if (valid) {
+      const double4 xi = ld4(d.cur + i), Xi = ld4(d.X0 + i);
+      const unsigned mi = d.meta[i];
+      const DevParam Pi = d.params[mi & META_PID_MASK];
+      const bool own = !(mi & META_KILLED);
+      double Fi[9], PKi[9];
+      if (own)
+        for (int k = 0; k < 9; k++) { Fi[k] = d.F64[9 * i + k]; PKi[k] = d.PK64[9 * i + k]; }
+      const long long b0 = d.off[i], b1 = d.off[i + 1];
+      auto own_term = [&](long long b) {
+        const int j = __ldg(d.nbr + b);
+        const double L = fabs(__ldg(d.len64 + b));
+        const double4 xj = ld4(d.cur + j), Xj = ld4(d.X0 + j);
+        const double DX[3] = {Xj.x - Xi.x, Xj.y - Xi.y, Xj.z - Xi.z};
+        const double dx[3] = {xj.x - xi.x, xj.y - xi.y, xj.z - xi.z};
+        const bool act = bond_bit(d.bits, b);
+        const double om = act ? omega_of(d.kernel, Pi.delta, L) : 0.0;
+        double t[3];
+        c_bond_t64(Fi, PKi, Pi.beta, om, DX, dx, t);
+        bx += t[0] * xj.w; by += t[1] * xj.w; bz += t[2] * xj.w;
+      };
+      auto nbr_term = [&](long long b) {
+        const int j = __ldg(d.nbr + b);
+        const unsigned mj = d.meta[j];
+        if (mj & META_KILLED) return;  // j returned early after too_much_damage!
+        const double L = fabs(__ldg(d.len64 + b));
+        const bool act = d.sym ? bond_bit(d.bits, b) : bond_bit(d.bits, __ldg(d.rev + b));
+        const DevParam Pj = d.params[mj & META_PID_MASK];
+        const double4 xj = ld4(d.cur + j), Xj = ld4(d.X0 + j);
+        const double DX[3] = {Xi.x - Xj.x, Xi.y - Xj.y, Xi.z - Xj.z};
+        const double dx[3] = {xi.x - xj.x, xi.y - xj.y, xi.z - xj.z};
+        const double om = act ? omega_of(d.kernel, Pj.delta, L) : 0.0;
+        double Fj[9], PKj[9], t[3];
+        for (int k = 0; k < 9; k++) { Fj[k] = d.F64[9 * (long long)j + k]; PKj[k] = d.PK64[9 * (long long)j + k]; }
+        c_bond_t64(Fj, PKj, Pj.beta, om, DX, dx, t);
+        bx += -t[0] * xj.w; by += -t[1] * xj.w; bz += -t[2] * xj.w;
+      };
+      if (EXACT) {
+        long long split = b0;
+        while (split < b1 && __ldg(d.nbr + split) < i) split++;
+        for (long long b = b0; b < split; b++) nbr_term(b);
+        if (own)
+          for (long long b = b0; b < b1; b++) own_term(b);
+        for (long long b = split; b < b1; b++) nbr_term(b);
+      } else {
+        for (long long b = b0 + gl; b < b1; b += G) {
+          if (own) own_term(b);
+          nbr_term(b);
+        }
+      }
+    }
+    if (G > 1) { bx = group_sum<G>(bx); by = group_sum<G>(by); bz = group_sum<G>(bz); }
+    if (valid && gl == 0) {
+      d.b64[3 * i] = bx; d.b64[3 * i + 1] = by; d.b64[3 * i + 2] = bz;
+      flag_nan(d, kstep, bx, by, bz);
+    }
+  }
+}
+
+// cauchy_stress (stress.jl:112-116) of the stored F, for the export of the CMat stress field
+__global__ void k_cauchy64(DevBody d, const double* F, int from_h32, double* out) {
+  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= d.n) return;
+  const DevParam P = d.params[d.meta[i] & META_PID_MASK];
+  double Fm[9], Pm[9], Ps[9], S[9];
+  for (int k = 0; k < 9; k++)
+    Fm[k] = from_h32 ? (double)d.H32[9 * i + k] + ((k % 4) == 0 ? 1.0 : 0.0) : F[9 * i + k];
+  pk1_64(d.cmodel, P, Fm, Pm);
+  const double J = det3(Fm), iJ = 1 / J;
+  for (int k = 0; k < 9; k++) Ps[k] = iJ * Pm[k];
+  matmulT3(Ps, Fm, S);
+  const bool killed = d.meta[i] & META_KILLED;
+  for (int k = 0; k < 9; k++) out[9 * i + k] = killed ? 0.0 : S[k];
+}
+
+// ------------------------------------------------------------------------------------------
+// launchers
+// ------------------------------------------------------------------------------------------
+#define PD_DISPATCH_G(G, CALL)                  \
+  switch (G) {                                  \
+    case 1: { constexpr int GG = 1; CALL; } break;  \
+    case 2: { constexpr int GG = 2; CALL; } break;  \
+    case 4: { constexpr int GG = 4; CALL; } break;  \
+    case 8: { constexpr int GG = 8; CALL; } break;  \
+    case 16: { constexpr int GG = 16; CALL; } break; \
+    default: { constexpr int GG = 32; CALL; } break; \
+  }
+
+static int grid_for(long long n, int G, int block) {
+  long long warps = (n + (32 / G) - 1) / (32 / G);
+  long long blocks = (warps + block / 32 - 1) / (block / 32);
+  if (blocks < 1) blocks = 1;
+  if (blocks > 148LL * 64) blocks = 148LL * 64;
+  return (int)blocks;
+}
+
+int launch_force64(const DevBody& d, const LaunchCfg& c, int kstep, int phase, cudaStream_t s) {
+  const int G = c.exact ? 1 : c.group;
+  const int grid = grid_for(d.n, G, c.block);
+  const bool A = phase != 2, B = phase != 1;
+  int launches = 0;
+  if (d.material == MAT_BB) {
+    if (!A) return 0;
+    if (d.multi) { PD_DISPATCH_G(G, (k_bb64<GG, true><<<grid, c.block, 0, s>>>(d, kstep))); }
+    else { PD_DISPATCH_G(G, (k_bb64<GG, false><<<grid, c.block, 0, s>>>(d, kstep))); }
+    return 1;
+  }
+  if (d.material == MAT_OSB) {
+    if (A) {
+      if (c.exact) k_osb_a64<1, true><<<grid, c.block, 0, s>>>(d, kstep);
+      else { PD_DISPATCH_G(G, (k_osb_a64<GG, false><<<grid, c.block, 0, s>>>(d, kstep))); }
+      launches++;
+    }
+    if (B) {
+      if (c.exact) {
+        if (d.multi) k_osb_b64<1, true, true><<<grid, c.block, 0, s>>>(d, kstep);
+        else k_osb_b64<1, true, false><<<grid, c.block, 0, s>>>(d, kstep);
+      } else if (d.multi) {
+        PD_DISPATCH_G(G, (k_osb_b64<GG, false, true><<<grid, c.block, 0, s>>>(d, kstep)));
+      } else {
+        PD_DISPATCH_G(G, (k_osb_b64<GG, false, false><<<grid, c.block, 0, s>>>(d, kstep)));
+      }
+      launches++;
+    }
+    return launches;
+  }
+  if (A) {
+    PD_DISPATCH_G(G, (k_c_a64<GG><<<grid, c.block, 0, s>>>(d, kstep)));
+    launches++;
+  }
+  if (B) {
+    if (c.exact) k_c_b64<1, true><<<grid, c.block, 0, s>>>(d, kstep);
+    else { PD_DISPATCH_G(G, (k_c_b64<GG, false><<<grid, c.block, 0, s>>>(d, kstep))); }
+    launches++;
+  }
+  return launches;
+}
+
+void launch_cauchy64(const DevBody& d, const double* F, int from_h32, double* out, cudaStream_t s) {
+  int grid = (int)((d.n + 255) / 256);
+  if (grid < 1) grid = 1;
+  k_cauchy64<<<grid, 256, 0, s>>>(d, F, from_h32, out);
+}
+
+}  // namespace pd

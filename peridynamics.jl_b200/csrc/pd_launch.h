@@ -1,0 +1,73 @@
+// pd_launch.h -- host-side launchers exported by each kernel translation unit of libpdcuda.
+#pragma once
+#include <cuda_runtime.h>
+#include "pd_common.cuh"
+
+namespace pd {
+
+struct LaunchCfg {
+  int group;  // lanes per point: 1, 2, 4, 8, 16, 32
+  int block;  // threads per block
+  bool exact; // FP64: one lane per point in the reference's serial summation order
+};
+
+// boundary conditions as the integration kernels see them
+struct BCInfo {
+  int field;  // 0 velocity_half, 1 b_ext
+  int dim;
+  int kind;   // 0 time table, 1 per point per step, 2 constant data
+  int col;    // column in the per-step table (kinds 0, 1) or offset into the data (kind 2)
+};
+struct BCEntry {
+  int bc;     // index into BCInfo
+  int q;      // position of the point in the condition's point list
+};
+struct BCDev {
+  int n_points;          // points that carry conditions
+  const int* point;      // [n_points]
+  const int* entry_off;  // [n_points + 1]
+  const BCEntry* entry;
+  const BCInfo* info;
+  const double* table;   // [table_n][per_step]
+  long long per_step;
+  const double* data;
+};
+
+// integration state (FP64 in both precision modes)
+struct IntDev {
+  double* u;    // FP64 path displacement [3n] (FP32 path: displacement lives in cur)
+  double* vh;
+  double* v;
+  double* a;
+  double* bext;
+  int fp32;     // 1: FP32 force output b32, displacement in cur
+};
+
+// force evaluation; phase 0 = all kernels, 1 = the first (BB: the only) kernel, 2 = the
+// second kernel of the state-based materials. Returns the number of kernels launched.
+int launch_force64(const DevBody& d, const LaunchCfg& c, int kstep, int phase, cudaStream_t s);
+int launch_force32(const DevBody& d, const LaunchCfg& c, int kstep, int phase, cudaStream_t s);
+void launch_cauchy64(const DevBody& d, const double* F, int from_h32, double* out, cudaStream_t s);
+
+// integration: mode 0 = kick from the stored (v, a), mode 1 = kick from the last force
+void launch_kick_drift(const DevBody& d, const IntDev& g, int mode, double dt_override, int kstep,
+                       cudaStream_t s);
+void launch_bc(const DevBody& d, const IntDev& g, const BCDev& bc, double dt_override, int kstep,
+               cudaStream_t s);
+void launch_finish(const DevBody& d, const IntDev& g, double dt_override, cudaStream_t s);
+
+// helpers of the API layer
+void launch_pack_bits(const unsigned char* bytes, unsigned int* bits, long long nb, cudaStream_t s);
+void launch_export_bond_active(const DevBody& d, unsigned char* out, cudaStream_t s);
+void launch_count_active(const DevBody& d, cudaStream_t s);
+void launch_reverse(const DevBody& d, int* rev, int* flags, cudaStream_t s);
+void launch_check_sym(const DevBody& d, const int* rev, int* flags, cudaStream_t s);
+void launch_export_damage(const DevBody& d, int valid, double* out, cudaStream_t s);
+void launch_export_position(const DevBody& d, const IntDev& g, double* out, int what, cudaStream_t s);
+void launch_timestep(const DevBody& d, double* dt_point, cudaStream_t s);
+void launch_build_len64(const DevBody& d, const double* L, const unsigned char* fp, double* out, cudaStream_t s);
+void launch_build_geo(const DevBody& d, const double* L, const unsigned char* fp, float4* out, cudaStream_t s);
+void launch_break_sets(const DevBody& d, const unsigned char* A, const unsigned char* B, cudaStream_t s);
+void launch_break_random(const DevBody& d, double fraction, unsigned long long seed, cudaStream_t s);
+
+}  // namespace pd

@@ -1,0 +1,134 @@
+"""ctypes binding of libpdcuda (the C ABI declared in include/pdcuda.h).
+
+The library is loaded from this package directory. There is no CPU fallback: when the
+library is missing or the machine has no CUDA device, the calls fail with an error.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libpdcuda.so")
+_LIB = None
+
+# status codes
+PD_OK, PD_ERR_ARG, PD_ERR_CUDA, PD_ERR_NAN, PD_ERR_TIMEOUT, PD_ERR_OOM, PD_ERR_UNSUPPORTED = range(7)
+# materials, models, kernels, precision
+MAT_BB, MAT_OSB, MAT_CMAT = 0, 1, 2
+CM_SVK, CM_NEOHOOKE, CM_NEOHOOKE_PENALTY = 0, 1, 2
+KERNEL_CONST_ONE, KERNEL_LINEAR, KERNEL_CUBIC_BSPLINE = 0, 1, 2
+PREC_FP64, PREC_FP32_KAHAN = 0, 1
+# fields
+(F_POSITION, F_DISPLACEMENT, F_VELOCITY, F_VELOCITY_HALF, F_ACCELERATION, F_B_INT, F_B_EXT,
+ F_DAMAGE, F_N_ACTIVE_BONDS, F_BOND_ACTIVE, F_DEFGRAD, F_CAUCHY_STRESS) = range(12)
+BC_VELOCITY_HALF, BC_B_EXT = 0, 1
+BC_KIND_TIME, BC_KIND_POINT_TIME, BC_KIND_DATA = 0, 1, 2
+
+# every symbol that include/pdcuda.h declares
+EXPORTS = (
+    "pd_last_error", "pd_version", "pd_find_bonds", "pd_create", "pd_create_search",
+    "pd_destroy", "pd_set_state", "pd_break_bonds", "pd_break_random_pairs", "pd_get_field",
+    "pd_set_bcs", "pd_set_bc_values", "pd_stable_timestep", "pd_set_param_timesteps",
+    "pd_force", "pd_run_vv", "pd_nan_step", "pd_run_vv_timed", "pd_autotune", "pd_set_mapping",
+    "pd_set_graph", "pd_info", "pd_launch_count", "pd_stream",
+)
+
+
+class PointParams(C.Structure):
+    _fields_ = [(k, C.c_double) for k in
+                ("delta", "rho", "E", "nu", "G", "K", "lambda_", "mu", "Gc", "epsilon_c", "bc")]
+
+
+class BodyDesc(C.Structure):
+    _fields_ = [("n_points", C.c_int64), ("position", C.c_void_p), ("volume", C.c_void_p),
+                ("n_bonds", C.c_int64), ("bond_offsets", C.c_void_p), ("neighbors", C.c_void_p),
+                ("bond_length", C.c_void_p), ("fail_permit", C.c_void_p),
+                ("param_id", C.c_void_p), ("n_params", C.c_int32), ("params", C.c_void_p),
+                ("material", C.c_int32), ("kernel", C.c_int32), ("cmodel", C.c_int32),
+                ("precision", C.c_int32), ("multi_params", C.c_int32), ("zem_cs", C.c_double),
+                ("maxdmg", C.c_double), ("device", C.c_int32)]
+
+
+class BCDesc(C.Structure):
+    _fields_ = [("field", C.c_int32), ("dim", C.c_int32), ("kind", C.c_int32),
+                ("n_points", C.c_int32), ("points", C.c_void_p), ("data", C.c_void_p)]
+
+
+class NaNError(RuntimeError):
+    """NaN values in the internal force density (the reference's NaNError, errors.jl:98-114)."""
+
+    def __init__(self, time, step):
+        self.time = time
+        self.step = step
+        super().__init__(f"NaN values detected in force density field!\n  time:    {time}\n"
+                         f"  step:    {step}")
+
+
+class PDCudaError(RuntimeError):
+    pass
+
+
+def lib():
+    """Load libpdcuda.so. Fails loudly when it has not been built."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    if not os.path.exists(LIB_PATH):
+        raise PDCudaError(f"libpdcuda.so not built ({LIB_PATH}); run __graft_entry__.build()")
+    L = C.CDLL(LIB_PATH)
+    vp, i64, i32, dbl, st = C.c_void_p, C.c_int64, C.c_int32, C.c_double, C.c_int32
+    L.pd_last_error.restype = C.c_char_p
+    L.pd_version.restype = C.c_char_p
+    sig = {
+        "pd_find_bonds": [i64, vp, vp, vp, i32, vp, vp, i64, vp, vp, vp, vp, vp, i32],
+        "pd_create": [vp, vp],
+        "pd_create_search": [vp, vp, i32, vp, vp, vp],
+        "pd_destroy": [vp],
+        "pd_set_state": [vp, vp, vp, vp, vp, vp, vp, vp],
+        "pd_break_bonds": [vp, vp, vp],
+        "pd_break_random_pairs": [vp, dbl, C.c_uint64],
+        "pd_get_field": [vp, i32, vp, C.c_size_t],
+        "pd_set_bcs": [vp, i32, vp],
+        "pd_set_bc_values": [vp, i64, i64, vp, i64],
+        "pd_stable_timestep": [vp, dbl, vp, vp],
+        "pd_set_param_timesteps": [vp, vp],
+        "pd_force": [vp, dbl, dbl],
+        "pd_run_vv": [vp, i64, i64, dbl],
+        "pd_nan_step": [vp, vp],
+        "pd_run_vv_timed": [vp, i64, i64, dbl, vp, vp, vp, vp],
+        "pd_autotune": [vp, vp, vp],
+        "pd_set_mapping": [vp, i32, i32],
+        "pd_set_graph": [vp, i32],
+        "pd_info": [vp, vp, vp, vp],
+        "pd_launch_count": [vp, vp],
+        "pd_stream": [vp, vp],
+    }
+    for name, args in sig.items():
+        f = getattr(L, name)
+        f.argtypes = args
+        f.restype = st
+    _LIB = L
+    return L
+
+
+def last_error():
+    return lib().pd_last_error().decode()
+
+
+def check(status, what=""):
+    """Map a pd_status to the reference's exception types."""
+    if status == PD_OK:
+        return
+    msg = last_error()
+    if status in (PD_ERR_ARG, PD_ERR_UNSUPPORTED):
+        raise ValueError(f"{what}: {msg}" if what else msg)
+    if status == PD_ERR_NAN:
+        raise NaNError(None, None)
+    raise PDCudaError(f"{what}: {msg} (status {status})" if what else f"{msg} (status {status})")
+
+
+def ptr(a):
+    return None if a is None else a.ctypes.data

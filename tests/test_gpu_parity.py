@@ -1,0 +1,288 @@
+"""Parity of the CUDA path with the FP64 CPU oracle on the same seeded inputs.
+
+FP64 with the serial-order mapping (group 0) must equal the oracle bit for bit (forces,
+failure, damage, trajectories). FP64 with lane groups differs only in summation order.
+The FP32-compensated path is held to the tolerances written in each test.
+"""
+import numpy as np
+import pytest
+
+import oracle as O
+import pdcuda as pd
+from helpers import cube_body, deform, oracle_body, oracle_bcs, plate_body
+
+pytestmark = pytest.mark.gpu
+
+MATERIALS = {
+    "BB": lambda: pd.BBMaterial(),
+    "OSB": lambda: pd.OSBMaterial(),
+    "C-SVK": lambda: pd.CMaterial(),
+    "C-NH": lambda: pd.CMaterial(model=pd.NeoHooke()),
+    "C-NHP": lambda: pd.CMaterial(model=pd.NeoHookePenalty()),
+}
+
+
+def rel_err(a, b):
+    return np.abs(a - b).max() / max(np.abs(b).max(), 1e-300)
+
+
+def jittered_cube(n, seed=1):
+    rng = np.random.default_rng(seed)
+    dx = 1.0 / n
+    pos, vol = pd.uniform_box(1.0, 1.0, 1.0, dx)
+    pos = pos + rng.uniform(-0.05 * dx, 0.05 * dx, pos.shape)
+    return pos, vol, dx
+
+
+def test_bond_search_matches_oracle():
+    pos, vol, dx = jittered_cube(12)
+    X = np.ascontiguousarray(pos.T)
+    delta = np.full(len(vol), 3.015 * dx)
+    off, nbr, L, fp = O.find_bonds(X, delta)
+    body = pd.Body(pd.OSBMaterial(), pos, vol)
+    pd.material(body, horizon=3.015 * dx, rho=1, E=1, nu=0.25, Gc=1)
+    ob = oracle_body(body)
+    dev = pd.DeviceBody(body)
+    assert dev.n_bonds == len(nbr)
+    assert np.array_equal(ob.off, off) and np.array_equal(ob.nbr, nbr) and np.array_equal(ob.L, L)
+
+
+@pytest.mark.parametrize("name", list(MATERIALS))
+def test_force_fp64_serial_order_bit_exact(name):
+    body = cube_body(MATERIALS[name](), n=7)
+    ob = oracle_body(body)
+    dev = pd.DeviceBody(body, precision="fp64")
+    dev.set_mapping(0)
+    u = deform(body._pos)
+    ob.pos[:] = body._pos + u
+    dev.set_state(position=ob.pos)
+    ob.force_density()
+    dev.force()
+    b = dev.field("b_int").T
+    if name in ("C-NH", "C-NHP"):
+        # log / pow of CUDA and of the C library may differ in the last bit
+        assert rel_err(b, ob.b_int) < 1e-13
+    else:
+        assert np.array_equal(b, ob.b_int), rel_err(b, ob.b_int)
+    assert np.array_equal(dev.field("n_active_bonds"), ob.n_active)
+
+
+@pytest.mark.parametrize("name", list(MATERIALS))
+@pytest.mark.parametrize("group", [1, 4, 32])
+def test_force_fp64_lane_groups(name, group):
+    body = cube_body(MATERIALS[name](), n=7)
+    ob = oracle_body(body)
+    dev = pd.DeviceBody(body, precision="fp64")
+    dev.set_mapping(group)
+    ob.pos[:] = body._pos + deform(body._pos)
+    dev.set_state(position=ob.pos)
+    ob.force_density()
+    dev.force()
+    assert rel_err(dev.field("b_int").T, ob.b_int) < 1e-12
+
+
+@pytest.mark.parametrize("name", list(MATERIALS))
+@pytest.mark.parametrize("group", [1, 8, 32])
+def test_force_fp32(name, group):
+    body = cube_body(MATERIALS[name](), n=7)
+    ob = oracle_body(body)
+    dev = pd.DeviceBody(body, precision="fp32")
+    dev.set_mapping(group)
+    u = deform(body._pos)
+    ob.pos[:] = body._pos + u
+    dev.set_state(displacement=u)
+    ob.force_density()
+    dev.force()
+    # FP32 bond arithmetic, compensated sums: relative to the largest force density
+    assert rel_err(dev.field("b_int").T, ob.b_int) < 2e-5
+
+
+@pytest.mark.parametrize("name", ["BB", "OSB", "C-SVK"])
+def test_bonds_break_beyond_critical_stretch(name):
+    # test/materials/test_force_density.jl:86-124
+    pos, vol = pd.uniform_box(1, 1, 1, 1 / 3)
+    mat = MATERIALS[name]()
+    body = pd.Body(mat, pos, vol)
+    kw = dict(horizon=3.015 / 3, rho=7850.0, E=210e9, Gc=1e-6)
+    if name != "BB":
+        kw["nu"] = 0.25
+    pd.material(body, **kw)
+    for prec in ("fp64", "fp32"):
+        dev = pd.DeviceBody(body, precision=prec)
+        x = body._pos.copy()
+        x[0] += 2.0
+        dev.set_state(position=x)
+        dev.force()
+        na = dev.field("n_active_bonds")
+        dmg = dev.field("damage")
+        assert na[0] == 0 and dmg[0] == pytest.approx(1.0)
+        ob = oracle_body(body)
+        nn = np.diff(ob.off)
+        for i in range(1, body.n_points):
+            lost = np.count_nonzero(ob.nbr[ob.off[i]:ob.off[i + 1]] == 0)
+            assert na[i] == nn[i] - lost
+            assert dmg[i] == pytest.approx(lost / nn[i])
+
+
+def run_pair(body, n_steps, prec, mapping=None, graph=0):
+    ob = oracle_body(body)
+    dev = pd.DeviceBody(body, precision=prec)
+    if mapping is not None:
+        dev.set_mapping(mapping)
+    if graph:
+        dev.set_graph(graph)
+    dt = ob.stable_timestep(0.7)
+    assert dev.stable_timestep(0.7) == dt
+    ob.force_density(0.0, dt)
+    dev.force(0.0, dt)
+    assert ob.run_vv(1, n_steps, dt, oracle_bcs(body, 1, n_steps, dt)) == 0
+    dev.run(1, n_steps, dt)
+    return ob, dev
+
+
+@pytest.mark.parametrize("name", ["BB", "OSB", "C-SVK"])
+def test_vv_plate_fp64_bit_exact(name):
+    """Mode-I plate with fracture: FP64 serial order reproduces the oracle trajectory."""
+    mat = MATERIALS[name]()
+    kw = {} if name == "BB" else {"nu": 0.25}
+    body = plate_body(mat, nx=24, ny=12, nz=3, **kw)
+    ob, dev = run_pair(body, 150, "fp64", mapping=0)
+    for f, ref in (("displacement", ob.u), ("velocity", ob.v), ("velocity_half", ob.vh),
+                   ("acceleration", ob.a), ("position", ob.pos)):
+        got = dev.field(f).T
+        if name == "BB" or name == "OSB":
+            assert np.array_equal(got, ref), (f, rel_err(got, ref))
+        else:
+            assert rel_err(got, ref) < 1e-10, f
+    assert np.array_equal(dev.field("bond_active"), ob.bond_active[:ob.n_bonds])
+    assert np.array_equal(dev.field("damage"), ob.damage)
+
+
+@pytest.mark.parametrize("name", ["BB", "OSB", "C-SVK"])
+def test_vv_plate_fp64_groups_and_graph(name):
+    mat = MATERIALS[name]()
+    kw = {} if name == "BB" else {"nu": 0.25}
+    body = plate_body(mat, nx=24, ny=12, nz=3, **kw)
+    ob, dev = run_pair(body, 150, "fp64", mapping=8, graph=25)
+    assert rel_err(dev.field("displacement").T, ob.u) < 1e-10
+    assert np.array_equal(dev.field("bond_active"), ob.bond_active[:ob.n_bonds])
+
+
+@pytest.mark.parametrize("name", ["BB", "OSB", "C-SVK"])
+def test_vv_plate_fp32(name):
+    mat = MATERIALS[name]()
+    kw = {} if name == "BB" else {"nu": 0.25}
+    body = plate_body(mat, nx=24, ny=12, nz=3, **kw)
+    ob, dev = run_pair(body, 150, "fp32", mapping=8)
+    assert rel_err(dev.field("displacement").T, ob.u) < 1e-5
+    assert rel_err(dev.field("velocity").T, ob.v) < 1e-4
+    broken_ref = np.count_nonzero(ob.bond_active[:ob.n_bonds] == 0)
+    broken = np.count_nonzero(dev.field("bond_active") == 0)
+    assert abs(broken - broken_ref) <= max(2, 0.01 * broken_ref)
+
+
+def test_graph_equals_eager():
+    body = plate_body(pd.OSBMaterial(), nx=24, ny=12, nz=3, nu=0.25)
+    res = []
+    for graph in (0, 16):
+        dev = pd.DeviceBody(body, precision="fp32")
+        dev.set_mapping(8)
+        dev.set_graph(graph)
+        dt = dev.stable_timestep(0.7)
+        dev.force(0.0, dt)
+        dev.run(1, 64, dt)
+        dev.run(65, 20, dt)
+        res.append((dev.field("displacement"), dev.field("velocity"), dev.field("bond_active")))
+    for a, b in zip(*res):
+        assert np.array_equal(a, b)
+
+
+def test_boundary_condition_kinds():
+    """f(t) with NaN switch-off, f(p, t), DataBC and b_ext conditions against the oracle."""
+    pos, vol = pd.uniform_box(1.0, 0.5, 0.25, 0.125)
+    body = pd.Body(pd.BBMaterial(), pos, vol)
+    pd.material(body, horizon=3.015 * 0.125, rho=8000.0, E=210e9, Gc=1e3)
+    pd.point_set(body, "left", where=lambda p: p[0] < -0.4)
+    pd.point_set(body, "right", where=lambda p: p[0] > 0.4)
+    pd.point_set(body, "mid", where=lambda p: abs(p[0]) < 0.07)
+    pd.velocity_bc(lambda t: -1.0 if t < 4e-5 else float("nan"), body, "left", "x")
+    pd.velocity_bc(lambda p, t: 100.0 * p[1] * t, body, "right", "y")
+    pd.forcedensity_bc(lambda t: 1e9, body, "mid", "z")
+    data = np.zeros((1, body.n_points))
+    data[0] = np.linspace(0, 0.5, body.n_points)
+    pd.velocity_databc(body, data, "right", ["z"])
+    pd.velocity_ic(body, "mid", "x", 0.25)
+    ob, dev = run_pair(body, 60, "fp64", mapping=0)
+    assert np.array_equal(dev.field("displacement").T, ob.u)
+    assert np.array_equal(dev.field("b_ext").T, ob.b_ext)
+    assert np.array_equal(dev.field("velocity").T, ob.v)
+
+
+def test_multi_parameter_bodies():
+    """Two parameter sets (ParameterHandler semantics) for BB and OSB."""
+    for mat, kw in ((pd.BBMaterial(), {}), (pd.OSBMaterial(), {"nu": 0.25})):
+        pos, vol = pd.uniform_box(1.0, 0.5, 0.25, 0.0625)
+        body = pd.Body(mat, pos, vol)
+        pd.point_set(body, "a", where=lambda p: p[0] < 0)
+        pd.point_set(body, "b", where=lambda p: p[0] >= 0)
+        pd.material(body, "a", horizon=3.015 * 0.0625, rho=8000.0, E=210e9, Gc=1e3, **kw)
+        pd.material(body, "b", horizon=3.015 * 0.0625, rho=2700.0, E=70e9, Gc=1e3, **kw)
+        pd.no_failure(body)
+        pd.velocity_ic(body, "a", "x", -2.0)
+        ob, dev = run_pair(body, 40, "fp64", mapping=0)
+        assert np.array_equal(dev.field("displacement").T, ob.u)
+        ob, dev = run_pair(body, 40, "fp32", mapping=4)
+        assert rel_err(dev.field("displacement").T, ob.u) < 1e-5
+
+
+def test_asymmetric_bond_states_use_reverse_bonds():
+    """A bond state set for one direction only: the reverse-bond path of the gather."""
+    body = cube_body(pd.OSBMaterial(), n=6)
+    ob = oracle_body(body)
+    rng = np.random.default_rng(3)
+    ba = (rng.random(ob.n_bonds) > 0.2).astype(np.uint8)
+    ob.bond_active[:ob.n_bonds] = ba
+    dev = pd.DeviceBody(body, precision="fp64")
+    dev.set_mapping(0)
+    dev.set_state(bond_active=ba)
+    assert dev.info()[2] == 0  # not symmetric
+    ob.pos[:] = body._pos + deform(body._pos)
+    dev.set_state(position=ob.pos)
+    ob.force_density()
+    dev.force()
+    assert np.array_equal(dev.field("b_int").T, ob.b_int)
+    dev32 = pd.DeviceBody(body, precision="fp32")
+    dev32.set_state(bond_active=ba, displacement=ob.pos - body._pos)
+    dev32.force()
+    assert rel_err(dev32.field("b_int").T, ob.b_int) < 2e-5
+
+
+def test_nan_is_detected_with_its_step():
+    body = plate_body(pd.BBMaterial(), nx=12, ny=6, nz=2)
+    dev = pd.DeviceBody(body)
+    dt = dev.stable_timestep(0.7)
+    dev.force(0.0, dt)
+    dev.run(1, 5, dt)
+    u = dev.field("displacement").T.copy()
+    u[3, 0] = np.nan
+    x = dev.field("position").T.copy()
+    x[3, 0] = np.nan
+    dev.set_state(position=x, displacement=u)
+    with pytest.raises(pd.NaNError) as e:
+        dev.run(6, 5, dt)
+    assert e.value.step == 6
+    with pytest.raises(pd.NaNError):
+        dev.force(0.0, dt)
+
+
+def test_autotune_keeps_results():
+    body = cube_body(pd.OSBMaterial(), n=8)
+    dev = pd.DeviceBody(body, precision="fp32")
+    dev.set_state(displacement=deform(body._pos))
+    dev.force()
+    ref = dev.field("b_int")
+    g, b = dev.autotune()
+    assert g in (1, 2, 4, 8, 16, 32) and b in (128, 256)
+    dev.force()
+    assert rel_err(dev.field("b_int"), ref) < 1e-6
+    assert dev.launch_count() > 0

@@ -236,6 +236,11 @@ pd_status pd_autotune(pd_handle *h, int32_t *group_out, int32_t *block_out);
  * to a serial CPU evaluation); block size 64, 128 or 256. */
 pd_status pd_set_mapping(pd_handle *h, int32_t group, int32_t block);
 
+/* How the FP32 force kernels read the bond stream: 0 = direct loads; 1, 2, 3 = chunks of
+ * the sliced bond arrays staged in shared memory by TMA bulk copies (4 rows x 3 stages,
+ * 4 rows x 4 stages, 8 rows x 3 stages per warp). Needs one lane per point and BB or OSB. */
+pd_status pd_set_pipeline(pd_handle *h, int32_t pipe);
+
 /* Enables CUDA-graph capture of blocks of `steps_per_graph` steps (0 disables). */
 pd_status pd_set_graph(pd_handle *h, int32_t steps_per_graph);
 

@@ -36,12 +36,12 @@ static pd_status fail(pd_status code, const std::string& msg) {
   } while (0)
 
 struct GraphKey {
-  int steps = 0, group = 0, block = 0, exact = 0, bcpts = 0;
+  int steps = 0, group = 0, block = 0, exact = 0, bcpts = 0, pipe = 0;
   double dt = 0;
   long long version = -1;
   bool operator==(const GraphKey& o) const {
     return steps == o.steps && group == o.group && block == o.block && exact == o.exact &&
-           bcpts == o.bcpts && dt == o.dt && version == o.version;
+           bcpts == o.bcpts && dt == o.dt && version == o.version && pipe == o.pipe;
   }
 };
 
@@ -60,7 +60,7 @@ struct pd_handle {
   DevParam* dparams = nullptr;
   int* rev = nullptr;
   int* flags = nullptr;
-  LaunchCfg cfg{8, 256, false};
+  LaunchCfg cfg{1, 256, false, 0};
   bool damage_valid = false;
   bool has_bext_state = false;
   // boundary conditions (host side)
@@ -79,6 +79,7 @@ struct pd_handle {
   GraphKey gkey;
   long long launches = 0;
   long long nan_step = -1;
+  long long nslots = 0;
 };
 
 template <class T>
@@ -190,47 +191,76 @@ static pd_status validate_desc(const pd_body_desc* desc, bool need_bonds) {
 }
 
 // symmetric-pair mode of the state-based materials: every bond has a reverse, both directions
-// share one state and one critical stretch. Otherwise the reverse index is kept.
-static pd_status setup_symmetry(pd_handle* h) {
-  if (h->material == PD_MAT_BB || h->nb == 0) { h->d.sym = 1; return PD_OK; }
+// share one state and one critical stretch. Otherwise the kernels read the reverse bond.
+static pd_status check_symmetry(pd_handle* h) {
+  if (h->material == PD_MAT_BB || h->nb == 0 || !h->d.rev) { h->d.sym = 1; return PD_OK; }
   int hf[4] = {0, 0, 0, 0};
-  if (!h->rev) PD_TRY(dalloc(h, &h->rev, h->nb));
   PD_CUDA(cudaMemsetAsync(h->flags, 0, sizeof(int) * 4, h->stream));
-  launch_reverse(h->d, h->rev, h->flags, h->stream);
-  launch_check_sym(h->d, h->rev, h->flags, h->stream);
+  launch_check_sym(h->d, h->flags, h->stream);
   PD_CUDA(cudaMemcpyAsync(hf, h->flags, sizeof(hf), cudaMemcpyDeviceToHost, h->stream));
   PD_CUDA(cudaStreamSynchronize(h->stream));
-  if (hf[0])
-    return fail(PD_ERR_UNSUPPORTED,
-                "bond lists are not symmetric (a bond i->j without j->i): the gather form of the "
-                "state-based materials needs symmetric bond lists (equal horizons)");
   h->d.sym = (hf[1] == 0 && hf[2] == 0) ? 1 : 0;
-  h->d.rev = h->rev;
   return PD_OK;
 }
 
-static pd_status finish_create(pd_handle* h, const pd_body_desc* desc, const double* dL,
-                               const unsigned char* dfp) {
+// CSR bond lists (device) -> sliced layout with one lane per point, bond geometry, reverse
+// positions, all bonds active; then the point state.
+static pd_status finish_create(pd_handle* h, int* dnbr_csr, const double* dL, const unsigned char* dfp) {
   const long long n = h->n, nb = h->nb;
-  // bond geometry
+  int* revk_csr = nullptr;
+  if (h->material != PD_MAT_BB && nb > 0) {
+    int hf = 0;
+    PD_TRY(dalloc(h, &revk_csr, nb));
+    PD_CUDA(cudaMemsetAsync(h->flags, 0, sizeof(int) * 4, h->stream));
+    launch_reverse(n, h->d.off, dnbr_csr, revk_csr, h->flags, h->stream);
+    PD_CUDA(cudaMemcpyAsync(&hf, h->flags, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    PD_CUDA(cudaStreamSynchronize(h->stream));
+    if (hf)
+      return fail(PD_ERR_UNSUPPORTED,
+                  "bond lists are not symmetric (a bond i->j without j->i): the gather form of the "
+                  "state-based materials needs symmetric bond lists (equal horizons)");
+  }
+  long long* soff = nullptr;
+  long long ns = 0, nslots = 0;
+  PD_CUDA(build_slices(n, h->d.off, 1, &soff, &ns, &nslots, h->stream));
+  h->allocs.push_back(soff);
+  h->d.soff = soff;
+  h->d.nslices = ns;
+  h->d.lg = 1;
+  h->nslots = nslots;
+  int* nbr = nullptr;
+  PD_TRY(dalloc(h, &nbr, nslots));
+  PD_CUDA(cudaMemsetAsync(nbr, 0, sizeof(int) * (nslots > 0 ? nslots : 1), h->stream));
+  if (nb) launch_scatter_i32(h->d, dnbr_csr, nbr, h->stream);
+  h->d.nbr = nbr;
+  if (revk_csr) {
+    int* rev = nullptr;
+    PD_TRY(dalloc(h, &rev, nslots));
+    PD_CUDA(cudaMemsetAsync(rev, 0, sizeof(int) * nslots, h->stream));
+    launch_scatter_i32(h->d, revk_csr, rev, h->stream);
+    h->d.rev = rev;
+  }
   if (h->precision == PD_PREC_FP64) {
     double* len = nullptr;
-    PD_TRY(dalloc(h, &len, nb));
+    PD_TRY(dalloc(h, &len, nslots));
+    PD_CUDA(cudaMemsetAsync(len, 0, sizeof(double) * (nslots > 0 ? nslots : 1), h->stream));
+    if (nb) launch_build_len64(h->d, dnbr_csr, dL, dfp, len, h->stream);
     h->d.len64 = len;
-    launch_build_len64(h->d, dL, dfp, len, h->stream);
   } else {
     float4* geo = nullptr;
-    PD_TRY(dalloc(h, &geo, nb));
+    PD_TRY(dalloc(h, &geo, nslots));
+    PD_CUDA(cudaMemsetAsync(geo, 0, sizeof(float4) * (nslots > 0 ? nslots : 1), h->stream));
+    if (nb) launch_build_geo(h->d, dnbr_csr, dL, dfp, geo, h->stream);
     h->d.geo = geo;
-    launch_build_geo(h->d, dL, dfp, geo, h->stream);
   }
-  PD_CUDA(cudaGetLastError());
-  // bond_active: all bonds active
   unsigned* bits = nullptr;
-  const long long nw = (nb + 31) / 32;
-  PD_TRY(dalloc(h, &bits, nw + 1));
-  PD_CUDA(cudaMemsetAsync(bits, 0xff, sizeof(unsigned) * (nw + 1), h->stream));
+  PD_TRY(dalloc(h, &bits, nslots / 32 + 1));
+  PD_CUDA(cudaMemsetAsync(bits, 0, sizeof(unsigned) * (nslots / 32 + 1), h->stream));
   h->d.bits = bits;
+  launch_pack_bits(h->d, nullptr, h->stream);
+  PD_CUDA(cudaGetLastError());
+  PD_CUDA(cudaStreamSynchronize(h->stream));
+  if (revk_csr) dfree(h, revk_csr);
   // point state
   PD_TRY(dalloc(h, &h->d.n_active, n));
   PD_TRY(dalloc(h, &h->g.vh, 3 * n));
@@ -250,27 +280,94 @@ static pd_status finish_create(pd_handle* h, const pd_body_desc* desc, const dou
   } else {
     PD_TRY(dalloc(h, &h->d.b32, 3 * n));
     PD_CUDA(cudaMemsetAsync(h->d.b32, 0, sizeof(float) * 3 * n, h->stream));
+    PD_TRY(dalloc(h, &h->d.uhi, n));
+    PD_TRY(dalloc(h, &h->d.ulo, n));
     h->g.fp32 = 1;
+    launch_split_u(h->d, h->stream);
   }
   if (h->material == PD_MAT_OSB) {
-    if (h->precision == PD_PREC_FP64) PD_TRY(dalloc(h, &h->d.coef64, n));
-    else PD_TRY(dalloc(h, &h->d.coef32, n));
+    if (h->precision == PD_PREC_FP64) {
+      PD_TRY(dalloc(h, &h->d.coef64, n));
+      PD_CUDA(cudaMemsetAsync(h->d.coef64, 0, sizeof(double4) * n, h->stream));
+    } else {
+      PD_TRY(dalloc(h, &h->d.cc32, n));
+      PD_TRY(dalloc(h, &h->d.cm32, n));
+      PD_CUDA(cudaMemsetAsync(h->d.cc32, 0, sizeof(float2) * n, h->stream));
+      PD_CUDA(cudaMemsetAsync(h->d.cm32, 0, sizeof(float2) * n, h->stream));
+    }
   } else if (h->material == PD_MAT_CMAT) {
     if (h->precision == PD_PREC_FP64) {
       PD_TRY(dalloc(h, &h->d.F64, 9 * n));
       PD_TRY(dalloc(h, &h->d.PK64, 9 * n));
       PD_CUDA(cudaMemsetAsync(h->d.F64, 0, sizeof(double) * 9 * n, h->stream));
+      PD_CUDA(cudaMemsetAsync(h->d.PK64, 0, sizeof(double) * 9 * n, h->stream));
     } else {
       PD_TRY(dalloc(h, &h->d.H32, 9 * n));
       PD_TRY(dalloc(h, &h->d.cst32, 3 * n));
       PD_CUDA(cudaMemsetAsync(h->d.H32, 0, sizeof(float) * 9 * n, h->stream));
+      PD_CUDA(cudaMemsetAsync(h->d.cst32, 0, sizeof(float4) * 3 * n, h->stream));
     }
   }
   launch_count_active(h->d, h->stream);
   PD_CUDA(cudaGetLastError());
-  PD_TRY(setup_symmetry(h));
+  PD_TRY(check_symmetry(h));
   PD_CUDA(cudaStreamSynchronize(h->stream));
-  (void)desc;
+  return PD_OK;
+}
+
+// moves every bond array into the layout with G lanes per point
+static pd_status relayout(pd_handle* h, int G) {
+  if (G == h->d.lg) return PD_OK;
+  PD_CUDA(cudaStreamSynchronize(h->stream));
+  DevBody a = h->d, b = h->d;
+  long long* soff = nullptr;
+  long long ns = 0, nslots = 0;
+  PD_CUDA(build_slices(h->n, h->d.off, G, &soff, &ns, &nslots, h->stream));
+  h->allocs.push_back(soff);
+  b.soff = soff;
+  b.nslices = ns;
+  b.lg = G;
+  int* nbr = nullptr;
+  PD_TRY(dalloc(h, &nbr, nslots));
+  PD_CUDA(cudaMemsetAsync(nbr, 0, sizeof(int) * (nslots > 0 ? nslots : 1), h->stream));
+  launch_relayout_i32(a, b, a.nbr, nbr, h->stream);
+  b.nbr = nbr;
+  if (a.rev) {
+    int* rev = nullptr;
+    PD_TRY(dalloc(h, &rev, nslots));
+    PD_CUDA(cudaMemsetAsync(rev, 0, sizeof(int) * (nslots > 0 ? nslots : 1), h->stream));
+    launch_relayout_i32(a, b, a.rev, rev, h->stream);
+    b.rev = rev;
+  }
+  if (a.len64) {
+    double* len = nullptr;
+    PD_TRY(dalloc(h, &len, nslots));
+    PD_CUDA(cudaMemsetAsync(len, 0, sizeof(double) * (nslots > 0 ? nslots : 1), h->stream));
+    launch_relayout_f64(a, b, a.len64, len, h->stream);
+    b.len64 = len;
+  } else {
+    float4* geo = nullptr;
+    PD_TRY(dalloc(h, &geo, nslots));
+    PD_CUDA(cudaMemsetAsync(geo, 0, sizeof(float4) * (nslots > 0 ? nslots : 1), h->stream));
+    launch_relayout_f4(a, b, a.geo, geo, h->stream);
+    b.geo = geo;
+  }
+  unsigned* bits = nullptr;
+  unsigned char* bytes = nullptr;
+  PD_TRY(dalloc(h, &bits, nslots / 32 + 1));
+  PD_CUDA(cudaMemsetAsync(bits, 0, sizeof(unsigned) * (nslots / 32 + 1), h->stream));
+  PD_TRY(dalloc(h, &bytes, h->nb));
+  launch_export_bond_active(a, bytes, 1, h->stream);
+  b.bits = bits;
+  launch_pack_bits(b, bytes, h->stream);
+  PD_CUDA(cudaGetLastError());
+  PD_CUDA(cudaStreamSynchronize(h->stream));
+  dfree(h, bytes);
+  dfree(h, (void*)a.soff); dfree(h, (void*)a.nbr); dfree(h, (void*)a.rev);
+  dfree(h, (void*)a.len64); dfree(h, (void*)a.geo); dfree(h, a.bits);
+  h->d = b;
+  h->nslots = nslots;
+  destroy_graph(h);
   return PD_OK;
 }
 
@@ -324,9 +421,10 @@ static pd_status begin_create(const pd_body_desc* desc, pd_handle** out, pd_hand
   h->d.maxdmg = h->maxdmg;
   h->d.cs = h->cs;
   h->d.sym = 1;
-  h->cfg.group = h->precision == PD_PREC_FP64 ? 1 : 8;
+  h->cfg.group = 1;
   h->cfg.block = 256;
   h->cfg.exact = false;
+  h->cfg.pipe = 0;
   return PD_OK;
 }
 
@@ -353,8 +451,8 @@ extern "C" pd_status pd_create(const pd_body_desc* desc, pd_handle** out) {
   if (e == cudaSuccess && dfp) e = cudaMemcpy(dfp, desc->fail_permit, nb, cudaMemcpyHostToDevice);
   if (e != cudaSuccess) { pd_destroy(h); return fail(PD_ERR_CUDA, cudaGetErrorString(e)); }
   h->d.off = doff;
-  h->d.nbr = dnbr;
-  st = finish_create(h, desc, dL, dfp);
+  st = finish_create(h, dnbr, dL, dfp);
+  dfree(h, dnbr);
   if (dL) dfree(h, dL);
   if (dfp) dfree(h, dfp);
   if (st != PD_OK) { std::string m = g_err; pd_destroy(h); return fail(st, m); }
@@ -504,14 +602,14 @@ extern "C" pd_status pd_create_search(const pd_body_desc* desc, const uint8_t* f
   h->nb = nb;
   h->d.nb = nb;
   h->d.off = doff;
-  h->d.nbr = dnbr;
   double* dL = nullptr;
   st = dalloc(h, &dL, nb);
   if (st == PD_OK) st = dalloc(h, &dfpb, nb);
   if (st != PD_OK) { std::string m = g_err; pd_destroy(h); return fail(st, m); }
   if (nb) launch_bond_props(n, dX, dfp, doff, dnbr, dL, dfpb, h->stream);
-  st = finish_create(h, desc, dL, dfpb);
-  dfree(h, dL); dfree(h, dfpb); dfree(h, dX); dfree(h, dd); dfree(h, dm); dfree(h, dfp);
+  dfree(h, dX); dfree(h, dd); dfree(h, dm); dfree(h, dfp);
+  st = finish_create(h, dnbr, dL, dfpb);
+  dfree(h, dnbr); dfree(h, dL); dfree(h, dfpb);
   if (st != PD_OK) { std::string m = g_err; pd_destroy(h); return fail(st, m); }
   *out = h;
   return PD_OK;
@@ -567,7 +665,11 @@ extern "C" pd_status pd_set_state(pd_handle* h, const double* position, const do
       cur_changed = true;
     }
   }
-  if (cur_changed) PD_CUDA(cudaMemcpy(h->d.cur, cur.data(), sizeof(double4) * n, cudaMemcpyHostToDevice));
+  if (cur_changed) {
+    PD_CUDA(cudaMemcpy(h->d.cur, cur.data(), sizeof(double4) * n, cudaMemcpyHostToDevice));
+    launch_split_u(h->d, h->stream);
+    PD_CUDA(cudaGetLastError());
+  }
   if (velocity) PD_CUDA(cudaMemcpy(h->g.v, velocity, sizeof(double) * 3 * n, cudaMemcpyHostToDevice));
   if (velocity_half) PD_CUDA(cudaMemcpy(h->g.vh, velocity_half, sizeof(double) * 3 * n, cudaMemcpyHostToDevice));
   if (acceleration) PD_CUDA(cudaMemcpy(h->g.a, acceleration, sizeof(double) * 3 * n, cudaMemcpyHostToDevice));
@@ -586,14 +688,14 @@ extern "C" pd_status pd_set_state(pd_handle* h, const double* position, const do
     PD_CUDA(cudaMalloc(&tmp, nb));
     cudaError_t e = cudaMemcpy(tmp, bond_active, nb, cudaMemcpyHostToDevice);
     if (e == cudaSuccess) {
-      launch_pack_bits(tmp, h->d.bits, nb, h->stream);
+      launch_pack_bits(h->d, tmp, h->stream);
       e = cudaStreamSynchronize(h->stream);
     }
     cudaFree(tmp);
     if (e != cudaSuccess) return fail(PD_ERR_CUDA, cudaGetErrorString(e));
     launch_count_active(h->d, h->stream);
     h->damage_valid = true;
-    PD_TRY(setup_symmetry(h));
+    PD_TRY(check_symmetry(h));
     destroy_graph(h);
   }
   PD_TRY(clear_error(h));
@@ -663,7 +765,7 @@ extern "C" pd_status pd_get_field(pd_handle* h, int32_t field, void* out, size_t
     case PD_FIELD_BOND_ACTIVE:
       if (nb == 0) break;
       PD_CUDA(cudaMalloc(&tmp, need));
-      launch_export_bond_active(h->d, (unsigned char*)tmp, h->stream);
+      launch_export_bond_active(h->d, (unsigned char*)tmp, 0, h->stream);
       PD_CUDA(cudaStreamSynchronize(h->stream));
       st = copy(tmp);
       break;
@@ -831,8 +933,10 @@ extern "C" pd_status pd_set_param_timesteps(pd_handle* h, const double* dtp) {
 }
 
 static int launch_force(pd_handle* h, int kstep, int phase) {
-  const int k = h->precision == PD_PREC_FP64 ? launch_force64(h->d, h->cfg, kstep, phase, h->stream)
-                                             : launch_force32(h->d, h->cfg, kstep, phase, h->stream);
+  int k;
+  if (h->precision == PD_PREC_FP64) k = launch_force64(h->d, h->cfg, kstep, phase, h->stream);
+  else if (h->cfg.pipe > 0 && tma_supported(h->d)) k = launch_force32_tma(h->d, h->cfg.pipe, kstep, phase, h->stream);
+  else k = launch_force32(h->d, h->cfg, kstep, phase, h->stream);
   h->launches += k;
   return k;
 }
@@ -845,6 +949,7 @@ static pd_status check_err(pd_handle* h) {
     h->nan_step = c.err_step;
     return fail(PD_ERR_NAN, "NaN values detected in force density field! step: " + std::to_string(c.err_step));
   }
+  if (c.err == 3) return fail(PD_ERR_TIMEOUT, "a bounded wait of a force kernel gave up");
   if (c.err == 2)
     return fail(PD_ERR_ARG, "boundary condition values missing for step " + std::to_string(c.err_step) +
                                 " (call pd_set_bc_values)");
@@ -887,7 +992,7 @@ static void issue_steps(pd_handle* h, int steps, double dto, std::vector<cudaEve
 static pd_status run_block_graph(pd_handle* h, int steps, double dto) {
   GraphKey key;
   key.steps = steps; key.group = h->cfg.group; key.block = h->cfg.block; key.exact = h->cfg.exact;
-  key.bcpts = h->bc.n_points; key.dt = dto; key.version = h->version;
+  key.bcpts = h->bc.n_points; key.dt = dto; key.version = h->version; key.pipe = h->cfg.pipe;
   if (!(h->gexec && key == h->gkey)) {
     destroy_graph(h);
     cudaGraph_t graph;
@@ -991,13 +1096,19 @@ extern "C" pd_status pd_set_mapping(pd_handle* h, int32_t group, int32_t block) 
   if (block != 64 && block != 128 && block != 256) return fail(PD_ERR_ARG, "block must be 64, 128 or 256");
   if (group == 0) {
     if (h->precision != PD_PREC_FP64) return fail(PD_ERR_ARG, "the serial-order mapping (group 0) is FP64 only");
+    PD_CUDA(cudaSetDevice(h->device));
+    PD_TRY(relayout(h, 1));
     h->cfg.exact = true;
     h->cfg.group = 1;
+    h->cfg.pipe = 0;
   } else {
     if (group != 1 && group != 2 && group != 4 && group != 8 && group != 16 && group != 32)
       return fail(PD_ERR_ARG, "group must be 0, 1, 2, 4, 8, 16 or 32");
+    PD_CUDA(cudaSetDevice(h->device));
+    PD_TRY(relayout(h, group));
     h->cfg.exact = false;
     h->cfg.group = group;
+    if (group != 1) h->cfg.pipe = 0;
   }
   h->cfg.block = block;
   destroy_graph(h);
@@ -1013,13 +1124,19 @@ extern "C" pd_status pd_autotune(pd_handle* h, int32_t* group_out, int32_t* bloc
   PD_CUDA(cudaEventCreate(&e1));
   float best = INFINITY;
   LaunchCfg bestc = keep;
-  const int groups[] = {1, 2, 4, 8, 16, 32};
+  const int groups[] = {1, 4, 32};
   const int blocks[] = {128, 256};
   // force evaluations are idempotent at fixed positions: bonds that broke stay broken and
   // every output is recomputed
-  for (int G : groups)
-    for (int B : blocks) {
+  for (int G : groups) {
+    pd_status st = relayout(h, G);
+    if (st == PD_ERR_OOM) { cudaGetLastError(); continue; }  // no room for a second layout
+    if (st != PD_OK) { cudaEventDestroy(e0); cudaEventDestroy(e1); return st; }
+    const bool tma = h->precision == PD_PREC_FP32_KAHAN && G == 1 && tma_supported(h->d);
+    for (int v = 0; v < (tma ? 5 : 2); v++) {
+      const int B = v < 2 ? blocks[v] : 128;
       h->cfg.group = G; h->cfg.block = B; h->cfg.exact = false;
+      h->cfg.pipe = v < 2 ? 0 : v - 1;
       launch_force(h, 0, 0);
       cudaEventRecord(e0, h->stream);
       for (int r = 0; r < 3; r++) launch_force(h, 0, 0);
@@ -1030,8 +1147,10 @@ extern "C" pd_status pd_autotune(pd_handle* h, int32_t* group_out, int32_t* bloc
       cudaEventElapsedTime(&ms, e0, e1);
       if (ms < best) { best = ms; bestc = h->cfg; }
     }
+  }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
+  PD_TRY(relayout(h, bestc.group));
   h->cfg = bestc;
   destroy_graph(h);
   if (group_out) *group_out = bestc.group;
@@ -1099,7 +1218,17 @@ extern "C" pd_status pd_break_random_pairs(pd_handle* h, double fraction, uint64
   launch_count_active(h->d, h->stream);
   PD_CUDA(cudaStreamSynchronize(h->stream));
   h->damage_valid = true;
-  PD_TRY(setup_symmetry(h));
+  PD_TRY(check_symmetry(h));
+  destroy_graph(h);
+  return PD_OK;
+}
+
+extern "C" pd_status pd_set_pipeline(pd_handle* h, int32_t pipe) {
+  if (!h) return fail(PD_ERR_ARG, "handle is NULL");
+  if (pipe < 0 || pipe > 3) return fail(PD_ERR_ARG, "pipe must be 0, 1, 2 or 3");
+  if (pipe > 0 && (h->precision != PD_PREC_FP32_KAHAN || !tma_supported(h->d)))
+    return fail(PD_ERR_ARG, "the staged bond stream needs the FP32 path, one lane per point and BB or OSB");
+  h->cfg.pipe = pipe;
   destroy_graph(h);
   return PD_OK;
 }

@@ -2,20 +2,38 @@
 // force, integration and neighbour-search kernels of libpdcuda.
 //
 // HBM layout of one body (n points, B directed bonds, CSR by point):
-//   off      int64[n+1]   bond range of point i is [off[i], off[i+1])
-//   nbr      int32[B]     neighbour index j
-//   bits     uint32[B/32] bond_active, one bit per bond (bit b&31 of word b>>5)
-//   rev      int32[B]     index of the reverse bond j->i (only for asymmetric bond states)
-//   FP64 path: len64 double[B] reference length L, negative when failure is not permitted
-//   FP32 path: geo  float4[B]  {xi_x, xi_y, xi_z, +-L}: reference bond vector X_j - X_i and
-//              length, the sign of w carrying fail_permit (negative = not permitted)
+//   off      int64[n+1]   n_neighbors of point i is off[i+1] - off[i] (the reference's CSR
+//                         order: bond k of point i is bond off[i] + k of the reference)
+//   Bond arrays are stored in a sliced layout with G lanes per point ("SELL"): the points
+//   are cut into slices of P = 32 / G consecutive points; slice s owns rows
+//   [soff[s] / 32, soff[s+1] / 32) of 32 bond slots; bond k of the point p of the slice sits
+//   in row k / G at lane p * G + k % G. A warp walks one slice row by row, so every
+//   bond-array load of a warp is one contiguous 128-byte (int32) or 512-byte (float4)
+//   segment, and the 32 bond_active bits of a row are one word owned by that warp.
+//   soff     int64[S+1]   slot offset of every slice (multiple of 32)
+//   nbr      int32[slots] neighbour index j (padding slots: 0)
+//   bits     uint32[slots/32] bond_active, bit (slot & 31) of word slot >> 5 (padding: 0)
+//   revk     int32[slots] position k' of i in the bond list of j (only for asymmetric states)
+//   FP64 path: len64 double[slots] reference length L, negative when failure is not permitted
+//   FP32 path: geo  float4[slots]  {xi_x, xi_y, xi_z, +-L}: reference bond vector X_j - X_i
+//              and length, the sign of w carrying fail_permit (negative = not permitted)
 //   X0       double4[n]   {X, Y, Z, V}: reference position and volume
 //   cur      double4[n]   FP64 path: {x, y, z, V} current position (kept incrementally as the
 //                         reference does); FP32 path: {u_x, u_y, u_z, V} displacement
+//   FP32 path, gathered by the bond loops: uhi float4[n] {(float)u, V} and ulo float4[n]
+//                         {(float)(u - hi), 0}: u_j - u_i = (hi_j - hi_i) + (lo_j - lo_i) in
+//                         FP32 carries the FP64 difference to FP32 precision
 //   meta     uint32[n]    parameter-set id (bits 0-15) and point flags
 #pragma once
 #include <cstdint>
 #include <cuda_runtime.h>
+
+// occupancy bound of the force kernels: blocks of up to 256 threads, at least PD_MINB resident
+// blocks of 256 threads per SM (limits the registers per thread)
+#ifndef PD_MINB
+#define PD_MINB 1
+#endif
+#define PD_LB __launch_bounds__(256, PD_MINB)
 
 namespace pd {
 
@@ -49,9 +67,12 @@ struct Ctrl {
 struct DevBody {
   long long n, nb;
   const long long* off;
+  const long long* soff;
+  long long nslices;
+  int lg;            // lanes per point of the bond layout
   const int* nbr;
   unsigned int* bits;
-  const int* rev;
+  const int* rev;    // revk
   const double* len64;
   const float4* geo;
   const double4* X0;
@@ -62,7 +83,10 @@ struct DevBody {
   double* b64;
   float* b32;
   double4* coef64;   // OSB FP64: {c1, c2, wvol, dil}
-  float4* coef32;    // OSB FP32: {c1, c2, wvol, dil}
+  float2* cc32;      // OSB FP32: {c1, c2}
+  float2* cm32;      // OSB FP32: {wvol, dil}
+  float4* uhi;       // FP32 path: {(float)u, V}
+  float4* ulo;       // FP32 path: {(float)(u - hi), 0}
   double* F64;       // CMat FP64: deformation gradient F (9 per point, column-major)
   double* PK64;      // CMat FP64: P K^-1 (9 per point)
   float* H32;        // CMat FP32: displacement gradient H = F - I (9 per point)
@@ -94,6 +118,19 @@ __device__ __forceinline__ float omega_of_f(int kernel, float delta, float L) {
   return 0.0f;
 }
 
+// slot of bond k of point i in the sliced layout
+__device__ __forceinline__ long long bond_slot(const DevBody& d, long long i, int k) {
+  const int G = d.lg, P = 32 / G;
+  const long long s = i / P;
+  const int p = (int)(i - s * P);
+  return d.soff[s] + (long long)(k / G) * 32 + p * G + (k % G);
+}
+
+// slot of the reverse bond j -> i of the bond in slot b (asymmetric bond states)
+__device__ __forceinline__ long long rev_slot(const DevBody& d, long long b, int j) {
+  return bond_slot(d, j, __ldg(d.rev + b));
+}
+
 __device__ __forceinline__ bool bond_bit(const unsigned int* bits, long long b) {
   return (__ldg(bits + (b >> 5)) >> (b & 31)) & 1u;
 }
@@ -107,32 +144,54 @@ __device__ __forceinline__ void clear_bit(unsigned int* bits, long long b) {
   atomicAnd(bits + (b >> 5), ~(1u << (b & 31)));
 }
 
+// Warp-uniform loop over the slices of the bond layout: one warp per slice; all lanes of a
+// warp walk the same rows, so ballots and group shuffles always see the full warp.
+#define PD_SLICE_LOOP(G)                                                                    \
+  constexpr int PPW = 32 / (G);                                                             \
+  const int lane = threadIdx.x & 31;                                                        \
+  const int sub = lane / (G), gl = lane % (G);                                              \
+  (void)sub; (void)gl;                                                                      \
+  const long long warp0 = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;          \
+  const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;                        \
+  for (long long s = warp0; s < d.nslices; s += nwarps)
+
+// point, slice rows and bond count of the lane
+#define PD_SLICE_SETUP                                                                      \
+  const long long i = s * PPW + sub;                                                        \
+  const bool valid = i < d.n;                                                               \
+  const long long sbase = d.soff[s];                                                        \
+  const int rows = (int)((d.soff[s + 1] - sbase) >> 5);                                     \
+  const int cnt = valid ? (int)(d.off[i + 1] - d.off[i]) : 0;
+
 // ---------------------------------------------------------------------------------------
 // compensated (Kahan-Babuska / Neumaier) FP32 accumulation and its lane-group reduction
 // ---------------------------------------------------------------------------------------
 struct KSum {
   float s, c;
   __device__ __forceinline__ KSum() : s(0.f), c(0.f) {}
+  // Kahan: c carries the low-order part lost by the previous additions
   __device__ __forceinline__ void add(float x) {
-    float t = s + x;
-    // Neumaier: the rounding error of s + x, whichever operand is larger
-    c += (fabsf(s) >= fabsf(x)) ? ((s - t) + x) : ((x - t) + s);
+    const float y = x - c;
+    const float t = s + y;
+    c = (t - s) - y;
     s = t;
   }
-  __device__ __forceinline__ float value() const { return s + c; }
+  __device__ __forceinline__ float value() const { return s - c; }
 };
 
-// lanes [g*G, g*G+G) of a warp form one group; fixed butterfly order => deterministic
+// lanes [g*G, g*G+G) of a warp form one group; fixed butterfly order => deterministic.
+// Partner sums are combined with TwoSum, their compensations added.
 template <int G>
 __device__ __forceinline__ void group_reduce(KSum& k) {
 #pragma unroll
   for (int o = G / 2; o > 0; o >>= 1) {
-    float s2 = __shfl_down_sync(0xffffffffu, k.s, o, G);
-    float c2 = __shfl_down_sync(0xffffffffu, k.c, o, G);
-    float t = k.s + s2;
-    float e = (fabsf(k.s) >= fabsf(s2)) ? ((k.s - t) + s2) : ((s2 - t) + k.s);
+    const float s2 = __shfl_down_sync(0xffffffffu, k.s, o, G);
+    const float c2 = __shfl_down_sync(0xffffffffu, k.c, o, G);
+    const float t = k.s + s2;
+    const float z = t - k.s;
+    const float e = (k.s - (t - z)) + (s2 - z);
     k.s = t;
-    k.c = (k.c + c2) + e;
+    k.c = (k.c + c2) - e;
   }
 }
 

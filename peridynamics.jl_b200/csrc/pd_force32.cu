@@ -29,25 +29,37 @@ __device__ __forceinline__ double4 ld4(const double4* p) {
 }
 
 struct BondF {
-  float gx, gy, gz, L;
+  float gx, gy, gz, L, rL;
   float dux, duy, duz;
-  float ex, ey, ez, l, e;
+  float ex, ey, ez, l, rl, e, eps;
   bool fp;
 };
 
-__device__ __forceinline__ void bond32(const float4 g, const double4& ui, const double4& uj,
-                                       BondF& B) {
+// One bond in FP32: the cancellation-free extension e = l - L, the stretch, and the inverse
+// lengths (reciprocal and reciprocal square root; the FP32 path is not bit-matched).
+__device__ __forceinline__ void bond32(const float4 g, const float4& hi, const float4& lo,
+                                       const float4& hj, const float4& lj, BondF& B) {
   B.gx = g.x; B.gy = g.y; B.gz = g.z;
   B.L = fabsf(g.w);
+  B.rL = __fdividef(1.f, B.L);
   B.fp = g.w > 0.f;
-  B.dux = (float)(uj.x - ui.x);
-  B.duy = (float)(uj.y - ui.y);
-  B.duz = (float)(uj.z - ui.z);
+  B.dux = (hj.x - hi.x) + (lj.x - lo.x);
+  B.duy = (hj.y - hi.y) + (lj.y - lo.y);
+  B.duz = (hj.z - hi.z) + (lj.z - lo.z);
   B.ex = g.x + B.dux; B.ey = g.y + B.duy; B.ez = g.z + B.duz;
-  B.l = sqrtf(B.ex * B.ex + B.ey * B.ey + B.ez * B.ez);
+  const float l2 = B.ex * B.ex + B.ey * B.ey + B.ez * B.ez;
+  B.rl = rsqrtf(l2);
+  B.l = l2 * B.rl;
   const float xd = g.x * B.dux + g.y * B.duy + g.z * B.duz;
   const float dd = B.dux * B.dux + B.duy * B.duy + B.duz * B.duz;
-  B.e = (2.f * xd + dd) / (B.l + B.L);
+  B.e = __fdividef(2.f * xd + dd, B.l + B.L);
+  B.eps = B.e * B.rL;
+}
+
+// influence function with the reciprocal length at hand
+__device__ __forceinline__ float omega_r(int kernel, float delta, float L, float rL) {
+  if (kernel == KER_LINEAR) return delta * rL;
+  return omega_of_f(kernel, delta, L);
 }
 
 __device__ __forceinline__ void flag_nan32(const DevBody& d, int kstep, float x, float y, float z) {
@@ -58,56 +70,54 @@ __device__ __forceinline__ void flag_nan32(const DevBody& d, int kstep, float x,
   }
 }
 
-#define PD_POINT_LOOP(G)                                                                     \
-  constexpr int PPW = 32 / (G);                                                              \
-  const int lane = threadIdx.x & 31;                                                         \
-  const int sub = lane / (G), gl = lane % (G);                                               \
-  const long long warp0 = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;           \
-  const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;                         \
-  for (long long w = warp0; w * PPW < d.n; w += nwarps)
-
 // failure test of CriticalStretch (bond_system.jl:309-327): eps > eps_c with permission
-__device__ __forceinline__ bool fail_test32(const DevBody& d, long long b, const BondF& B,
-                                            float epsc) {
-  bool act = bond_bit_live(d.bits, b);
-  if (act && B.e / B.L > epsc && B.fp) {
-    clear_bit(d.bits, b);
-    act = false;
-  }
-  return act;
+__device__ __forceinline__ bool fails32(const BondF& B, float epsc) {
+  return B.eps > epsc && B.fp;
+}
+
+// new bond_active word of a row after the failure tests of its lanes; the warp owns the word
+__device__ __forceinline__ void commit_row(unsigned int* bits, long long word_idx, unsigned old,
+                                           bool act, int lane) {
+  const unsigned nw = __ballot_sync(0xffffffffu, act);
+  if (lane == 0 && nw != old) bits[word_idx] = nw;
 }
 
 // -------------------------------------------------------------------------------------------
 // BB (bond_based.jl:125-180): one sweep, failure then the pairwise force
 // -------------------------------------------------------------------------------------------
 template <int G, bool MULTI>
-__global__ void __launch_bounds__(256) k_bb32(DevBody d, int kstep) {
+__global__ void PD_LB k_bb32(DevBody d, int kstep) {
   if (d.ctrl->err) return;
-  PD_POINT_LOOP(G) {
-    const long long i = w * PPW + sub;
-    const bool valid = i < d.n;
+  PD_SLICE_LOOP(G) {
+    PD_SLICE_SETUP
     KSum bx, by, bz;
     int na = 0;
-    if (valid) {
-      const double4 ui = ld4(d.cur + i);
-      const DevParam& P = d.params[d.meta[i] & META_PID_MASK];
-      const float epsc = P.epscf, bci = P.bcf;
-      const long long b0 = d.off[i], b1 = d.off[i + 1];
-      for (long long b = b0 + gl; b < b1; b += G) {
+    const float4 hi = valid ? d.uhi[i] : make_float4(0.f, 0.f, 0.f, 0.f);
+    const float4 lo = valid ? d.ulo[i] : make_float4(0.f, 0.f, 0.f, 0.f);
+    const DevParam& P = d.params[valid ? (d.meta[i] & META_PID_MASK) : 0];
+    const float epsc = P.epscf, bci = P.bcf;
+    for (int r = 0; r < rows; r++) {
+      const long long wi = (sbase >> 5) + r;
+      const unsigned word = d.bits[wi];
+      const int k = r * G + gl;
+      bool act = false;
+      if (k < cnt) {
+        const long long b = sbase + (long long)r * 32 + lane;
         const int j = __ldg(d.nbr + b);
         const float4 g = __ldg(d.geo + b);
-        const double4 uj = ld4(d.cur + j);
+        const float4 hj = __ldg(d.uhi + j), lj = __ldg(d.ulo + j);
         BondF B;
-        bond32(g, ui, uj, B);
-        const bool act = fail_test32(d, b, B, epsc);
-        na += act;
+        bond32(g, hi, lo, hj, lj, B);
+        act = ((word >> lane) & 1u) && !fails32(B, epsc);
         if (act) {
           float bc = bci;
           if (MULTI) bc = 0.5f * (bci + d.params[d.meta[j] & META_PID_MASK].bcf);
-          const float s = bc * (B.e / B.L) * (float)uj.w / B.l;
-          bx.add(s * B.ex); by.add(s * B.ey); bz.add(s * B.ez);
+          const float sc = bc * B.eps * hj.w * B.rl;
+          bx.add(sc * B.ex); by.add(sc * B.ey); bz.add(sc * B.ez);
         }
       }
+      na += act;
+      commit_row(d.bits, wi, word, act, lane);
     }
     if (G > 1) { group_reduce<G>(bx); group_reduce<G>(by); group_reduce<G>(bz); na = group_sum<G>(na); }
     if (valid && gl == 0) {
@@ -124,32 +134,45 @@ __global__ void __launch_bounds__(256) k_bb32(DevBody d, int kstep) {
 // dilatation theta, and c1 = 15 G / m, c2 = theta (3 K / m - c1 / 3) (:135-136)
 // -------------------------------------------------------------------------------------------
 template <int G>
-__global__ void __launch_bounds__(256) k_osb_a32(DevBody d, int kstep) {
+__global__ void PD_LB k_osb_a32(DevBody d, int kstep) {
   if (d.ctrl->err) return;
-  PD_POINT_LOOP(G) {
-    const long long i = w * PPW + sub;
-    const bool valid = i < d.n;
+  PD_SLICE_LOOP(G) {
+    PD_SLICE_SETUP
     KSum m, th;
     int na = 0;
     const DevParam& P = d.params[valid ? (d.meta[i] & META_PID_MASK) : 0];
-    if (valid) {
-      const double4 ui = ld4(d.cur + i);
-      const float epsc = P.epscf, delta = P.deltaf;
-      const long long b0 = d.off[i], b1 = d.off[i + 1];
-      for (long long b = b0 + gl; b < b1; b += G) {
-        const int j = __ldg(d.nbr + b);
-        const float4 g = __ldg(d.geo + b);
-        const double4 uj = ld4(d.cur + j);
+    const float4 hi = valid ? d.uhi[i] : make_float4(0.f, 0.f, 0.f, 0.f);
+    const float4 lo = valid ? d.ulo[i] : make_float4(0.f, 0.f, 0.f, 0.f);
+    const float epsc = P.epscf, delta = P.deltaf;
+    const long long b0 = sbase + lane;
+    int jn = 0;
+    float4 gn = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (rows > 0 && gl < cnt) { jn = __ldg(d.nbr + b0); gn = __ldg(d.geo + b0); }
+    for (int r = 0; r < rows; r++) {
+      const long long wi = (sbase >> 5) + r;
+      const unsigned word = d.bits[wi];
+      const int k = r * G + gl;
+      const int j = jn;
+      const float4 g = gn;
+      if (r + 1 < rows && k + G < cnt) {
+        const long long b1 = b0 + (long long)(r + 1) * 32;
+        jn = __ldg(d.nbr + b1);
+        gn = __ldg(d.geo + b1);
+      }
+      bool act = false;
+      if (k < cnt) {
+        const float4 hj = __ldg(d.uhi + j), lj = __ldg(d.ulo + j);
         BondF B;
-        bond32(g, ui, uj, B);
-        const bool act = fail_test32(d, b, B, epsc);
-        na += act;
+        bond32(g, hi, lo, hj, lj, B);
+        act = ((word >> lane) & 1u) && !fails32(B, epsc);
         if (act) {
-          const float om = omega_of_f(d.kernel, delta, B.L) * (float)uj.w;
+          const float om = omega_r(d.kernel, delta, B.L, B.rL) * hj.w;
           m.add(om * (B.gx * B.gx + B.gy * B.gy + B.gz * B.gz));
           th.add(om * B.L * B.e);
         }
       }
+      na += act;
+      commit_row(d.bits, wi, word, act, lane);
     }
     if (G > 1) { group_reduce<G>(m); group_reduce<G>(th); na = group_sum<G>(na); }
     if (valid && gl == 0) {
@@ -160,20 +183,23 @@ __global__ void __launch_bounds__(256) k_osb_a32(DevBody d, int kstep) {
         c1 = 15.f * P.Gf / wv;
         c2 = dil * (3.f * P.Kf / wv - c1 / 3.f);
       }
-      d.coef32[i] = make_float4(c1, c2, wv, dil);
+      d.cc32[i] = make_float2(c1, c2);
+      d.cm32[i] = make_float2(wv, dil);
       d.n_active[i] = na;
     }
   }
 }
 
+// s = omega (c2 L + c1 e) of the bond owner o with partner q; with ParameterHandler
+// semantics (ordinary_state_based.jl:165-166) c1, c2 come from (wvol, dil) and both moduli
 template <bool MULTI>
-__device__ __forceinline__ float osb_s32(const float4& co, const DevParam& Po, const DevParam& Pq,
-                                         float om, float L, float e) {
-  float c1 = co.x, c2 = co.y;
+__device__ __forceinline__ float osb_s32(const float2& c, const float2& m, const DevParam& Po,
+                                         const DevParam& Pq, float om, float L, float e) {
+  float c1 = c.x, c2 = c.y;
   if (MULTI) {
-    if (co.z == 0.f) return 0.f;
-    c1 = 15.f * (Po.Gf + Pq.Gf) / (2.f * co.z);
-    c2 = co.w * (3.f * (Po.Kf + Pq.Kf) / (2.f * co.z) - c1 / 3.f);
+    if (m.x == 0.f) return 0.f;
+    c1 = 15.f * (Po.Gf + Pq.Gf) / (2.f * m.x);
+    c2 = m.y * (3.f * (Po.Kf + Pq.Kf) / (2.f * m.x) - c1 / 3.f);
   }
   return om * (c2 * L + c1 * e);
 }
@@ -182,37 +208,57 @@ __device__ __forceinline__ float osb_s32(const float4& co, const DevParam& Po, c
 // OSB phase B (ordinary_state_based.jl:128-174): b_i = sum_j (s_ij + s_ji) V_j eta / l
 // -------------------------------------------------------------------------------------------
 template <int G, bool MULTI>
-__global__ void __launch_bounds__(256) k_osb_b32(DevBody d, int kstep) {
+__global__ void PD_LB k_osb_b32(DevBody d, int kstep) {
   if (d.ctrl->err) return;
-  PD_POINT_LOOP(G) {
-    const long long i = w * PPW + sub;
-    const bool valid = i < d.n;
+  PD_SLICE_LOOP(G) {
+    PD_SLICE_SETUP
     KSum bx, by, bz;
-    if (valid) {
-      const double4 ui = ld4(d.cur + i);
-      const DevParam& Pi = d.params[d.meta[i] & META_PID_MASK];
-      const float4 ci = d.coef32[i];
-      const long long b0 = d.off[i], b1 = d.off[i + 1];
-      for (long long b = b0 + gl; b < b1; b += G) {
-        const int j = __ldg(d.nbr + b);
-        const float4 g = __ldg(d.geo + b);
-        const double4 uj = ld4(d.cur + j);
-        const float4 cj = __ldg(d.coef32 + j);
-        BondF B;
-        bond32(g, ui, uj, B);
-        const bool ai = bond_bit(d.bits, b);
-        const bool aj = d.sym ? ai : bond_bit(d.bits, __ldg(d.rev + b));
-        if (!(ai || aj)) continue;
-        float oi, oj;
-        const DevParam* Pj = &Pi;
-        if (MULTI) Pj = &d.params[d.meta[j] & META_PID_MASK];
-        oi = ai ? omega_of_f(d.kernel, Pi.deltaf, B.L) : 0.f;
-        oj = aj ? (MULTI ? omega_of_f(d.kernel, Pj->deltaf, B.L) : omega_of_f(d.kernel, Pi.deltaf, B.L)) : 0.f;
-        const float si = osb_s32<MULTI>(ci, Pi, *Pj, oi, B.L, B.e);
-        const float sj = osb_s32<MULTI>(cj, *Pj, Pi, oj, B.L, B.e);
-        const float f = (si + sj) * (float)uj.w / B.l;
-        bx.add(f * B.ex); by.add(f * B.ey); bz.add(f * B.ez);
+    const float4 hi = valid ? d.uhi[i] : make_float4(0.f, 0.f, 0.f, 0.f);
+    const float4 lo = valid ? d.ulo[i] : make_float4(0.f, 0.f, 0.f, 0.f);
+    const DevParam& Pi = d.params[valid ? (d.meta[i] & META_PID_MASK) : 0];
+    const float2 ci = valid ? d.cc32[i] : make_float2(0.f, 0.f);
+    const float2 mi = (MULTI && valid) ? d.cm32[i] : make_float2(0.f, 0.f);
+    // the bond stream of row r + 1 is loaded while row r is processed
+    const unsigned* wrow = d.bits + (sbase >> 5);
+    const long long b0 = sbase + lane;
+    int jn = 0;
+    float4 gn = make_float4(0.f, 0.f, 0.f, 0.f);
+    unsigned wn = 0;
+    if (rows > 0) {
+      wn = __ldg(wrow);
+      if (gl < cnt) { jn = __ldg(d.nbr + b0); gn = __ldg(d.geo + b0); }
+    }
+    for (int r = 0; r < rows; r++) {
+      const int j = jn;
+      const float4 g = gn;
+      const unsigned word = wn;
+      const int k = r * G + gl;
+      if (r + 1 < rows) {
+        wn = __ldg(wrow + r + 1);
+        if (k + G < cnt) {
+          const long long b1 = b0 + (long long)(r + 1) * 32;
+          jn = __ldg(d.nbr + b1);
+          gn = __ldg(d.geo + b1);
+        }
       }
+      if (k >= cnt) continue;
+      const long long b = b0 + (long long)r * 32;
+      const bool ai = (word >> lane) & 1u;
+      const bool aj = d.sym ? ai : bond_bit(d.bits, rev_slot(d, b, j));
+      if (!(ai || aj)) continue;
+      const float4 hj = __ldg(d.uhi + j), lj = __ldg(d.ulo + j);
+      const float2 cj = __ldg(d.cc32 + j);
+      const float2 mj = MULTI ? __ldg(d.cm32 + j) : make_float2(0.f, 0.f);
+      BondF B;
+      bond32(g, hi, lo, hj, lj, B);
+      const DevParam* Pj = &Pi;
+      if (MULTI) Pj = &d.params[d.meta[j] & META_PID_MASK];
+      const float oi = ai ? omega_r(d.kernel, Pi.deltaf, B.L, B.rL) : 0.f;
+      const float oj = aj ? omega_r(d.kernel, Pj->deltaf, B.L, B.rL) : 0.f;
+      const float si = osb_s32<MULTI>(ci, mi, Pi, *Pj, oi, B.L, B.e);
+      const float sj = osb_s32<MULTI>(cj, mj, *Pj, Pi, oj, B.L, B.e);
+      const float f = (si + sj) * hj.w * B.rl;
+      bx.add(f * B.ex); by.add(f * B.ey); bz.add(f * B.ez);
     }
     if (G > 1) { group_reduce<G>(bx); group_reduce<G>(by); group_reduce<G>(bz); }
     if (valid && gl == 0) {
@@ -299,31 +345,32 @@ __device__ void pk1_32(int cmodel, const DevParam& p, const float* H, float* P) 
 // CMat phase A (correspondence.jl:193-224, 288-298; bond_system.jl:309-327)
 // -------------------------------------------------------------------------------------------
 template <int G>
-__global__ void __launch_bounds__(256) k_c_a32(DevBody d, int kstep) {
+__global__ void PD_LB k_c_a32(DevBody d, int kstep) {
   if (d.ctrl->err) return;
-  PD_POINT_LOOP(G) {
-    const long long i = w * PPW + sub;
-    const bool valid = i < d.n;
+  PD_SLICE_LOOP(G) {
+    PD_SLICE_SETUP
     KSum K[6], Hs[9];
     int na = 0;
-    unsigned meta = 0;
-    long long b0 = 0, b1 = 0;
-    const DevParam& P = d.params[valid ? (d.meta[i] & META_PID_MASK) : 0];
-    if (valid) {
-      meta = d.meta[i];
-      const double4 ui = ld4(d.cur + i);
-      const float epsc = P.epscf, id = P.inv_delta, vs = P.vscale;
-      b0 = d.off[i]; b1 = d.off[i + 1];
-      for (long long b = b0 + gl; b < b1; b += G) {
+    const unsigned meta = valid ? d.meta[i] : 0u;
+    const DevParam& P = d.params[meta & META_PID_MASK];
+    const float4 hi = valid ? d.uhi[i] : make_float4(0.f, 0.f, 0.f, 0.f);
+    const float4 lo = valid ? d.ulo[i] : make_float4(0.f, 0.f, 0.f, 0.f);
+    const float epsc = P.epscf, id = P.inv_delta, vs = P.vscale;
+    for (int r = 0; r < rows; r++) {
+      const long long wi = (sbase >> 5) + r;
+      const unsigned word = d.bits[wi];
+      const int k = r * G + gl;
+      bool act = false;
+      if (k < cnt) {
+        const long long b = sbase + (long long)r * 32 + lane;
         const int j = __ldg(d.nbr + b);
         const float4 g = __ldg(d.geo + b);
-        const double4 uj = ld4(d.cur + j);
+        const float4 hj = __ldg(d.uhi + j), lj = __ldg(d.ulo + j);
         BondF B;
-        bond32(g, ui, uj, B);
-        const bool act = fail_test32(d, b, B, epsc);
-        na += act;
+        bond32(g, hi, lo, hj, lj, B);
+        act = ((word >> lane) & 1u) && !fails32(B, epsc);
         if (act) {
-          const float t = omega_of_f(d.kernel, P.deltaf, B.L) * (float)uj.w * vs;
+          const float t = omega_r(d.kernel, P.deltaf, B.L, B.rL) * hj.w * vs;
           const float X[3] = {B.gx * id, B.gy * id, B.gz * id};
           const float U[3] = {B.dux * id, B.duy * id, B.duz * id};
           K[0].add(t * X[0] * X[0]); K[1].add(t * X[1] * X[1]); K[2].add(t * X[2] * X[2]);
@@ -331,15 +378,17 @@ __global__ void __launch_bounds__(256) k_c_a32(DevBody d, int kstep) {
 #pragma unroll
           for (int c = 0; c < 3; c++)
 #pragma unroll
-            for (int r = 0; r < 3; r++) Hs[r + 3 * c].add(t * U[r] * X[c]);
+            for (int q = 0; q < 3; q++) Hs[q + 3 * c].add(t * U[q] * X[c]);
         }
       }
+      na += act;
+      commit_row(d.bits, wi, word, act, lane);
     }
     if (G > 1) {
 #pragma unroll
-      for (int k = 0; k < 6; k++) group_reduce<G>(K[k]);
+      for (int q = 0; q < 6; q++) group_reduce<G>(K[q]);
 #pragma unroll
-      for (int k = 0; k < 9; k++) group_reduce<G>(Hs[k]);
+      for (int q = 0; q < 9; q++) group_reduce<G>(Hs[q]);
       na = group_sum<G>(na);
     }
     bool killed = false;
@@ -349,11 +398,11 @@ __global__ void __launch_bounds__(256) k_c_a32(DevBody d, int kstep) {
                            K[4].value(), K[5].value(), K[2].value()};
       float Kinv[9], Hm[9], H[9];
       finv3(Km, Kinv);
-      for (int k = 0; k < 9; k++) Hm[k] = Hs[k].value();
+      for (int q = 0; q < 9; q++) Hm[q] = Hs[q].value();
       fmatmul(Hm, Kinv, H);
       bool hasnan = false;
-      for (int k = 0; k < 9; k++) { d.H32[9 * i + k] = H[k]; hasnan |= isnan(H[k]); }
-      const double damage = 1.0 - (double)na / (double)(b1 - b0);
+      for (int q = 0; q < 9; q++) { d.H32[9 * i + q] = H[q]; hasnan |= isnan(H[q]); }
+      const double damage = 1.0 - (double)na / (double)cnt;
       killed = (meta & META_KILLED) || damage > d.maxdmg || hasnan;
       float4* cs = d.cst32 + 3 * i;
       if (killed) {
@@ -366,8 +415,8 @@ __global__ void __launch_bounds__(256) k_c_a32(DevBody d, int kstep) {
         float Pm[9], PK[9], A[9];
         pk1_32(d.cmodel, P, H, Pm);
         fmatmul(Pm, Kinv, PK);
-        const float id = P.inv_delta, id5 = id * id * id * id * id;
-        for (int k = 0; k < 9; k++) A[k] = PK[k] * id5 - P.betaf * H[k];
+        const float id5 = id * id * id * id * id;
+        for (int q = 0; q < 9; q++) A[q] = PK[q] * id5 - P.betaf * H[q];
         cs[0] = make_float4(A[0], A[1], A[2], A[3]);
         cs[1] = make_float4(A[4], A[5], A[6], A[7]);
         cs[2] = make_float4(A[8], P.betaf, 0.f, 0.f);
@@ -375,9 +424,11 @@ __global__ void __launch_bounds__(256) k_c_a32(DevBody d, int kstep) {
       d.n_active[i] = na;
     }
     if (!d.sym) {
+      // directed bond states: a killed point loses all its bonds (correspondence.jl:293)
       if (G > 1) killed = group_bcast<G>(killed);
-      if (valid && killed)
-        for (long long b = b0 + gl; b < b1; b += G) clear_bit(d.bits, b);
+      const unsigned kill_mask = __ballot_sync(0xffffffffu, valid && killed);
+      if (kill_mask && lane == 0)
+        for (int r = 0; r < rows; r++) d.bits[(sbase >> 5) + r] &= ~kill_mask;
     }
   }
 }
@@ -387,49 +438,55 @@ __global__ void __launch_bounds__(256) k_c_a32(DevBody d, int kstep) {
 //   t_ij = w (A_i xi + beta_i du), and j's term -t_ji = w (A_j xi + beta_j du)
 // -------------------------------------------------------------------------------------------
 template <int G>
-__global__ void __launch_bounds__(256) k_c_b32(DevBody d, int kstep) {
+__global__ void PD_LB k_c_b32(DevBody d, int kstep) {
   if (d.ctrl->err) return;
-  PD_POINT_LOOP(G) {
-    const long long i = w * PPW + sub;
-    const bool valid = i < d.n;
+  PD_SLICE_LOOP(G) {
+    PD_SLICE_SETUP
     KSum bx, by, bz;
+    const float4 hi = valid ? d.uhi[i] : make_float4(0.f, 0.f, 0.f, 0.f);
+    const float4 lo = valid ? d.ulo[i] : make_float4(0.f, 0.f, 0.f, 0.f);
+    const DevParam& Pi = d.params[valid ? (d.meta[i] & META_PID_MASK) : 0];
+    float Ai[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, bi = 0.f;
     if (valid) {
-      const double4 ui = ld4(d.cur + i);
-      const DevParam& Pi = d.params[d.meta[i] & META_PID_MASK];
       const float4 a0 = d.cst32[3 * i], a1 = d.cst32[3 * i + 1], a2 = d.cst32[3 * i + 2];
-      const float Ai[9] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w, a2.x};
-      const float bi = a2.y;
-      const long long b0 = d.off[i], b1 = d.off[i + 1];
-      for (long long b = b0 + gl; b < b1; b += G) {
-        const int j = __ldg(d.nbr + b);
-        const float4 g = __ldg(d.geo + b);
-        const double4 uj = ld4(d.cur + j);
-        const bool ai = bond_bit(d.bits, b);
-        const bool aj = d.sym ? ai : bond_bit(d.bits, __ldg(d.rev + b));
-        if (!(ai || aj)) continue;
-        const float4 c0 = __ldg(d.cst32 + 3 * (long long)j), c1 = __ldg(d.cst32 + 3 * (long long)j + 1),
-                     c2 = __ldg(d.cst32 + 3 * (long long)j + 2);
-        const float L = fabsf(g.w);
-        const float du[3] = {(float)(uj.x - ui.x), (float)(uj.y - ui.y), (float)(uj.z - ui.z)};
-        const float oi = ai ? omega_of_f(d.kernel, Pi.deltaf, L) : 0.f;
-        float oj = 0.f;
-        if (aj) {
-          float dj = Pi.deltaf;
-          if (d.multi) dj = d.params[d.meta[j] & META_PID_MASK].deltaf;
-          oj = omega_of_f(d.kernel, dj, L);
-        }
-        const float Aj[9] = {c0.x, c0.y, c0.z, c0.w, c1.x, c1.y, c1.z, c1.w, c2.x};
-        const float bj = c2.y;
-        const float V = (float)uj.w;
-        float t[3];
-#pragma unroll
-        for (int r = 0; r < 3; r++) {
-          const float ti = Ai[r] * g.x + Ai[r + 3] * g.y + Ai[r + 6] * g.z + bi * du[r];
-          const float tj = Aj[r] * g.x + Aj[r + 3] * g.y + Aj[r + 6] * g.z + bj * du[r];
-          t[r] = (oi * ti + oj * tj) * V;
-        }
-        bx.add(t[0]); by.add(t[1]); bz.add(t[2]);
+      Ai[0] = a0.x; Ai[1] = a0.y; Ai[2] = a0.z; Ai[3] = a0.w;
+      Ai[4] = a1.x; Ai[5] = a1.y; Ai[6] = a1.z; Ai[7] = a1.w; Ai[8] = a2.x;
+      bi = a2.y;
+    }
+    for (int r = 0; r < rows; r++) {
+      const unsigned word = __ldg(d.bits + (sbase >> 5) + r);
+      const int k = r * G + gl;
+      if (k >= cnt) continue;
+      const long long b = sbase + (long long)r * 32 + lane;
+      const bool ai = (word >> lane) & 1u;
+      const int j = __ldg(d.nbr + b);
+      const bool aj = d.sym ? ai : bond_bit(d.bits, rev_slot(d, b, j));
+      if (!(ai || aj)) continue;
+      const float4 g = __ldg(d.geo + b);
+      const float4 hj = __ldg(d.uhi + j), lj = __ldg(d.ulo + j);
+      const float4 c0 = __ldg(d.cst32 + 3 * (long long)j), c1 = __ldg(d.cst32 + 3 * (long long)j + 1),
+                   c2 = __ldg(d.cst32 + 3 * (long long)j + 2);
+      const float L = fabsf(g.w);
+      const float du[3] = {(hj.x - hi.x) + (lj.x - lo.x), (hj.y - hi.y) + (lj.y - lo.y),
+                           (hj.z - hi.z) + (lj.z - lo.z)};
+      const float oi = ai ? omega_of_f(d.kernel, Pi.deltaf, L) : 0.f;
+      float oj = 0.f;
+      if (aj) {
+        float dj = Pi.deltaf;
+        if (d.multi) dj = d.params[d.meta[j] & META_PID_MASK].deltaf;
+        oj = omega_of_f(d.kernel, dj, L);
       }
+      const float Aj[9] = {c0.x, c0.y, c0.z, c0.w, c1.x, c1.y, c1.z, c1.w, c2.x};
+      const float bj = c2.y;
+      const float V = hj.w;
+      float t[3];
+#pragma unroll
+      for (int q = 0; q < 3; q++) {
+        const float ti = Ai[q] * g.x + Ai[q + 3] * g.y + Ai[q + 6] * g.z + bi * du[q];
+        const float tj = Aj[q] * g.x + Aj[q + 3] * g.y + Aj[q + 6] * g.z + bj * du[q];
+        t[q] = (oi * ti + oj * tj) * V;
+      }
+      bx.add(t[0]); by.add(t[1]); bz.add(t[2]);
     }
     if (G > 1) { group_reduce<G>(bx); group_reduce<G>(by); group_reduce<G>(bz); }
     if (valid && gl == 0) {
@@ -451,8 +508,8 @@ __global__ void __launch_bounds__(256) k_c_b32(DevBody d, int kstep) {
     default: { constexpr int GG = 32; CALL; } break;    \
   }
 
-static int grid_for32(long long n, int G, int block) {
-  long long warps = (n + (32 / G) - 1) / (32 / G);
+static int grid_for32(long long nslices, int block) {
+  long long warps = nslices;
   long long blocks = (warps + block / 32 - 1) / (block / 32);
   if (blocks < 1) blocks = 1;
   if (blocks > 148LL * 64) blocks = 148LL * 64;
@@ -460,8 +517,8 @@ static int grid_for32(long long n, int G, int block) {
 }
 
 int launch_force32(const DevBody& d, const LaunchCfg& c, int kstep, int phase, cudaStream_t s) {
-  const int G = c.group < 1 ? 1 : c.group;
-  const int grid = grid_for32(d.n, G, c.block);
+  const int G = d.lg;
+  const int grid = grid_for32(d.nslices, c.block);
   const bool A = phase != 2, B = phase != 1;
   int launches = 0;
   if (d.material == MAT_BB) {

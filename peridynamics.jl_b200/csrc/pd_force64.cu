@@ -109,32 +109,32 @@ __device__ __forceinline__ void flag_nan(const DevBody& d, int kstep, double x, 
   }
 }
 
-// the warp-uniform loop over point groups: every lane of a warp runs the same number of
-// iterations so that the group shuffles see all lanes
-#define PD_POINT_LOOP(G)                                                                     \
-  constexpr int PPW = 32 / (G);                                                              \
-  const int lane = threadIdx.x & 31;                                                         \
-  const int sub = lane / (G), gl = lane % (G);                                               \
-  const long long warp0 = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;           \
-  const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;                         \
-  for (long long w = warp0; w * PPW < d.n; w += nwarps)
+// new bond_active word of a row after the failure tests of its lanes; the warp owns the word
+__device__ __forceinline__ void commit_row64(unsigned int* bits, long long word_idx, unsigned old,
+                                             bool act, int lane) {
+  const unsigned nw = __ballot_sync(0xffffffffu, act);
+  if (lane == 0 && nw != old) bits[word_idx] = nw;
+}
 
 // -------------------------------------------------------------------------------------------
 // BB: bond_based.jl:125-180 (calc_failure! storing the bond length, force_density_point!)
 // -------------------------------------------------------------------------------------------
 template <int G, bool MULTI>
-__global__ void __launch_bounds__(256) k_bb64(DevBody d, int kstep) {
+__global__ void PD_LB k_bb64(DevBody d, int kstep) {
   if (d.ctrl->err) return;
-  PD_POINT_LOOP(G) {
-    const long long i = w * PPW + sub;
-    const bool valid = i < d.n;
+  PD_SLICE_LOOP(G) {
+    PD_SLICE_SETUP
     double bx = 0.0, by = 0.0, bz = 0.0;
     int na = 0;
-    if (valid) {
-      const double4 xi = ld4(d.cur + i);
-      const DevParam P = d.params[d.meta[i] & META_PID_MASK];
-      const long long b0 = d.off[i], b1 = d.off[i + 1];
-      for (long long b = b0 + gl; b < b1; b += G) {
+    const double4 xi = valid ? ld4(d.cur + i) : make_double4(0, 0, 0, 0);
+    const DevParam& P = d.params[valid ? (d.meta[i] & META_PID_MASK) : 0];
+    for (int r = 0; r < rows; r++) {
+      const long long wi = (sbase >> 5) + r;
+      const unsigned word = d.bits[wi];
+      const int k = r * G + gl;
+      bool act = false;
+      if (k < cnt) {
+        const long long b = sbase + (long long)r * 32 + lane;
         const int j = __ldg(d.nbr + b);
         const double Ls = __ldg(d.len64 + b);
         const double L = fabs(Ls);
@@ -142,21 +142,21 @@ __global__ void __launch_bounds__(256) k_bb64(DevBody d, int kstep) {
         const double dx = xj.x - xi.x, dy = xj.y - xi.y, dz = xj.z - xi.z;
         const double l = sqrt((dx * dx + dy * dy) + dz * dz);
         const double eps = (l - L) / L;
-        bool act = bond_bit_live(d.bits, b);
-        if (act && eps > P.epsc && Ls > 0) { act = false; clear_bit(d.bits, b); }
-        na += act;
+        act = ((word >> lane) & 1u) && !(eps > P.epsc && Ls > 0);
         const double om = act ? 1.0 : 0.0;
-        double s;
+        double sc;
         if (MULTI) {
           const double bcj = d.params[d.meta[j] & META_PID_MASK].bc;
-          s = om * (P.bc + bcj) / 2 * eps * xj.w;
+          sc = om * (P.bc + bcj) / 2 * eps * xj.w;
         } else {
-          s = om * P.bc * eps * xj.w;
+          sc = om * P.bc * eps * xj.w;
         }
-        bx += s * dx / l;
-        by += s * dy / l;
-        bz += s * dz / l;
+        bx += sc * dx / l;
+        by += sc * dy / l;
+        bz += sc * dz / l;
       }
+      na += act;
+      commit_row64(d.bits, wi, word, act, lane);
     }
     if (G > 1) {
       bx = group_sum<G>(bx); by = group_sum<G>(by); bz = group_sum<G>(bz); na = group_sum<G>(na);
@@ -174,20 +174,22 @@ __global__ void __launch_bounds__(256) k_bb64(DevBody d, int kstep) {
 // calc_weighted_volume (:176-189), calc_dilatation (:191-204), c1, c2 (:135-136)
 // -------------------------------------------------------------------------------------------
 template <int G, bool EXACT>
-__global__ void __launch_bounds__(256) k_osb_a64(DevBody d, int kstep) {
+__global__ void PD_LB k_osb_a64(DevBody d, int kstep) {
   if (d.ctrl->err) return;
-  PD_POINT_LOOP(G) {
-    const long long i = w * PPW + sub;
-    const bool valid = i < d.n;
+  PD_SLICE_LOOP(G) {
+    PD_SLICE_SETUP
     double wvol = 0.0, sdil = 0.0;
     int na = 0;
-    const DevParam P = d.params[valid ? (d.meta[i] & META_PID_MASK) : 0];
-    long long b0 = 0, b1 = 0;
-    double4 xi = make_double4(0, 0, 0, 0), Xi = xi;
-    if (valid) {
-      xi = ld4(d.cur + i); Xi = ld4(d.X0 + i);
-      b0 = d.off[i]; b1 = d.off[i + 1];
-      for (long long b = b0 + gl; b < b1; b += G) {
+    const DevParam& P = d.params[valid ? (d.meta[i] & META_PID_MASK) : 0];
+    const double4 xi = valid ? ld4(d.cur + i) : make_double4(0, 0, 0, 0);
+    const double4 Xi = valid ? ld4(d.X0 + i) : make_double4(0, 0, 0, 0);
+    for (int r = 0; r < rows; r++) {
+      const long long wi = (sbase >> 5) + r;
+      const unsigned word = d.bits[wi];
+      const int k = r * G + gl;
+      bool act = false;
+      if (k < cnt) {
+        const long long b = sbase + (long long)r * 32 + lane;
         const int j = __ldg(d.nbr + b);
         const double Ls = __ldg(d.len64 + b);
         const double L = fabs(Ls);
@@ -195,23 +197,28 @@ __global__ void __launch_bounds__(256) k_osb_a64(DevBody d, int kstep) {
         const double dx = xj.x - xi.x, dy = xj.y - xi.y, dz = xj.z - xi.z;
         const double l = sqrt((dx * dx + dy * dy) + dz * dz);
         const double eps = (l - L) / L;
-        bool act = bond_bit_live(d.bits, b);
-        if (act && eps > P.epsc && Ls > 0) { act = false; clear_bit(d.bits, b); }
-        na += act;
+        act = ((word >> lane) & 1u) && !(eps > P.epsc && Ls > 0);
         const double DX = Xj.x - Xi.x, DY = Xj.y - Xi.y, DZ = Xj.z - Xi.z;
         const double om = act ? omega_of(d.kernel, P.delta, L) : 0.0;
         wvol += om * 1.0 * ((DX * DX + DY * DY) + DZ * DZ) * xj.w;
         if (!EXACT) sdil += om * 1.0 * L * (l - L) * xj.w;
       }
+      na += act;
+      commit_row64(d.bits, wi, word, act, lane);
     }
     if (G > 1) {
       wvol = group_sum<G>(wvol); sdil = group_sum<G>(sdil); na = group_sum<G>(na);
     }
     double dil = 0.0;
-    if (EXACT && valid && wvol != 0.0) {
-      // second sweep of the reference with c1 = 3 / wvol inside every term
+    if (EXACT) {
+      // second sweep of the reference with c1 = 3 / wvol inside every term; the bits were
+      // written above by lane 0 of the warp, so the decision is recomputed from the same eps
+      __syncwarp();
       const double c1d = 3.0 / wvol;
-      for (long long b = b0; b < b1; b++) {
+      for (int r = 0; r < rows; r++) {
+        const int k = r * G + gl;
+        if (k >= cnt || wvol == 0.0) continue;
+        const long long b = sbase + (long long)r * 32 + lane;
         const int j = __ldg(d.nbr + b);
         const double Ls = __ldg(d.len64 + b);
         const double L = fabs(Ls);
@@ -219,12 +226,11 @@ __global__ void __launch_bounds__(256) k_osb_a64(DevBody d, int kstep) {
         const double dx = xj.x - xi.x, dy = xj.y - xi.y, dz = xj.z - xi.z;
         const double l = sqrt((dx * dx + dy * dy) + dz * dz);
         const double eps = (l - L) / L;
-        // the bit may have been cleared above; the decision is recomputed from the same eps
         const bool act = bond_bit_live(d.bits, b) && !(eps > P.epsc && Ls > 0);
         const double om = act ? omega_of(d.kernel, P.delta, L) : 0.0;
         dil += om * 1.0 * c1d * L * (l - L) * xj.w;
       }
-    } else if (!EXACT && wvol != 0.0) {
+    } else if (wvol != 0.0) {
       dil = 3.0 / wvol * sdil;
     }
     if (valid && gl == 0) {
@@ -242,8 +248,8 @@ __global__ void __launch_bounds__(256) k_osb_a64(DevBody d, int kstep) {
 // p = omega beta (c2 L + c1 (l - L)) / l (ordinary_state_based.jl:144), coefficients of the
 // bond owner o with the partner q (ParameterHandler form :165-166 when MULTI)
 template <bool MULTI>
-__device__ __forceinline__ double osb_s64(const DevBody& d, const double4& co, const DevParam& Po,
-                                          const DevParam& Pq, double om, double L, double l) {
+__device__ __forceinline__ double osb_s64(const double4& co, const DevParam& Po, const DevParam& Pq,
+                                          double om, double L, double l) {
   double c1, c2;
   if (MULTI) {
     c1 = 15.0 * (Po.G + Pq.G) / (2 * co.z);
@@ -259,64 +265,71 @@ __device__ __forceinline__ double osb_s64(const DevBody& d, const double4& co, c
 // OSB phase B: force_density_point! (ordinary_state_based.jl:128-174) in gather form
 // -------------------------------------------------------------------------------------------
 template <int G, bool EXACT, bool MULTI>
-__global__ void __launch_bounds__(256) k_osb_b64(DevBody d, int kstep) {
+__global__ void PD_LB k_osb_b64(DevBody d, int kstep) {
   if (d.ctrl->err) return;
-  PD_POINT_LOOP(G) {
-    const long long i = w * PPW + sub;
-    const bool valid = i < d.n;
+  PD_SLICE_LOOP(G) {
+    PD_SLICE_SETUP
     double bx = 0.0, by = 0.0, bz = 0.0;
-    if (valid) {
-      const double4 xi = ld4(d.cur + i);
-      const double Vi = xi.w;
-      (void)Vi;
-      const DevParam Pi = d.params[d.meta[i] & META_PID_MASK];
-      const double4 ci = d.coef64[i];
-      const bool own = ci.z != 0.0;
-      const long long b0 = d.off[i], b1 = d.off[i + 1];
-      // own term of bond b
-      auto own_term = [&](long long b) {
-        const int j = __ldg(d.nbr + b);
-        const double L = fabs(__ldg(d.len64 + b));
-        const double4 xj = ld4(d.cur + j);
-        const double dx = xj.x - xi.x, dy = xj.y - xi.y, dz = xj.z - xi.z;
-        const double l = sqrt((dx * dx + dy * dy) + dz * dz);
-        const bool act = bond_bit(d.bits, b);
-        const double om = act ? omega_of(d.kernel, Pi.delta, L) : 0.0;
-        const DevParam& Pj = MULTI ? d.params[d.meta[j] & META_PID_MASK] : Pi;
-        const double s = osb_s64<MULTI>(d, ci, Pi, Pj, om, L, l);
-        bx += s * dx * xj.w;
-        by += s * dy * xj.w;
-        bz += s * dz * xj.w;
-      };
-      // term that j's loop scatters into b_i through its bond j -> i
-      auto nbr_term = [&](long long b) {
-        const int j = __ldg(d.nbr + b);
-        const double4 cj = d.coef64[j];
-        if (cj.z == 0.0) return;  // j returned early (iszero(wvol))
-        const double L = fabs(__ldg(d.len64 + b));
-        const double4 xj = ld4(d.cur + j);
-        const double dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
-        const double l = sqrt((dx * dx + dy * dy) + dz * dz);
-        const bool act = d.sym ? bond_bit(d.bits, b) : bond_bit(d.bits, __ldg(d.rev + b));
-        const DevParam Pj = d.params[d.meta[j] & META_PID_MASK];
-        const double om = act ? omega_of(d.kernel, Pj.delta, L) : 0.0;
-        const double s = osb_s64<MULTI>(d, cj, Pj, Pi, om, L, l);
-        bx += -(s * dx) * xj.w;
-        by += -(s * dy) * xj.w;
-        bz += -(s * dz) * xj.w;
-      };
-      if (EXACT) {
-        long long split = b0;
-        while (split < b1 && __ldg(d.nbr + split) < i) split++;
-        for (long long b = b0; b < split; b++) nbr_term(b);
-        if (own)
-          for (long long b = b0; b < b1; b++) own_term(b);
-        for (long long b = split; b < b1; b++) nbr_term(b);
-      } else {
-        for (long long b = b0 + gl; b < b1; b += G) {
-          if (own) own_term(b);
-          nbr_term(b);
+    const double4 xi = valid ? ld4(d.cur + i) : make_double4(0, 0, 0, 0);
+    const DevParam& Pi = d.params[valid ? (d.meta[i] & META_PID_MASK) : 0];
+    const double4 ci = valid ? d.coef64[i] : make_double4(0, 0, 0, 0);
+    const bool own = ci.z != 0.0;
+    // own term of the bond in slot b
+    auto own_term = [&](long long b) {
+      const int j = __ldg(d.nbr + b);
+      const double L = fabs(__ldg(d.len64 + b));
+      const double4 xj = ld4(d.cur + j);
+      const double dx = xj.x - xi.x, dy = xj.y - xi.y, dz = xj.z - xi.z;
+      const double l = sqrt((dx * dx + dy * dy) + dz * dz);
+      const bool act = bond_bit(d.bits, b);
+      const double om = act ? omega_of(d.kernel, Pi.delta, L) : 0.0;
+      const DevParam& Pj = MULTI ? d.params[d.meta[j] & META_PID_MASK] : Pi;
+      const double sc = osb_s64<MULTI>(ci, Pi, Pj, om, L, l);
+      bx += sc * dx * xj.w;
+      by += sc * dy * xj.w;
+      bz += sc * dz * xj.w;
+    };
+    // term that j's loop scatters into b_i through its bond j -> i
+    auto nbr_term = [&](long long b) {
+      const int j = __ldg(d.nbr + b);
+      const double4 cj = d.coef64[j];
+      if (cj.z == 0.0) return;  // j returned early (iszero(wvol))
+      const double L = fabs(__ldg(d.len64 + b));
+      const double4 xj = ld4(d.cur + j);
+      const double dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
+      const double l = sqrt((dx * dx + dy * dy) + dz * dz);
+      const bool act = d.sym ? bond_bit(d.bits, b) : bond_bit(d.bits, rev_slot(d, b, j));
+      const DevParam& Pj = d.params[d.meta[j] & META_PID_MASK];
+      const double om = act ? omega_of(d.kernel, Pj.delta, L) : 0.0;
+      const double sc = osb_s64<MULTI>(cj, Pj, Pi, om, L, l);
+      bx += -(sc * dx) * xj.w;
+      by += -(sc * dy) * xj.w;
+      bz += -(sc * dz) * xj.w;
+    };
+    if (EXACT) {
+      // the serial scatter order: neighbours j < i, own bonds, neighbours j > i
+      for (int r = 0; r < rows; r++) {
+        const int k = r * G + gl;
+        const long long b = sbase + (long long)r * 32 + lane;
+        if (k < cnt && __ldg(d.nbr + b) < i) nbr_term(b);
+      }
+      if (own)
+        for (int r = 0; r < rows; r++) {
+          const int k = r * G + gl;
+          if (k < cnt) own_term(sbase + (long long)r * 32 + lane);
         }
+      for (int r = 0; r < rows; r++) {
+        const int k = r * G + gl;
+        const long long b = sbase + (long long)r * 32 + lane;
+        if (k < cnt && __ldg(d.nbr + b) > i) nbr_term(b);
+      }
+    } else {
+      for (int r = 0; r < rows; r++) {
+        const int k = r * G + gl;
+        if (k >= cnt) continue;
+        const long long b = sbase + (long long)r * 32 + lane;
+        if (own) own_term(b);
+        nbr_term(b);
       }
     }
     if (G > 1) { bx = group_sum<G>(bx); by = group_sum<G>(by); bz = group_sum<G>(bz); }
@@ -333,23 +346,24 @@ __global__ void __launch_bounds__(256) k_osb_b64(DevBody d, int kstep) {
 // calc_first_piola_kirchhoff! (:216-224)
 // -------------------------------------------------------------------------------------------
 template <int G>
-__global__ void __launch_bounds__(256) k_c_a64(DevBody d, int kstep) {
+__global__ void PD_LB k_c_a64(DevBody d, int kstep) {
   if (d.ctrl->err) return;
-  PD_POINT_LOOP(G) {
-    const long long i = w * PPW + sub;
-    const bool valid = i < d.n;
+  PD_SLICE_LOOP(G) {
+    PD_SLICE_SETUP
     double K[9], Ft[9];
-    for (int k = 0; k < 9; k++) { K[k] = 0.0; Ft[k] = 0.0; }
+    for (int q = 0; q < 9; q++) { K[q] = 0.0; Ft[q] = 0.0; }
     int na = 0;
-    unsigned meta = 0;
-    long long b0 = 0, b1 = 0;
-    DevParam P = d.params[0];
-    if (valid) {
-      meta = d.meta[i];
-      P = d.params[meta & META_PID_MASK];
-      const double4 xi = ld4(d.cur + i), Xi = ld4(d.X0 + i);
-      b0 = d.off[i]; b1 = d.off[i + 1];
-      for (long long b = b0 + gl; b < b1; b += G) {
+    const unsigned meta = valid ? d.meta[i] : 0u;
+    const DevParam& P = d.params[meta & META_PID_MASK];
+    const double4 xi = valid ? ld4(d.cur + i) : make_double4(0, 0, 0, 0);
+    const double4 Xi = valid ? ld4(d.X0 + i) : make_double4(0, 0, 0, 0);
+    for (int r = 0; r < rows; r++) {
+      const long long wi = (sbase >> 5) + r;
+      const unsigned word = d.bits[wi];
+      const int k = r * G + gl;
+      bool act = false;
+      if (k < cnt) {
+        const long long b = sbase + (long long)r * 32 + lane;
         const int j = __ldg(d.nbr + b);
         const double Ls = __ldg(d.len64 + b);
         const double L = fabs(Ls);
@@ -357,32 +371,31 @@ __global__ void __launch_bounds__(256) k_c_a64(DevBody d, int kstep) {
         const double dx[3] = {xj.x - xi.x, xj.y - xi.y, xj.z - xi.z};
         const double l = sqrt(dot3(dx, dx));
         const double eps = (l - L) / L;
-        bool act = bond_bit_live(d.bits, b);
-        if (act && eps > P.epsc && Ls > 0) { act = false; clear_bit(d.bits, b); }
-        na += act;
+        act = ((word >> lane) & 1u) && !(eps > P.epsc && Ls > 0);
         const double DX[3] = {Xj.x - Xi.x, Xj.y - Xi.y, Xj.z - Xi.z};
         const double om = act ? omega_of(d.kernel, P.delta, L) : 0.0;
         const double temp = om * xj.w;
         for (int c = 0; c < 3; c++)
-          for (int r = 0; r < 3; r++) {
-            K[r + 3 * c] = K[r + 3 * c] + temp * (DX[r] * DX[c]);
-            Ft[r + 3 * c] = Ft[r + 3 * c] + temp * (dx[r] * DX[c]);
+          for (int q = 0; q < 3; q++) {
+            K[q + 3 * c] = K[q + 3 * c] + temp * (DX[q] * DX[c]);
+            Ft[q + 3 * c] = Ft[q + 3 * c] + temp * (dx[q] * DX[c]);
           }
       }
+      na += act;
+      commit_row64(d.bits, wi, word, act, lane);
     }
     if (G > 1) {
-      for (int k = 0; k < 9; k++) { K[k] = group_sum<G>(K[k]); Ft[k] = group_sum<G>(Ft[k]); }
+      for (int q = 0; q < 9; q++) { K[q] = group_sum<G>(K[q]); Ft[q] = group_sum<G>(Ft[q]); }
       na = group_sum<G>(na);
     }
     bool killed = false;
     if (valid && gl == 0) {
-      const long long nn = b1 - b0;
-      const double damage = 1.0 - (double)na / (double)nn;
+      const double damage = 1.0 - (double)na / (double)cnt;
       double Kinv[9], F[9];
       inv3(K, Kinv);
       matmul3(Ft, Kinv, F);
       bool hasnan = false;
-      for (int k = 0; k < 9; k++) { d.F64[9 * i + k] = F[k]; hasnan |= isnan(F[k]); }
+      for (int q = 0; q < 9; q++) { d.F64[9 * i + q] = F[q]; hasnan |= isnan(F[q]); }
       killed = (meta & META_KILLED) || damage > d.maxdmg || hasnan;
       if (killed) {
         if (!(meta & META_KILLED)) d.meta[i] = meta | META_KILLED;
@@ -391,15 +404,16 @@ __global__ void __launch_bounds__(256) k_c_a64(DevBody d, int kstep) {
         double Pm[9], PKinv[9];
         pk1_64(d.cmodel, P, F, Pm);
         matmul3(Pm, Kinv, PKinv);
-        for (int k = 0; k < 9; k++) d.PK64[9 * i + k] = PKinv[k];
+        for (int q = 0; q < 9; q++) d.PK64[9 * i + q] = PKinv[q];
       }
       d.n_active[i] = na;
     }
-    // directed bond states: a killed point loses all its bonds (correspondence.jl:293)
     if (!d.sym) {
+      // directed bond states: a killed point loses all its bonds (correspondence.jl:293)
       if (G > 1) killed = group_bcast<G>(killed);
-      if (valid && killed)
-        for (long long b = b0 + gl; b < b1; b += G) clear_bit(d.bits, b);
+      const unsigned kill_mask = __ballot_sync(0xffffffffu, valid && killed);
+      if (kill_mask && lane == 0)
+        for (int r = 0; r < rows; r++) d.bits[(sbase >> 5) + r] &= ~kill_mask;
     }
   }
 }
@@ -412,69 +426,80 @@ __device__ __forceinline__ void c_bond_t64(const double* F, const double* PK, do
                                            double* t) {
   double FD[3], z[3], W[9], WD[3];
   matvec3(F, DX, FD);
-  for (int k = 0; k < 3; k++) z[k] = dx[k] - FD[k];
+  for (int q = 0; q < 3; q++) z[q] = dx[q] - FD[q];
   const double ob = om * beta;
-  for (int k = 0; k < 9; k++) W[k] = om * PK[k];
+  for (int q = 0; q < 9; q++) W[q] = om * PK[q];
   matvec3(W, DX, WD);
-  for (int k = 0; k < 3; k++) t[k] = WD[k] + ob * z[k];
+  for (int q = 0; q < 3; q++) t[q] = WD[q] + ob * z[q];
 }
 
 template <int G, bool EXACT>
-__global__ void __launch_bounds__(256) k_c_b64(DevBody d, int kstep) {
+__global__ void PD_LB k_c_b64(DevBody d, int kstep) {
   if (d.ctrl->err) return;
-  PD_POINT_LOOP(G) {
-    const long long i = w * PPW + sub;
-    const bool valid = i < d.n;
+  PD_SLICE_LOOP(G) {
+    PD_SLICE_SETUP
     double bx = 0.0, by = 0.0, bz = 0.0;
-    if (valid) {
-      const double4 xi = ld4(d.cur + i), Xi = ld4(d.X0 + i);
-      const unsigned mi = d.meta[i];
-      const DevParam Pi = d.params[mi & META_PID_MASK];
-      const bool own = !(mi & META_KILLED);
-      double Fi[9], PKi[9];
+    const double4 xi = valid ? ld4(d.cur + i) : make_double4(0, 0, 0, 0);
+    const double4 Xi = valid ? ld4(d.X0 + i) : make_double4(0, 0, 0, 0);
+    const unsigned mi = valid ? d.meta[i] : META_KILLED;
+    const DevParam& Pi = d.params[mi & META_PID_MASK];
+    const bool own = !(mi & META_KILLED);
+    double Fi[9], PKi[9];
+    for (int q = 0; q < 9; q++) {
+      Fi[q] = own ? d.F64[9 * i + q] : 0.0;
+      PKi[q] = own ? d.PK64[9 * i + q] : 0.0;
+    }
+    auto own_term = [&](long long b) {
+      const int j = __ldg(d.nbr + b);
+      const double L = fabs(__ldg(d.len64 + b));
+      const double4 xj = ld4(d.cur + j), Xj = ld4(d.X0 + j);
+      const double DX[3] = {Xj.x - Xi.x, Xj.y - Xi.y, Xj.z - Xi.z};
+      const double dx[3] = {xj.x - xi.x, xj.y - xi.y, xj.z - xi.z};
+      const bool act = bond_bit(d.bits, b);
+      const double om = act ? omega_of(d.kernel, Pi.delta, L) : 0.0;
+      double t[3];
+      c_bond_t64(Fi, PKi, Pi.beta, om, DX, dx, t);
+      bx += t[0] * xj.w; by += t[1] * xj.w; bz += t[2] * xj.w;
+    };
+    auto nbr_term = [&](long long b) {
+      const int j = __ldg(d.nbr + b);
+      const unsigned mj = d.meta[j];
+      if (mj & META_KILLED) return;  // j returned early after too_much_damage!
+      const double L = fabs(__ldg(d.len64 + b));
+      const bool act = d.sym ? bond_bit(d.bits, b) : bond_bit(d.bits, rev_slot(d, b, j));
+      const DevParam& Pj = d.params[mj & META_PID_MASK];
+      const double4 xj = ld4(d.cur + j), Xj = ld4(d.X0 + j);
+      const double DX[3] = {Xi.x - Xj.x, Xi.y - Xj.y, Xi.z - Xj.z};
+      const double dx[3] = {xi.x - xj.x, xi.y - xj.y, xi.z - xj.z};
+      const double om = act ? omega_of(d.kernel, Pj.delta, L) : 0.0;
+      double Fj[9], PKj[9], t[3];
+      for (int q = 0; q < 9; q++) { Fj[q] = d.F64[9 * (long long)j + q]; PKj[q] = d.PK64[9 * (long long)j + q]; }
+      c_bond_t64(Fj, PKj, Pj.beta, om, DX, dx, t);
+      bx += -t[0] * xj.w; by += -t[1] * xj.w; bz += -t[2] * xj.w;
+    };
+    if (EXACT) {
+      for (int r = 0; r < rows; r++) {
+        const int k = r * G + gl;
+        const long long b = sbase + (long long)r * 32 + lane;
+        if (k < cnt && __ldg(d.nbr + b) < i) nbr_term(b);
+      }
       if (own)
-        for (int k = 0; k < 9; k++) { Fi[k] = d.F64[9 * i + k]; PKi[k] = d.PK64[9 * i + k]; }
-      const long long b0 = d.off[i], b1 = d.off[i + 1];
-      auto own_term = [&](long long b) {
-        const int j = __ldg(d.nbr + b);
-        const double L = fabs(__ldg(d.len64 + b));
-        const double4 xj = ld4(d.cur + j), Xj = ld4(d.X0 + j);
-        const double DX[3] = {Xj.x - Xi.x, Xj.y - Xi.y, Xj.z - Xi.z};
-        const double dx[3] = {xj.x - xi.x, xj.y - xi.y, xj.z - xi.z};
-        const bool act = bond_bit(d.bits, b);
-        const double om = act ? omega_of(d.kernel, Pi.delta, L) : 0.0;
-        double t[3];
-        c_bond_t64(Fi, PKi, Pi.beta, om, DX, dx, t);
-        bx += t[0] * xj.w; by += t[1] * xj.w; bz += t[2] * xj.w;
-      };
-      auto nbr_term = [&](long long b) {
-        const int j = __ldg(d.nbr + b);
-        const unsigned mj = d.meta[j];
-        if (mj & META_KILLED) return;  // j returned early after too_much_damage!
-        const double L = fabs(__ldg(d.len64 + b));
-        const bool act = d.sym ? bond_bit(d.bits, b) : bond_bit(d.bits, __ldg(d.rev + b));
-        const DevParam Pj = d.params[mj & META_PID_MASK];
-        const double4 xj = ld4(d.cur + j), Xj = ld4(d.X0 + j);
-        const double DX[3] = {Xi.x - Xj.x, Xi.y - Xj.y, Xi.z - Xj.z};
-        const double dx[3] = {xi.x - xj.x, xi.y - xj.y, xi.z - xj.z};
-        const double om = act ? omega_of(d.kernel, Pj.delta, L) : 0.0;
-        double Fj[9], PKj[9], t[3];
-        for (int k = 0; k < 9; k++) { Fj[k] = d.F64[9 * (long long)j + k]; PKj[k] = d.PK64[9 * (long long)j + k]; }
-        c_bond_t64(Fj, PKj, Pj.beta, om, DX, dx, t);
-        bx += -t[0] * xj.w; by += -t[1] * xj.w; bz += -t[2] * xj.w;
-      };
-      if (EXACT) {
-        long long split = b0;
-        while (split < b1 && __ldg(d.nbr + split) < i) split++;
-        for (long long b = b0; b < split; b++) nbr_term(b);
-        if (own)
-          for (long long b = b0; b < b1; b++) own_term(b);
-        for (long long b = split; b < b1; b++) nbr_term(b);
-      } else {
-        for (long long b = b0 + gl; b < b1; b += G) {
-          if (own) own_term(b);
-          nbr_term(b);
+        for (int r = 0; r < rows; r++) {
+          const int k = r * G + gl;
+          if (k < cnt) own_term(sbase + (long long)r * 32 + lane);
         }
+      for (int r = 0; r < rows; r++) {
+        const int k = r * G + gl;
+        const long long b = sbase + (long long)r * 32 + lane;
+        if (k < cnt && __ldg(d.nbr + b) > i) nbr_term(b);
+      }
+    } else {
+      for (int r = 0; r < rows; r++) {
+        const int k = r * G + gl;
+        if (k >= cnt) continue;
+        const long long b = sbase + (long long)r * 32 + lane;
+        if (own) own_term(b);
+        nbr_term(b);
       }
     }
     if (G > 1) { bx = group_sum<G>(bx); by = group_sum<G>(by); bz = group_sum<G>(bz); }
@@ -514,8 +539,8 @@ __global__ void k_cauchy64(DevBody d, const double* F, int from_h32, double* out
     default: { constexpr int GG = 32; CALL; } break; \
   }
 
-static int grid_for(long long n, int G, int block) {
-  long long warps = (n + (32 / G) - 1) / (32 / G);
+static int grid_for(long long nslices, int block) {
+  long long warps = nslices;
   long long blocks = (warps + block / 32 - 1) / (block / 32);
   if (blocks < 1) blocks = 1;
   if (blocks > 148LL * 64) blocks = 148LL * 64;
@@ -523,8 +548,8 @@ static int grid_for(long long n, int G, int block) {
 }
 
 int launch_force64(const DevBody& d, const LaunchCfg& c, int kstep, int phase, cudaStream_t s) {
-  const int G = c.exact ? 1 : c.group;
-  const int grid = grid_for(d.n, G, c.block);
+  const int G = d.lg;
+  const int grid = grid_for(d.nslices, c.block);
   const bool A = phase != 2, B = phase != 1;
   int launches = 0;
   if (d.material == MAT_BB) {

@@ -9,6 +9,7 @@ struct LaunchCfg {
   int group;  // lanes per point: 1, 2, 4, 8, 16, 32
   int block;  // threads per block
   bool exact; // FP64: one lane per point in the reference's serial summation order
+  int pipe;   // FP32: 0 = plain loads, > 0 = TMA-staged bond stream (pd_force32_tma.cu)
 };
 
 // boundary conditions as the integration kernels see them
@@ -47,6 +48,8 @@ struct IntDev {
 // second kernel of the state-based materials. Returns the number of kernels launched.
 int launch_force64(const DevBody& d, const LaunchCfg& c, int kstep, int phase, cudaStream_t s);
 int launch_force32(const DevBody& d, const LaunchCfg& c, int kstep, int phase, cudaStream_t s);
+bool tma_supported(const DevBody& d);
+int launch_force32_tma(const DevBody& d, int pipe, int kstep, int phase, cudaStream_t s);
 void launch_cauchy64(const DevBody& d, const double* F, int from_h32, double* out, cudaStream_t s);
 
 // integration: mode 0 = kick from the stored (v, a), mode 1 = kick from the last force
@@ -55,18 +58,27 @@ void launch_kick_drift(const DevBody& d, const IntDev& g, int mode, double dt_ov
 void launch_bc(const DevBody& d, const IntDev& g, const BCDev& bc, double dt_override, int kstep,
                cudaStream_t s);
 void launch_finish(const DevBody& d, const IntDev& g, double dt_override, cudaStream_t s);
+void launch_split_u(const DevBody& d, cudaStream_t s);
 
-// helpers of the API layer
-void launch_pack_bits(const unsigned char* bytes, unsigned int* bits, long long nb, cudaStream_t s);
-void launch_export_bond_active(const DevBody& d, unsigned char* out, cudaStream_t s);
+// sliced bond layout and bond-array helpers (pd_layout.cu)
+cudaError_t build_slices(long long n, const long long* off, int G, long long** soff_out,
+                         long long* nslices_out, long long* nslots_out, cudaStream_t s);
+void launch_scatter_i32(const DevBody& d, const int* src, int* dst, cudaStream_t s);
+void launch_relayout_i32(const DevBody& a, const DevBody& b, const int* src, int* dst, cudaStream_t s);
+void launch_relayout_f64(const DevBody& a, const DevBody& b, const double* src, double* dst, cudaStream_t s);
+void launch_relayout_f4(const DevBody& a, const DevBody& b, const float4* src, float4* dst, cudaStream_t s);
+void launch_build_len64(const DevBody& d, const int* nbr_csr, const double* L, const unsigned char* fp,
+                        double* out, cudaStream_t s);
+void launch_build_geo(const DevBody& d, const int* nbr_csr, const double* L, const unsigned char* fp,
+                      float4* out, cudaStream_t s);
+void launch_pack_bits(const DevBody& d, const unsigned char* bytes, cudaStream_t s);
+void launch_export_bond_active(const DevBody& d, unsigned char* out, int raw, cudaStream_t s);
 void launch_count_active(const DevBody& d, cudaStream_t s);
-void launch_reverse(const DevBody& d, int* rev, int* flags, cudaStream_t s);
-void launch_check_sym(const DevBody& d, const int* rev, int* flags, cudaStream_t s);
+void launch_reverse(long long n, const long long* off, const int* nbr, int* revk, int* flags, cudaStream_t s);
+void launch_check_sym(const DevBody& d, int* flags, cudaStream_t s);
 void launch_export_damage(const DevBody& d, int valid, double* out, cudaStream_t s);
 void launch_export_position(const DevBody& d, const IntDev& g, double* out, int what, cudaStream_t s);
 void launch_timestep(const DevBody& d, double* dt_point, cudaStream_t s);
-void launch_build_len64(const DevBody& d, const double* L, const unsigned char* fp, double* out, cudaStream_t s);
-void launch_build_geo(const DevBody& d, const double* L, const unsigned char* fp, float4* out, cudaStream_t s);
 void launch_break_sets(const DevBody& d, const unsigned char* A, const unsigned char* B, cudaStream_t s);
 void launch_break_random(const DevBody& d, double fraction, unsigned long long seed, cudaStream_t s);
 

@@ -33,7 +33,7 @@ EXPORTS = (
     "pd_destroy", "pd_set_state", "pd_break_bonds", "pd_break_random_pairs", "pd_get_field",
     "pd_set_bcs", "pd_set_bc_values", "pd_stable_timestep", "pd_set_param_timesteps",
     "pd_force", "pd_run_vv", "pd_nan_step", "pd_run_vv_timed", "pd_autotune", "pd_set_mapping",
-    "pd_set_graph", "pd_info", "pd_launch_count", "pd_stream",
+    "pd_set_graph", "pd_set_pipeline", "pd_info", "pd_launch_count", "pd_stream",
 )
 
 
@@ -102,6 +102,7 @@ def lib():
         "pd_autotune": [vp, vp, vp],
         "pd_set_mapping": [vp, i32, i32],
         "pd_set_graph": [vp, i32],
+        "pd_set_pipeline": [vp, i32],
         "pd_info": [vp, vp, vp, vp],
         "pd_launch_count": [vp, vp],
         "pd_stream": [vp, vp],

@@ -271,6 +271,9 @@ class DeviceBody:
     def set_mapping(self, group, block=256):
         L.check(L.lib().pd_set_mapping(self.h, group, block), "pd_set_mapping")
 
+    def set_pipeline(self, pipe):
+        L.check(L.lib().pd_set_pipeline(self.h, pipe), "pd_set_pipeline")
+
     def autotune(self):
         g, b = C.c_int32(), C.c_int32()
         L.check(L.lib().pd_autotune(self.h, C.byref(g), C.byref(b)), "pd_autotune")

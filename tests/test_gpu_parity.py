@@ -286,3 +286,20 @@ def test_autotune_keeps_results():
     dev.force()
     assert rel_err(dev.field("b_int"), ref) < 1e-6
     assert dev.launch_count() > 0
+
+
+@pytest.mark.parametrize("name", ["BB", "OSB"])
+def test_staged_bond_stream_matches_direct_loads(name):
+    """The TMA-staged bond stream (pipelines 1-3) computes the same forces as direct loads."""
+    mat = MATERIALS[name]()
+    body = cube_body(mat, n=9)
+    u = deform(body._pos)
+    res = []
+    for pipe in (0, 1, 2, 3):
+        dev = pd.DeviceBody(body, precision="fp32")
+        dev.set_pipeline(pipe)
+        dev.set_state(displacement=u)
+        dev.force()
+        res.append((dev.field("b_int"), dev.field("n_active_bonds")))
+    for b, na in res[1:]:
+        assert np.array_equal(b, res[0][0]) and np.array_equal(na, res[0][1])

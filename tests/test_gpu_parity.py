@@ -301,5 +301,6 @@ def test_staged_bond_stream_matches_direct_loads(name):
         dev.set_state(displacement=u)
         dev.force()
         res.append((dev.field("b_int"), dev.field("n_active_bonds")))
+    # the same FP32 arithmetic; FMA contraction may differ between the two kernels
     for b, na in res[1:]:
-        assert np.array_equal(b, res[0][0]) and np.array_equal(na, res[0][1])
+        assert rel_err(b, res[0][0]) < 1e-6 and np.array_equal(na, res[0][1])

@@ -253,6 +253,33 @@ pd_status pd_launch_count(pd_handle *h, int64_t *count);
 /* The cudaStream_t of the handle, as an opaque pointer. */
 pd_status pd_stream(pd_handle *h, void **stream);
 
+/* Ordinary state-based force evaluation that allocates no device memory. No counterpart in
+ * the reference: it exists for callers that must not let the library allocate GPU memory --
+ * a host that owns every device buffer through its own pool, a time loop that must not stall
+ * on the allocator, or memory carved out of a fixed arena (the reference itself asserts that
+ * its force loop allocates nothing, test/perf/perf.jl).
+ * Every array is a device pointer owned by the caller, in the reference's CSR bond order
+ * (bond lists sorted by neighbour, symmetric, one parameter set): ref_position, position
+ * [3n], volume [n], bond_offsets [n+1], neighbors, bond_length, fail_permit [n_bonds];
+ * bond_active [n_bonds] is updated by the failure test; b_int [3n] and n_active [n] are
+ * written. Kernels run on `stream` (NULL: the default stream); the call does not wait.
+ * Limit: n <= 262144 points. The per-point coefficients live in a static device array of
+ * that size (8 MiB, held by every GPU that loads the library until the process exits);
+ * larger bodies are rejected with PD_ERR_ARG. All calls share that array: calls whose
+ * kernels may overlap on the GPU (other streams, other host threads) race. Every entry a
+ * call reads is written earlier in the same call, so nothing has to start at zero. The
+ * first call on each device looks up the array's device address with that device current;
+ * make that first call before any stream capture. Errors: pd_static_last_error(). */
+pd_status pd_osb_force_static(int64_t n, const double *ref_position, const double *position,
+                              const double *volume, const int64_t *bond_offsets,
+                              const int32_t *neighbors, const double *bond_length,
+                              const uint8_t *fail_permit, uint8_t *bond_active,
+                              const pd_point_params *params, int32_t kernel, double *b_int,
+                              int64_t *n_active, void *stream);
+
+/* Message of the last failed pd_osb_force_static call on this thread. */
+const char *pd_static_last_error(void);
+
 #ifdef __cplusplus
 }
 #endif

@@ -34,6 +34,7 @@ EXPORTS = (
     "pd_set_bcs", "pd_set_bc_values", "pd_stable_timestep", "pd_set_param_timesteps",
     "pd_force", "pd_run_vv", "pd_nan_step", "pd_run_vv_timed", "pd_autotune", "pd_set_mapping",
     "pd_set_graph", "pd_set_pipeline", "pd_info", "pd_launch_count", "pd_stream",
+    "pd_osb_force_static", "pd_static_last_error",
 )
 
 
@@ -82,6 +83,7 @@ def lib():
     vp, i64, i32, dbl, st = C.c_void_p, C.c_int64, C.c_int32, C.c_double, C.c_int32
     L.pd_last_error.restype = C.c_char_p
     L.pd_version.restype = C.c_char_p
+    L.pd_static_last_error.restype = C.c_char_p
     sig = {
         "pd_find_bonds": [i64, vp, vp, vp, i32, vp, vp, i64, vp, vp, vp, vp, vp, i32],
         "pd_create": [vp, vp],
@@ -106,6 +108,7 @@ def lib():
         "pd_info": [vp, vp, vp, vp],
         "pd_launch_count": [vp, vp],
         "pd_stream": [vp, vp],
+        "pd_osb_force_static": [i64] + [vp] * 8 + [vp, i32, vp, vp, vp],
     }
     for name, args in sig.items():
         f = getattr(L, name)

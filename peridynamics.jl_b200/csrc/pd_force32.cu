@@ -134,7 +134,7 @@ __global__ void PD_LB k_bb32(DevBody d, int kstep) {
 // dilatation theta, and c1 = 15 G / m, c2 = theta (3 K / m - c1 / 3) (:135-136)
 // -------------------------------------------------------------------------------------------
 template <int G>
-__global__ void PD_LB k_osb_a32(DevBody d, int kstep) {
+__global__ void PD_LB_A k_osb_a32(DevBody d, int kstep) {
   if (d.ctrl->err) return;
   PD_SLICE_LOOP(G) {
     PD_SLICE_SETUP

@@ -120,7 +120,7 @@ __device__ __forceinline__ void commit_row64(unsigned int* bits, long long word_
 // BB: bond_based.jl:125-180 (calc_failure! storing the bond length, force_density_point!)
 // -------------------------------------------------------------------------------------------
 template <int G, bool MULTI>
-__global__ void PD_LB k_bb64(DevBody d, int kstep) {
+__global__ void PD_LB64 k_bb64(DevBody d, int kstep) {
   if (d.ctrl->err) return;
   PD_SLICE_LOOP(G) {
     PD_SLICE_SETUP
@@ -174,7 +174,7 @@ __global__ void PD_LB k_bb64(DevBody d, int kstep) {
 // calc_weighted_volume (:176-189), calc_dilatation (:191-204), c1, c2 (:135-136)
 // -------------------------------------------------------------------------------------------
 template <int G, bool EXACT>
-__global__ void PD_LB k_osb_a64(DevBody d, int kstep) {
+__global__ void PD_LB64 k_osb_a64(DevBody d, int kstep) {
   if (d.ctrl->err) return;
   PD_SLICE_LOOP(G) {
     PD_SLICE_SETUP
@@ -265,7 +265,7 @@ __device__ __forceinline__ double osb_s64(const double4& co, const DevParam& Po,
 // OSB phase B: force_density_point! (ordinary_state_based.jl:128-174) in gather form
 // -------------------------------------------------------------------------------------------
 template <int G, bool EXACT, bool MULTI>
-__global__ void PD_LB k_osb_b64(DevBody d, int kstep) {
+__global__ void PD_LB64 k_osb_b64(DevBody d, int kstep) {
   if (d.ctrl->err) return;
   PD_SLICE_LOOP(G) {
     PD_SLICE_SETUP
@@ -346,7 +346,7 @@ __global__ void PD_LB k_osb_b64(DevBody d, int kstep) {
 // calc_first_piola_kirchhoff! (:216-224)
 // -------------------------------------------------------------------------------------------
 template <int G>
-__global__ void PD_LB k_c_a64(DevBody d, int kstep) {
+__global__ void PD_LB64 k_c_a64(DevBody d, int kstep) {
   if (d.ctrl->err) return;
   PD_SLICE_LOOP(G) {
     PD_SLICE_SETUP
@@ -434,7 +434,7 @@ __device__ __forceinline__ void c_bond_t64(const double* F, const double* PK, do
 }
 
 template <int G, bool EXACT>
-__global__ void PD_LB k_c_b64(DevBody d, int kstep) {
+__global__ void PD_LB64 k_c_b64(DevBody d, int kstep) {
   if (d.ctrl->err) return;
   PD_SLICE_LOOP(G) {
     PD_SLICE_SETUP

@@ -275,6 +275,16 @@ def main():
         pt_bytes = {"phase_a": 64 + 8 + 32 + 4 + 4, "phase_b": 64 + 8 + 32 + 24 + 4}[dom]
     alg_bytes = n_bonds * B_BOND[prec] + n_pts * pt_bytes
     achieved = alg_bytes / (dom_ms / 1e3) / 1e9
+    # DRAM traffic per launch from the committed ncu capture, scaled by the bond count
+    traffic = None
+    try:
+        with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
+            tb = json.load(f)["dram_bytes_per_bond"]
+        key = {"phase_a": f"{mat.lower()}_phase_a", "phase_b": f"{mat.lower()}_phase_b"}[dom]
+        if prec == "fp32" and key in tb:
+            traffic = tb[key] * n_bonds
+    except Exception:
+        traffic = None
     step_bytes = n_bonds * B_BOND[prec] + n_pts * (B_POINT[prec] + B_POINT_EXTRA[mat])
     step_ms = ms_max / args.steps
     step_achieved = step_bytes / (step_ms / 1e3) / 1e9
@@ -330,7 +340,8 @@ def main():
                        "parallelism": f"replicas x{world}"},
             "roofline": {"bound": "hbm", "kernel": f"{mat.lower()} force {dom}",
                          "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": None, "peak_kind": peak_kind,
+                         "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
+                         "traffic_source": "profiles/traffic.json (ncu, 1M-point case, scaled by bonds)",
                          "alg_bytes_per_launch": alg_bytes, "ms_per_launch": dom_ms},
             "roofline_step": {"achieved": step_achieved, "peak": peak, "frac": step_achieved / peak,
                               "alg_bytes_per_step": step_bytes,

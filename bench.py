@@ -122,9 +122,9 @@ class ClockSampler:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "error": str(e)}
 
 
-def cpu_baseline(cfg, threads, budget_s=20.0):
-    """The FP64 oracle (CPU restatement of the reference, OpenMP) on a sub-block of the same
-    lattice, spacing and parameters: bond-updates/s over whole Velocity Verlet steps."""
+def oracle_sample(cfg, threads):
+    """The FP64 oracle (CPU restatement of the reference, OpenMP) on a 64x64x40 sub-block of the
+    same lattice, spacing and parameters, initialised and ready to step."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
     nx, ny, nz, dx, mat, frac, vbc = CONFIGS[cfg]
@@ -141,6 +141,12 @@ def cpu_baseline(cfg, threads, budget_s=20.0):
     dt = b.stable_timestep(0.7)
     b.v[:, 1] = np.where(X[:, 1] > 0, vbc, -vbc)
     b.force_density(0.0, dt)
+    return b, dt, (sx, sy, sz)
+
+
+def cpu_baseline(cfg, threads, budget_s=20.0):
+    """bond-updates/s of the oracle sample over whole Velocity Verlet steps (bounded run)."""
+    b, dt, (sx, sy, sz) = oracle_sample(cfg, threads)
     steps, t0 = 0, time.perf_counter()
     while True:
         b.run_vv(steps + 1, 1, dt)
@@ -148,37 +154,38 @@ def cpu_baseline(cfg, threads, budget_s=20.0):
         el = time.perf_counter() - t0
         if el > budget_s or steps >= 50:
             break
-    O.set_threads(1)
     return {"value": b.n_bonds * steps / el, "unit": UNIT, "cores": threads, "kind": "port",
-            "sample": f"{sx}x{sy}x{sz} sub-block ({len(X)} points, {b.n_bonds} bonds) of the same "
+            "sample": f"{sx}x{sy}x{sz} sub-block ({b.n} points, {b.n_bonds} bonds) of the same "
                       f"lattice and parameters, {steps} FP64 VV steps in {el:.1f} s"}
 
 
 def run_reference(args, rank, world):
+    """The reference arm: the CPU restatement of the reference (Julia is not installed) on all
+    host threads; every step is one Velocity Verlet step of the bounded sample."""
     if rank != 0:
         return
     threads = os.cpu_count() or 1
-    vals = []
-    for _ in range(max(args.warmup, 0)):
-        pass
-    budget = 20.0 / max(args.steps, 1)
-    t = time.perf_counter()
-    res = None
-    for _ in range(args.steps):
-        res = cpu_baseline(args.config, threads, budget_s=max(budget, 2.0))
-        vals.append(res["value"])
-    el = time.perf_counter() - t
-    v = float(np.median(vals))
+    b, dt, (sx, sy, sz) = oracle_sample(args.config, threads)
+    for k in range(max(args.warmup, 0)):
+        b.run_vv(k + 1, 1, dt)
+    t0 = time.perf_counter()
+    for k in range(args.steps):
+        b.run_vv(args.warmup + k + 1, 1, dt)
+    el = time.perf_counter() - t0
+    v = b.n_bonds * args.steps / el
     nx, ny, nz, dx, mat, frac, vbc = CONFIGS[args.config]
+    sample = (f"{sx}x{sy}x{sz} sub-block ({b.n} points, {b.n_bonds} bonds) of the {args.config} "
+              f"lattice and parameters, {args.steps} FP64 VV steps in {el:.2f} s")
     line = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "impl": "reference",
+            "warmup": args.warmup, "ms_per_step": 1e3 * el / max(args.steps, 1),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "impl": "reference",
             "config": {"workload": args.config, "points": nx * ny * nz, "material": mat},
-            "cpu_baseline": dict(res, value=v),
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
+                             "sample": sample},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
             "note": "Julia is not installed: the reference arm is the CPU restatement of the "
-                    "reference (oracle/, FP64, OpenMP on all host threads)", "wall_s": el}
+                    "reference (oracle/, FP64, OpenMP on all host threads)"}
     print(json.dumps(line), flush=True)
 
 

@@ -69,6 +69,7 @@ typedef int32_t pd_status;
 #define PD_FIELD_BOND_ACTIVE 9    /* uint8[n_bonds] */
 #define PD_FIELD_DEFGRAD 10       /* double[9n] (CMaterial) */
 #define PD_FIELD_CAUCHY_STRESS 11 /* double[9n] (CMaterial) */
+#define PD_FIELD_N_NEIGHBORS 12   /* int64[n]: bonds per point (BondSystem.n_neighbors, bond_system.jl:48) */
 
 /* boundary-condition targets (velocity_bc! writes velocity_half, forcedensity_bc! b_ext:
  * src/physics/boundary_conditions.jl:422-435, 559-575) */
@@ -151,9 +152,12 @@ pd_status pd_create(const pd_body_desc *desc, pd_handle **out);
  * (desc->bond_offsets, neighbors, bond_length and fail_permit are ignored): the horizon of a
  * point is the delta of its parameter set, fp_point (n bytes, may be NULL = all 1) is the
  * failure permission per point (failure_permit!, fracture.jl:38-42) and the n_filters
- * filter-mode pre-cracks are point masks as in pd_find_bonds. */
-pd_status pd_create_search(const pd_body_desc *desc, const uint8_t *fp_point, int32_t n_filters,
-                           const uint8_t *filter_a, const uint8_t *filter_b, pd_handle **out);
+ * filter-mode pre-cracks are point masks as in pd_find_bonds. search_position (3n, may be
+ * NULL = desc->position) are the coordinates the search runs on: several independent bodies
+ * are kept apart there while the body stores their own coordinates. */
+pd_status pd_create_search(const pd_body_desc *desc, const double *search_position,
+                           const uint8_t *fp_point, int32_t n_filters, const uint8_t *filter_a,
+                           const uint8_t *filter_b, pd_handle **out);
 
 /* Frees all device memory of the handle. */
 pd_status pd_destroy(pd_handle *h);

@@ -560,27 +560,30 @@ extern "C" pd_status pd_find_bonds(int64_t n, const double* position, const doub
   return st;
 }
 
-extern "C" pd_status pd_create_search(const pd_body_desc* desc, const uint8_t* fp_point,
-                                      int32_t n_filters, const uint8_t* filter_a,
-                                      const uint8_t* filter_b, pd_handle** out) {
+extern "C" pd_status pd_create_search(const pd_body_desc* desc, const double* search_position,
+                                      const uint8_t* fp_point, int32_t n_filters,
+                                      const uint8_t* filter_a, const uint8_t* filter_b,
+                                      pd_handle** out) {
   PD_TRY(validate_desc(desc, false));
   const long long n = desc->n_points;
+  const double* spos = search_position ? search_position : desc->position;
   std::vector<double> delta(n);
   for (long long i = 0; i < n; i++) delta[i] = desc->params[desc->param_id ? desc->param_id[i] : 0].delta;
   double lo[3], hc;
   long long nc[3];
-  PD_TRY(search_grid(n, desc->position, delta.data(), lo, hc, nc));
+  PD_TRY(search_grid(n, spos, delta.data(), lo, hc, nc));
   std::vector<unsigned short> mask;
   if (n_filters > 0) PD_TRY(pack_masks(n, n_filters, filter_a, filter_b, mask));
   pd_handle* h = nullptr;
   pd_status st = begin_create(desc, out, &h);
   if (st != PD_OK) { if (h) pd_destroy(h); return st; }
-  double *dX = nullptr, *dd = nullptr;
+  double *dX = nullptr, *dXs = nullptr, *dd = nullptr;
   unsigned short* dm = nullptr;
   long long* doff = nullptr;
   unsigned char *dfp = nullptr, *dfpb = nullptr;
   std::vector<double> X(desc->position, desc->position + 3 * n);
   st = dalloc(h, &dX, 3 * n);
+  if (st == PD_OK && search_position) st = dalloc(h, &dXs, 3 * n);
   if (st == PD_OK) st = dalloc(h, &dd, n);
   if (st == PD_OK) st = dalloc(h, &doff, n + 1);
   if (st == PD_OK && n_filters > 0) st = dalloc(h, &dm, n);
@@ -589,13 +592,15 @@ extern "C" pd_status pd_create_search(const pd_body_desc* desc, const uint8_t* f
   std::vector<unsigned char> fp(n, 1);
   if (fp_point) std::copy(fp_point, fp_point + n, fp.begin());
   cudaError_t e = cudaMemcpy(dX, X.data(), sizeof(double) * 3 * n, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess && dXs) e = cudaMemcpy(dXs, search_position, sizeof(double) * 3 * n, cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMemcpy(dd, delta.data(), sizeof(double) * n, cudaMemcpyHostToDevice);
   if (e == cudaSuccess && dm) e = cudaMemcpy(dm, mask.data(), sizeof(unsigned short) * n, cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMemcpy(dfp, fp.data(), n, cudaMemcpyHostToDevice);
   int* dnbr = nullptr;
   long long nb = 0;
   int dup = 0;
-  if (e == cudaSuccess) e = device_find_bonds_grid(n, dX, dd, dm, lo, hc, nc, doff, &dnbr, &nb, &dup, h->stream);
+  if (e == cudaSuccess)
+    e = device_find_bonds_grid(n, dXs ? dXs : dX, dd, dm, lo, hc, nc, doff, &dnbr, &nb, &dup, h->stream);
   if (e != cudaSuccess) { pd_destroy(h); return fail(PD_ERR_CUDA, cudaGetErrorString(e)); }
   if (dup) { pd_destroy(h); return fail(PD_ERR_ARG, "point duplicate found!"); }
   h->allocs.push_back(dnbr);
@@ -607,7 +612,7 @@ extern "C" pd_status pd_create_search(const pd_body_desc* desc, const uint8_t* f
   if (st == PD_OK) st = dalloc(h, &dfpb, nb);
   if (st != PD_OK) { std::string m = g_err; pd_destroy(h); return fail(st, m); }
   if (nb) launch_bond_props(n, dX, dfp, doff, dnbr, dL, dfpb, h->stream);
-  dfree(h, dX); dfree(h, dd); dfree(h, dm); dfree(h, dfp);
+  dfree(h, dX); dfree(h, dXs); dfree(h, dd); dfree(h, dm); dfree(h, dfp);
   st = finish_create(h, dnbr, dL, dfpb);
   dfree(h, dnbr); dfree(h, dL); dfree(h, dfpb);
   if (st != PD_OK) { std::string m = g_err; pd_destroy(h); return fail(st, m); }
@@ -714,7 +719,7 @@ extern "C" pd_status pd_get_field(pd_handle* h, int32_t field, void* out, size_t
     case PD_FIELD_VELOCITY_HALF: case PD_FIELD_ACCELERATION: case PD_FIELD_B_INT:
     case PD_FIELD_B_EXT: need = sizeof(double) * 3 * n; break;
     case PD_FIELD_DAMAGE: need = sizeof(double) * n; break;
-    case PD_FIELD_N_ACTIVE_BONDS: need = sizeof(int64_t) * n; break;
+    case PD_FIELD_N_ACTIVE_BONDS: case PD_FIELD_N_NEIGHBORS: need = sizeof(int64_t) * n; break;
     case PD_FIELD_BOND_ACTIVE: need = nb; break;
     case PD_FIELD_DEFGRAD: case PD_FIELD_CAUCHY_STRESS:
       if (h->material != PD_MAT_CMAT) return fail(PD_ERR_ARG, "field only exists for CMaterial");
@@ -760,6 +765,13 @@ extern "C" pd_status pd_get_field(pd_handle* h, int32_t field, void* out, size_t
       PD_CUDA(cudaMemcpy(na.data(), h->d.n_active, sizeof(int) * n, cudaMemcpyDeviceToHost));
       int64_t* o = (int64_t*)out;
       for (long long i = 0; i < n; i++) o[i] = na[i];
+      break;
+    }
+    case PD_FIELD_N_NEIGHBORS: {
+      std::vector<long long> off(n + 1);
+      PD_CUDA(cudaMemcpy(off.data(), h->d.off, sizeof(long long) * (n + 1), cudaMemcpyDeviceToHost));
+      int64_t* o = (int64_t*)out;
+      for (long long i = 0; i < n; i++) o[i] = off[i + 1] - off[i];
       break;
     }
     case PD_FIELD_BOND_ACTIVE:

@@ -14,5 +14,6 @@ from .body import (Body, point_set, material, failure_permit, no_failure, veloci
                    forcedensity_bc, displacement_bc, velocity_databc, forcedensity_databc,
                    velocity_ic, precrack, uniform_box, get_dim)
 from .solver import VelocityVerlet, Job, DeviceBody, submit
+from .ensemble import Ensemble
 
 __version__ = "0.1.0"

@@ -23,7 +23,7 @@ KERNEL_CONST_ONE, KERNEL_LINEAR, KERNEL_CUBIC_BSPLINE = 0, 1, 2
 PREC_FP64, PREC_FP32_KAHAN = 0, 1
 # fields
 (F_POSITION, F_DISPLACEMENT, F_VELOCITY, F_VELOCITY_HALF, F_ACCELERATION, F_B_INT, F_B_EXT,
- F_DAMAGE, F_N_ACTIVE_BONDS, F_BOND_ACTIVE, F_DEFGRAD, F_CAUCHY_STRESS) = range(12)
+ F_DAMAGE, F_N_ACTIVE_BONDS, F_BOND_ACTIVE, F_DEFGRAD, F_CAUCHY_STRESS, F_N_NEIGHBORS) = range(13)
 BC_VELOCITY_HALF, BC_B_EXT = 0, 1
 BC_KIND_TIME, BC_KIND_POINT_TIME, BC_KIND_DATA = 0, 1, 2
 
@@ -87,7 +87,7 @@ def lib():
     sig = {
         "pd_find_bonds": [i64, vp, vp, vp, i32, vp, vp, i64, vp, vp, vp, vp, vp, i32],
         "pd_create": [vp, vp],
-        "pd_create_search": [vp, vp, i32, vp, vp, vp],
+        "pd_create_search": [vp, vp, vp, i32, vp, vp, vp],
         "pd_destroy": [vp],
         "pd_set_state": [vp, vp, vp, vp, vp, vp, vp, vp],
         "pd_break_bonds": [vp, vp, vp],

@@ -25,6 +25,7 @@ _FIELDS = {
     "n_active_bonds": (L.F_N_ACTIVE_BONDS, 1, np.int64),
     "bond_active": (L.F_BOND_ACTIVE, 0, np.uint8),
     "defgrad": (L.F_DEFGRAD, 9, np.float64), "cauchy_stress": (L.F_CAUCHY_STRESS, 9, np.float64),
+    "n_neighbors": (L.F_N_NEIGHBORS, 1, np.int64),
 }
 _PREC = {"fp64": L.PREC_FP64, "fp32": L.PREC_FP32_KAHAN}
 
@@ -75,7 +76,8 @@ class Job:
 class DeviceBody:
     """One body (all points in one chunk) resident on a CUDA device."""
 
-    def __init__(self, body: Body, precision="fp64", device=0, param_dt=None):
+    def __init__(self, body: Body, precision="fp64", device=0, param_dt=None,
+                 independent_params=False):
         if precision not in _PREC:
             raise ValueError("precision must be 'fp64' or 'fp32'")
         if np.any(body.params_map == 0):
@@ -101,7 +103,9 @@ class DeviceBody:
         desc.kernel = mat.kernel_id
         desc.cmodel = mat.model.id if isinstance(mat, CMaterial) else 0
         desc.precision = _PREC[precision]
-        desc.multi_params = 1 if len(body.point_params) > 1 else 0
+        # several parameter sets: the reference's ParameterHandler semantics (bond-averaged
+        # parameters), unless every bonded pair shares its set (independent specimens)
+        desc.multi_params = 1 if (len(body.point_params) > 1 and not independent_params) else 0
         desc.zem_cs = mat.zem.Cs if isinstance(mat, CMaterial) else 0.5
         desc.maxdmg = mat.maxdmg
         desc.device = device
@@ -113,8 +117,9 @@ class DeviceBody:
             fa[k, body.point_sets[a]] = 1
             fb[k, body.point_sets[b]] = 1
         fp = body.fail_permit.astype(np.uint8)
-        L.check(lib.pd_create_search(C.byref(desc), L.ptr(fp), nf, L.ptr(fa), L.ptr(fb),
-                                     C.byref(self.h)), "pd_create_search")
+        spos = getattr(body, "_search_pos", None)
+        L.check(lib.pd_create_search(C.byref(desc), L.ptr(spos), L.ptr(fp), nf, L.ptr(fa),
+                                     L.ptr(fb), C.byref(self.h)), "pd_create_search")
         self.n_bonds = self.info()[1]
         # apply_precracks! (predefined_cracks.jl:31-60): damage-mode cracks break bonds
         for a, b, filt_mode in body.point_sets_precracks:

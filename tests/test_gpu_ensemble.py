@@ -1,0 +1,76 @@
+"""Ensembles of specimens on one device against the oracle run on every specimen alone,
+each with its own CFL step (the reference runs such studies one job after the other)."""
+import numpy as np
+import pytest
+
+import oracle as O
+import pdcuda as pd
+from helpers import oracle_bcs, oracle_body
+
+pytestmark = pytest.mark.gpu
+
+
+def specimen(mat_factory, nx, ny, nz, E, rho, crack_frac, seed, dx=1e-3):
+    lx, ly, lz = nx * dx, ny * dx, nz * dx
+    pos, vol = pd.uniform_box(lx, ly, lz, dx, center=(lx / 2, ly / 2, lz / 2))
+    mat = mat_factory()
+    body = pd.Body(mat, pos, vol)
+    kw = dict(horizon=3.015 * dx, rho=rho, E=E, Gc=100.0)
+    if not isinstance(mat, pd.BBMaterial):
+        kw["nu"] = 0.3 if isinstance(mat, pd.CMaterial) else 0.25
+    pd.material(body, **kw)
+    a = crack_frac * lx
+    pd.point_set(body, "ca", where=lambda p: (p[1] <= ly / 2) & (p[0] < a))
+    pd.point_set(body, "cb", where=lambda p: (p[1] > ly / 2) & (p[0] < a))
+    pd.precrack(body, "ca", "cb")
+    pd.point_set(body, "left", where=lambda p: p[0] < 1.5 * dx)
+    pd.point_set(body, "right", where=lambda p: p[0] > lx - 1.5 * dx)
+    pd.velocity_bc(lambda t: -0.6, body, "left", "x")
+    pd.velocity_bc(lambda p, t: 0.6 + 10.0 * p[1] * t, body, "right", "x")
+    pd.velocity_ic(lambda p: 0.01 * p[2], body, "all_points", "z")
+    return body
+
+
+def build(mat_factory):
+    rng = np.random.default_rng(7)
+    bodies = []
+    for k in range(3):
+        nx, ny, nz = int(rng.integers(10, 16)), int(rng.integers(6, 10)), 3
+        bodies.append(specimen(mat_factory, nx, ny, nz, E=float(rng.uniform(50e9, 200e9)),
+                               rho=float(rng.uniform(2000, 8000)),
+                               crack_frac=float(rng.uniform(0.1, 0.4)), seed=k))
+    return bodies
+
+
+@pytest.mark.parametrize("name,factory", [("BB", pd.BBMaterial), ("OSB", pd.OSBMaterial),
+                                          ("C", lambda: pd.CMaterial(model=pd.NeoHooke()))])
+def test_ensemble_matches_specimens_run_alone(name, factory):
+    bodies = build(factory)
+    n_steps = 60
+    for prec, mapping in (("fp64", 0), ("fp32", 1)):
+        ens = pd.Ensemble(bodies, precision=prec, graph_steps=16 if prec == "fp32" else 0)
+        ens.dev.set_mapping(mapping)
+        ens.run(n_steps)
+        for k, b in enumerate(bodies):
+            ob = oracle_body(b)
+            dt = ob.stable_timestep(0.7)
+            assert ens.dt[k] == dt
+            ob.force_density(0.0, dt)
+            assert ob.run_vv(1, n_steps, dt, oracle_bcs(b, 1, n_steps, dt)) == 0
+            u = ens.field("displacement", k).T
+            if prec == "fp64":
+                if name == "C":
+                    assert np.abs(u - ob.u).max() <= 1e-10 * np.abs(ob.u).max()
+                else:
+                    assert np.array_equal(u, ob.u), (name, k)
+                assert np.array_equal(ens.field("bond_active", k), ob.bond_active[:ob.n_bonds])
+            else:
+                assert np.abs(u - ob.u).max() <= 1e-5 * np.abs(ob.u).max(), (name, k)
+        ens.close()
+
+
+def test_ensemble_rejects_mixed_materials():
+    a = specimen(pd.BBMaterial, 8, 6, 3, 70e9, 2700, 0.2, 0)
+    b = specimen(pd.OSBMaterial, 8, 6, 3, 70e9, 2700, 0.2, 0)
+    with pytest.raises(ValueError):
+        pd.Ensemble([a, b])

@@ -35,6 +35,7 @@ typedef int32_t pd_status;
 #define PD_ERR_TIMEOUT 4  /* a bounded device wait gave up */
 #define PD_ERR_OOM 5      /* device allocation failed */
 #define PD_ERR_UNSUPPORTED 6
+#define PD_ERR_NOCONV 7   /* Newton iterations exhausted (reference: ErrorException "did not converge") */
 
 /* material families (src/physics/bond_based.jl, ordinary_state_based.jl, correspondence.jl) */
 #define PD_MAT_BB 0
@@ -256,6 +257,85 @@ pd_status pd_launch_count(pd_handle *h, int64_t *count);
 
 /* The cudaStream_t of the handle, as an opaque pointer. */
 pd_status pd_stream(pd_handle *h, void **stream);
+
+/* ---------------------------------------------------------------------------------------
+ * Quasi-static Jacobian-free Newton-Krylov solve (src/time_solvers/newton_krylov.jl).
+ * Needs a PD_PREC_FP64 handle without fracture (validate_chunk_for_newton_krylov!,
+ * newton_krylov.jl:219-253). Position-dependent conditions f(p) are evaluated by the host at
+ * the reference positions and uploaded once; every load increment scales them by
+ * beta = n / n_steps on the device (apply_incr_boundary_conditions!,
+ * boundary_conditions.jl:148-163, 229-236).
+ * --------------------------------------------------------------------------------------- */
+
+/* Frechet step of the Jacobian-vector product */
+#define PD_NK_CENTRAL 0  /* eps = s cbrt(eps_mach)(|u|+1)/|v|, Jv = (F(u+eps v) - F(u-eps v))/(2 eps)
+                            (compute_perturbation / jacobian_vector_product!, newton_krylov.jl:504-567) */
+#define PD_NK_FORWARD 1  /* eps = s sqrt(eps_mach)|u|/|v| (|u| = 0: 1), Jv = (F(u+eps v) - F(u))/eps */
+
+/* preconditioner of the Krylov solve (right preconditioning, flexible GMRES) */
+#define PD_PC_NONE 0          /* plain restarted GMRES, as the reference (newton_krylov.jl:448-450) */
+#define PD_PC_BLOCK_JACOBI 1  /* z_i = P_i v_i, P_i = inverse of the 3x3 diagonal block J_ii (BB) */
+#define PD_PC_BLOCK_POLY 2    /* z = P (2v - K0 P v), K0 the small-strain bond stiffness (BB) */
+#define PD_PC_LEARNED_POLY 3  /* z = B (2v - K0 B v), B_i = P_i (I + D_i), D from pd_nk_set_corrections */
+#define PD_PC_LEARNED 4       /* z_i = B_i v_i */
+
+typedef struct pd_nk_condition {
+  int32_t field;           /* 0: displacement (constrains the dof), 1: b_ext */
+  int32_t dim;             /* 0, 1, 2 */
+  int64_t n_points;
+  const int32_t *points;   /* 0-based point indices */
+  const double *values;    /* f(p) at the reference position of every point (full load) */
+} pd_nk_condition;
+
+typedef struct pd_nk_params {
+  int32_t maxiter;              /* Newton iterations per increment (NewtonKrylov maxiter) */
+  double tol;                   /* Newton tolerance on ||r||, r = (b_int + b_ext) V */
+  int32_t tol_relative;         /* 0: ||r|| < tol (reference); 1: ||r|| <= tol ||r_first|| */
+  double perturbation_scale;    /* s */
+  int32_t frechet;              /* PD_NK_* */
+  int32_t gmres_maxiter;        /* Arnoldi steps per linear solve */
+  double gmres_reltol, gmres_abstol;
+  int32_t gmres_restart;        /* Krylov basis size between restarts */
+  int32_t precond;              /* PD_PC_* */
+} pd_nk_params;
+
+typedef struct pd_nk_stats {
+  int32_t newton_iters;     /* residual evaluations of the increment */
+  int32_t converged;
+  int64_t gmres_iters;      /* Arnoldi steps (Jacobian-vector products inside the bases) */
+  int64_t matvecs;          /* all Jacobian-vector products, restart residuals included */
+  int64_t force_evals;      /* force-density evaluations of the increment */
+  int64_t precond_applies;
+  double residual_first;    /* ||r|| at the first Newton iteration of the increment */
+  double residual;          /* ||r|| at the last Newton iteration */
+} pd_nk_stats;
+
+/* Conditions of the solve (pos_single_dim_bcs of the body, condition_handler.jl:5-36):
+ * replaces earlier ones. Displacement conditions define the constrained dofs. */
+pd_status pd_nk_set_conditions(pd_handle *h, int32_t n, const pd_nk_condition *conds);
+
+/* One load increment, newton_krylov_step! (newton_krylov.jl:298-332): apply the conditions at
+ * beta, then Newton iterations of force, residual and a (F)GMRES solve of J du = -r.
+ * `step` is the increment number used in NaN reports. PD_ERR_NOCONV when maxiter Newton
+ * iterations did not reach the tolerance (stats are filled either way). */
+pd_status pd_nk_step(pd_handle *h, int64_t step, double beta, const pd_nk_params *p,
+                     pd_nk_stats *stats);
+
+/* Learned corrections D (9 floats per point, 3x3 column-major) of PD_PC_LEARNED*; NULL
+ * clears them. Host pointer. No counterpart in the reference. */
+pd_status pd_nk_set_corrections(pd_handle *h, const float *D);
+
+/* Operators at the current state, for tests: op 0 out = J v (the Frechet product of p),
+ * 1 out = K0 v, 2 out = M v (the preconditioner p->precond), 3 out = residual r (v unused).
+ * Host vectors of 3n doubles. */
+pd_status pd_nk_apply(pd_handle *h, int32_t op, const pd_nk_params *p, const double *v,
+                      double *out);
+
+/* Record the unit residual direction of every (re)start of the Krylov solves, FP32, up to
+ * `capacity` vectors (0 stops and frees); pd_nk_recorded returns how many are held. The
+ * recorded vectors are the training data of the learned preconditioner. */
+pd_status pd_nk_record(pd_handle *h, int64_t capacity);
+pd_status pd_nk_recorded(pd_handle *h, int64_t *n);
 
 /* Ordinary state-based force evaluation that allocates no device memory. No counterpart in
  * the reference: it exists for callers that must not let the library allocate GPU memory --

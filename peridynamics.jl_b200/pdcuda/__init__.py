@@ -15,5 +15,7 @@ from .body import (Body, point_set, material, failure_permit, no_failure, veloci
                    velocity_ic, precrack, uniform_box, get_dim)
 from .solver import VelocityVerlet, Job, DeviceBody, submit
 from .ensemble import Ensemble
+from .newton_krylov import NewtonKrylov
+from ._lib import NotConvergedError
 
 __version__ = "0.1.0"

@@ -15,7 +15,8 @@ LIB_PATH = os.path.join(_HERE, "libpdcuda.so")
 _LIB = None
 
 # status codes
-PD_OK, PD_ERR_ARG, PD_ERR_CUDA, PD_ERR_NAN, PD_ERR_TIMEOUT, PD_ERR_OOM, PD_ERR_UNSUPPORTED = range(7)
+(PD_OK, PD_ERR_ARG, PD_ERR_CUDA, PD_ERR_NAN, PD_ERR_TIMEOUT, PD_ERR_OOM, PD_ERR_UNSUPPORTED,
+ PD_ERR_NOCONV) = range(8)
 # materials, models, kernels, precision
 MAT_BB, MAT_OSB, MAT_CMAT = 0, 1, 2
 CM_SVK, CM_NEOHOOKE, CM_NEOHOOKE_PENALTY = 0, 1, 2
@@ -26,6 +27,10 @@ PREC_FP64, PREC_FP32_KAHAN = 0, 1
  F_DAMAGE, F_N_ACTIVE_BONDS, F_BOND_ACTIVE, F_DEFGRAD, F_CAUCHY_STRESS, F_N_NEIGHBORS) = range(13)
 BC_VELOCITY_HALF, BC_B_EXT = 0, 1
 BC_KIND_TIME, BC_KIND_POINT_TIME, BC_KIND_DATA = 0, 1, 2
+# Newton-Krylov: Frechet rules, preconditioners, condition fields
+NK_CENTRAL, NK_FORWARD = 0, 1
+PC_NONE, PC_BLOCK_JACOBI, PC_BLOCK_POLY, PC_LEARNED_POLY, PC_LEARNED = range(5)
+NKC_DISPLACEMENT, NKC_B_EXT = 0, 1
 
 # every symbol that include/pdcuda.h declares
 EXPORTS = (
@@ -34,6 +39,8 @@ EXPORTS = (
     "pd_set_bcs", "pd_set_bc_values", "pd_stable_timestep", "pd_set_param_timesteps",
     "pd_force", "pd_run_vv", "pd_nan_step", "pd_run_vv_timed", "pd_autotune", "pd_set_mapping",
     "pd_set_graph", "pd_set_pipeline", "pd_info", "pd_launch_count", "pd_stream",
+    "pd_nk_set_conditions", "pd_nk_step", "pd_nk_set_corrections", "pd_nk_apply",
+    "pd_nk_record", "pd_nk_recorded",
     "pd_osb_force_static", "pd_static_last_error",
 )
 
@@ -58,6 +65,29 @@ class BCDesc(C.Structure):
                 ("n_points", C.c_int32), ("points", C.c_void_p), ("data", C.c_void_p)]
 
 
+class NKCondition(C.Structure):
+    _fields_ = [("field", C.c_int32), ("dim", C.c_int32), ("n_points", C.c_int64),
+                ("points", C.c_void_p), ("values", C.c_void_p)]
+
+
+class NKParams(C.Structure):
+    _fields_ = [("maxiter", C.c_int32), ("tol", C.c_double), ("tol_relative", C.c_int32),
+                ("perturbation_scale", C.c_double), ("frechet", C.c_int32),
+                ("gmres_maxiter", C.c_int32), ("gmres_reltol", C.c_double),
+                ("gmres_abstol", C.c_double), ("gmres_restart", C.c_int32),
+                ("precond", C.c_int32)]
+
+
+class NKStats(C.Structure):
+    _fields_ = [("newton_iters", C.c_int32), ("converged", C.c_int32),
+                ("gmres_iters", C.c_int64), ("matvecs", C.c_int64),
+                ("force_evals", C.c_int64), ("precond_applies", C.c_int64),
+                ("residual_first", C.c_double), ("residual", C.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 class NaNError(RuntimeError):
     """NaN values in the internal force density (the reference's NaNError, errors.jl:98-114)."""
 
@@ -70,6 +100,10 @@ class NaNError(RuntimeError):
 
 class PDCudaError(RuntimeError):
     pass
+
+
+class NotConvergedError(RuntimeError):
+    """Newton iterations exhausted (the reference's ErrorException, newton_krylov.jl:317-324)."""
 
 
 def lib():
@@ -109,6 +143,12 @@ def lib():
         "pd_launch_count": [vp, vp],
         "pd_stream": [vp, vp],
         "pd_osb_force_static": [i64] + [vp] * 8 + [vp, i32, vp, vp, vp],
+        "pd_nk_set_conditions": [vp, i32, vp],
+        "pd_nk_step": [vp, i64, dbl, vp, vp],
+        "pd_nk_set_corrections": [vp, vp],
+        "pd_nk_apply": [vp, i32, vp, vp, vp],
+        "pd_nk_record": [vp, i64],
+        "pd_nk_recorded": [vp, vp],
     }
     for name, args in sig.items():
         f = getattr(L, name)
@@ -131,6 +171,8 @@ def check(status, what=""):
         raise ValueError(f"{what}: {msg}" if what else msg)
     if status == PD_ERR_NAN:
         raise NaNError(None, None)
+    if status == PD_ERR_NOCONV:
+        raise NotConvergedError(msg)
     raise PDCudaError(f"{what}: {msg} (status {status})" if what else f"{msg} (status {status})")
 
 

@@ -307,10 +307,30 @@ class DeviceBody:
             pass
 
 
+def check_conditions_applicable(body, solver):
+    """check_conditions_applicable (discretization/body.jl:287-302): displacement conditions
+    are applied only by the Newton-Krylov solver."""
+    if body.pos_single_dim_bcs:
+        raise ValueError(
+            "conditions of this body cannot be applied by the specified time solver!\n"
+            f"The body has {len(body.pos_single_dim_bcs)} prescribed displacement condition(s) "
+            "defined with\n`displacement_bc!`. These are only applied by the `NewtonKrylov` "
+            f"solver, but the job uses\na `{type(solver).__name__}` solver, which would ignore "
+            "them completely.\nUse a `NewtonKrylov` solver, or specify the load with "
+            "`velocity_bc!` or\n`forcedensity_bc!` instead.\n")
+
+
 def submit(job: Job, quiet=True):
     """submit (core/submit.jl:14-29) on the device: builds the device body, computes the CFL
     step (velocity_verlet.jl:103-163), runs initialize! (a force evaluation at t = 0) and
     solve! (velocity_verlet.jl:165-179). Returns the DeviceBody with the final state."""
+    from .newton_krylov import NewtonKrylov, solve as nk_solve
+    if isinstance(job.solver, NewtonKrylov):
+        dev = DeviceBody(job.body, precision=job.precision, device=job.device)
+        if job.mapping is not None:
+            dev.set_mapping(*job.mapping)
+        return nk_solve(dev, job.solver, job.export, job.freq if job.export is not None else 0)
+    check_conditions_applicable(job.body, job.solver)
     vv = job.solver
     dev = DeviceBody(job.body, precision=job.precision, device=job.device)
     if job.mapping is not None:

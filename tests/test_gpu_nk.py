@@ -1,0 +1,144 @@
+"""Device Newton-Krylov solve against the CPU restatement (oracle/jfnk.py).
+
+The Krylov arithmetic is not pinned by the reference; the device solve is judged by the
+true nonlinear residual it reaches, by the converged displacement against the oracle's and,
+for the operators, by their values against the oracle's at the same state.
+"""
+import numpy as np
+import pytest
+
+import pdcuda as pd
+from pdcuda import newton_krylov as nkm
+from helpers import oracle_body
+from jfnk import OracleNK
+from test_nk_host import (EBAR, FBAR, HBAR, LBAR, WBAR, nk_conditions, small_beam,
+                          tension_bar)
+
+pytestmark = pytest.mark.gpu
+
+
+def rel(a, b):
+    return np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300)
+
+
+def test_uniform_tension_bar_device_matches_oracle_and_analytic():
+    body = tension_bar(1 / 30)
+    nk = pd.NewtonKrylov(steps=5, tol=1e-3, maxiter=50)
+    dev = pd.submit(pd.Job(body, nk))
+    u = dev.field("displacement").T
+    right = body.point_sets["right"]
+    exact = FBAR / (EBAR * WBAR * HBAR) * LBAR
+    assert abs(u[right, 0].mean() - exact) / exact < 0.02
+    assert all(s["converged"] and s["residual"] < 1e-3 for s in nk.stats)
+    ob = oracle_body(body)
+    onk = OracleNK(ob, nk_conditions(body))
+    for n in range(1, 6):
+        assert onk.step(n, 5, maxiter=50, tol=1e-3)[0]
+    # both solves end below the same absolute residual: the states agree to the solution's
+    # sensitivity to a residual of 1e-3 N (displacements ~1e-4 m)
+    assert np.max(np.abs(u - ob.u)) <= 1e-6 * np.max(np.abs(ob.u))
+
+
+def deformed_beam(dev, ob, seed=3):
+    """Put the same small random displacement into the device body and the oracle."""
+    rng = np.random.default_rng(seed)
+    u = rng.uniform(-1, 1, (dev.n, 3)) * 1e-6
+    dev.set_state(displacement=u, position=dev.body._pos + u)
+    ob.u[:] = u
+    ob.pos[:] = ob.X + u
+    return u
+
+
+@pytest.mark.parametrize("frechet,tol", [("central", 1e-7), ("forward", 1e-4)])
+def test_jacobian_vector_product_matches_oracle(frechet, tol):
+    body = small_beam()
+    dev = pd.DeviceBody(body, precision="fp64")
+    dev.set_mapping(0)  # serial order: the same force arithmetic as the oracle
+    nk = pd.NewtonKrylov(steps=1, frechet=frechet)
+    nkm.setup(dev, nk)
+    ob = oracle_body(body)
+    onk = OracleNK(ob, nk_conditions(body))
+    deformed_beam(dev, ob)
+    v = np.random.default_rng(5).standard_normal(3 * dev.n)
+    v[onk.cmask] = 0.0
+    got = nkm.apply_operator(dev, nk, "jv", v)
+    want = onk.jv(v, frechet)
+    assert rel(got, want) <= tol
+    # the residual operator equals the oracle's
+    assert rel(nkm.apply_operator(dev, nk, "residual"), onk.residual()) <= 1e-14
+
+
+def test_k0_and_preconditioners_match_oracle():
+    body = small_beam()
+    dev = pd.DeviceBody(body, precision="fp64")
+    ob = oracle_body(body)
+    onk = OracleNK(ob, nk_conditions(body))
+    nk = pd.NewtonKrylov(steps=1)
+    nkm.setup(dev, nk)
+    deformed_beam(dev, ob)
+    v = np.random.default_rng(7).standard_normal(3 * dev.n)
+    v[onk.cmask] = 0.0
+    assert rel(nkm.apply_operator(dev, nk, "k0", v), onk.k0(v)) <= 1e-5
+    # K0 is the tangent at the reference configuration: close to the Frechet product
+    assert rel(onk.k0(v), onk.jv(v, "central")) <= 1e-2
+    for pc, tol in (("block_jacobi", 1e-6), ("block_poly", 1e-5)):
+        nk.preconditioner = pc
+        assert rel(nkm.apply_operator(dev, nk, "precond", v), onk.precond(pc, v)) <= tol
+    D = np.random.default_rng(9).uniform(-0.2, 0.2, (dev.n, 3, 3))
+    nk.preconditioner, nk.corrections = "learned_poly", D.transpose(0, 2, 1).reshape(dev.n, 9)
+    nkm.setup(dev, nk)
+    assert rel(nkm.apply_operator(dev, nk, "precond", v), onk.precond("learned_poly", v, D=D)) <= 1e-5
+
+
+@pytest.mark.parametrize("precond", ["none", "block_jacobi", "block_poly"])
+def test_beam_solve_reaches_relative_residual(precond):
+    body = small_beam()
+    nk = pd.NewtonKrylov(steps=2, tol=1e-8, tol_mode="relative", frechet="forward",
+                         gmres_restart=50, gmres_maxiter=5000, maxiter=20, preconditioner=precond)
+    dev = pd.submit(pd.Job(body, nk))
+    for s in nk.stats:
+        assert s["converged"] and s["residual"] <= 1e-8 * s["residual_first"]
+    ob = oracle_body(body)
+    onk = OracleNK(ob, nk_conditions(body))
+    for n in (1, 2):
+        assert onk.step(n, 2, maxiter=20, tol=1e-8, tol_relative=True, rule="forward",
+                        restart=50, gmres_maxiter=5000, precond=precond)[0]
+    u = dev.field("displacement").T
+    assert np.max(np.abs(u - ob.u)) <= 1e-6 * np.max(np.abs(ob.u))
+    # the true residual of the device state, evaluated again
+    r = nkm.apply_operator(dev, nk, "residual")
+    assert np.linalg.norm(r) <= 1e-8 * nk.stats[-1]["residual_first"] * 1.0001
+
+
+def test_polynomial_needs_fewer_krylov_steps_and_zero_corrections_are_neutral():
+    body = small_beam(nx=40, ny=8, nz=6)
+    its = {}
+    for pc in ("block_jacobi", "block_poly", "learned_poly"):
+        nk = pd.NewtonKrylov(steps=1, tol=1e-8, tol_mode="relative", frechet="forward",
+                             gmres_restart=50, gmres_maxiter=5000, maxiter=20, preconditioner=pc,
+                             corrections=np.zeros((body.n_points, 9), np.float32))
+        pd.submit(pd.Job(body, nk))
+        its[pc] = sum(s["gmres_iters"] for s in nk.stats)
+    assert its["block_poly"] < its["block_jacobi"]
+    assert its["learned_poly"] == its["block_poly"]
+
+
+def test_errors_and_recording():
+    body = small_beam()
+    with pytest.raises(ValueError, match="fp64"):
+        pd.submit(pd.Job(body, pd.NewtonKrylov(steps=1), precision="fp32"))
+    nk = pd.NewtonKrylov(steps=1, maxiter=2, tol=1e-30)
+    with pytest.raises(pd.NotConvergedError, match="did not converge"):
+        pd.submit(pd.Job(body, nk))
+    dev = pd.DeviceBody(body, precision="fp64")
+    nkm.record(dev, 4)
+    nk = pd.NewtonKrylov(steps=1, tol=1e-8, tol_mode="relative", frechet="forward",
+                         gmres_restart=10, gmres_maxiter=5000, preconditioner="block_jacobi")
+    nkm.solve(dev, nk)
+    assert nkm.recorded(dev) == 4
+    osb = pd.Body(pd.OSBMaterial(), *pd.uniform_box(0.01, 0.004, 0.004, 1e-3))
+    pd.material(osb, horizon=3.015e-3, rho=2700.0, E=70e9, nu=0.25)
+    pd.point_set(osb, "a", [0])
+    pd.displacement_bc(lambda p: 0.0, osb, "a", "x")
+    with pytest.raises(ValueError, match="bond-based"):
+        pd.submit(pd.Job(osb, pd.NewtonKrylov(steps=1, preconditioner="block_jacobi")))

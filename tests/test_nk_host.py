@@ -1,0 +1,168 @@
+"""Newton-Krylov host logic and the CPU restatement of the solver (no GPU).
+
+Mirrors test/unit/time_solvers/test_newton_krylov.jl (constructor, newton_krylov_check,
+validation) and pins the oracle on the reference's analytic uniform-tension run
+(test/simulation/test_analytic_solutions.jl:7-66, 86-91).
+"""
+import numpy as np
+import pytest
+
+import pdcuda as pd
+from pdcuda.newton_krylov import validate_body
+from pdcuda.solver import check_conditions_applicable
+from helpers import oracle_body
+from jfnk import OracleNK
+
+
+def test_newtonkrylov_wrong_input():
+    bad = [dict(time=1, steps=10), dict(), dict(steps=10, stepsize=0), dict(steps=10, stepsize=-0.1)]
+    for k, v in (("maxiter", 0), ("maxiter", -1), ("tol", 0), ("tol", -1e-8),
+                 ("gmres_reltol", 0), ("gmres_reltol", -1e-4), ("gmres_abstol", 0),
+                 ("gmres_abstol", -1e-8), ("gmres_maxiter", 0), ("gmres_maxiter", -10),
+                 ("gmres_restart", 0), ("gmres_restart", -10), ("perturbation_scale", 0),
+                 ("perturbation_scale", -1)):
+        bad.append({"steps": 10, "stepsize": 0.1, k: v})
+    for kw in bad:
+        with pytest.raises(ValueError):
+            pd.NewtonKrylov(**kw)
+
+
+def test_newtonkrylov_fields():
+    nr = pd.NewtonKrylov(steps=100)
+    assert (nr.end_time, nr.n_steps, nr.dt, nr.maxiter, nr.tol) == (100, 100, 1.0, 100, 1e-4)
+    assert (nr.perturbation_scale, nr.gmres_maxiter, nr.gmres_reltol, nr.gmres_abstol) == \
+        (1.0, 200, 1e-4, 1e-8)
+    nr = pd.NewtonKrylov(time=1.0, stepsize=0.01)
+    assert (nr.end_time, nr.n_steps, nr.dt) == (1.0, 100, 0.01)
+    nr = pd.NewtonKrylov(time=1.0, stepsize=0.02, maxiter=75, tol=1e-6, perturbation_scale=2.0,
+                         gmres_maxiter=150, gmres_reltol=1e-5, gmres_abstol=1e-9)
+    assert (nr.n_steps, nr.dt, nr.maxiter, nr.tol, nr.perturbation_scale) == (50, 0.02, 75, 1e-6, 2.0)
+    assert "NewtonKrylov(end_time=1.0, n_steps=50, Δt=0.02, maxiter=75" in repr(nr)
+
+
+def test_newton_krylov_check():
+    for field, label in (("end_time", "end_time"), ("n_steps", "n_steps"), ("dt", "Δt"),
+                         ("maxiter", "maxiter"), ("tol", "tol")):
+        nr = pd.NewtonKrylov(steps=10, stepsize=0.1)
+        setattr(nr, field, -1)
+        with pytest.raises(RuntimeError, match=f"`{label}` of NewtonKrylov smaller than zero"):
+            nr.check()
+    nr = pd.NewtonKrylov(steps=10, stepsize=0.1)
+    nr.perturbation_scale = 0
+    with pytest.raises(RuntimeError, match="must be larger than zero"):
+        nr.check()
+
+
+def _tetra(**kw):
+    pos = np.array([[0.0, 1.0, 0.0, 0.0], [0.0, 0.0, 1.0, 0.0], [0.0, 0.0, 0.0, 1.0]])
+    body = pd.Body(pd.BBMaterial(), pos, np.array([1.1, 1.2, 1.3, 1.4]))
+    pd.material(body, horizon=2, rho=1, E=1, **kw)
+    pd.point_set(body, "top", [1])
+    return body
+
+
+def test_validation_rejects_time_conditions_and_fracture():
+    body = _tetra()
+    pd.forcedensity_bc(lambda t: 0.1, body, "top", "y")
+    with pytest.raises(ValueError, match="position-dependent"):
+        validate_body(body)
+    body = _tetra(Gc=1.0)
+    pd.displacement_bc(lambda p: 0.1, body, "top", "y")
+    with pytest.raises(ValueError, match="does not support damage or fracture"):
+        validate_body(body)
+    body = _tetra()
+    pd.displacement_bc(lambda p: 0.1, body, "top", "y")
+    validate_body(body)
+    # a displacement condition is ignored by Velocity Verlet: rejected before any device work
+    with pytest.raises(ValueError, match="only applied by the `NewtonKrylov`"):
+        check_conditions_applicable(body, pd.VelocityVerlet(steps=10))
+
+
+# -- the uniform-tension bar of the reference's analytic test ---------------------------------
+LBAR, WBAR, HBAR, FBAR, EBAR = 1.0, 0.1, 0.1, 2e6, 200e9
+
+
+def tension_bar(dx):
+    """`newton_bar` of test_analytic_solutions.jl: CMaterial with ZEMSilling(Cs=0.5), left end
+    fixed by displacement conditions, the force F spread over the right layer as b_ext."""
+    pos, vol = pd.uniform_box(LBAR + 3 * dx, WBAR, HBAR, dx, center=(-1.5 * dx, 0, 0))
+    body = pd.Body(pd.CMaterial(zem=pd.ZEMSilling(Cs=0.5)), pos, vol)
+    pd.material(body, horizon=3.015 * dx, rho=7850.0, E=EBAR, nu=0.25)
+    pd.point_set(body, "left", where=lambda p: p[0] < -LBAR / 2)
+    pd.point_set(body, "right", where=lambda p: p[0] > LBAR / 2 - dx)
+    b_right = FBAR / vol[body.point_sets["right"]].sum()
+    for d in ("x", "y", "z"):
+        pd.displacement_bc(lambda p: 0.0, body, "left", d)
+    pd.forcedensity_bc(lambda p: b_right, body, "right", "x")
+    return body
+
+
+def nk_conditions(body):
+    out = []
+    for c in body.pos_single_dim_bcs:
+        pts = np.asarray(body.point_sets[c.point_set])
+        out.append((c.field, c.dim, pts, [float(c.fun(body._pos[i])) for i in pts]))
+    return out
+
+
+def test_oracle_uniform_tension_matches_analytic_band():
+    body = tension_bar(1 / 30)
+    assert body.n_points == 297
+    ob = oracle_body(body)
+    nk = OracleNK(ob, nk_conditions(body))
+    for n in range(1, 6):
+        conv, *_ = nk.step(n, 5, maxiter=50, tol=1e-3)
+        assert conv
+    right = body.point_sets["right"]
+    elong = ob.u[right, 0].mean()
+    exact = FBAR / (EBAR * WBAR * HBAR) * LBAR
+    # the reference's band: measured 0.5 %, asserted < 2 %
+    assert abs(elong - exact) / exact < 0.02
+
+
+def small_beam(nx=24, ny=6, nz=4, dx=1e-3, load=-0.05e-3):
+    """A three-point-bending beam: bottom support lines near both ends fixed, the mid-span
+    top line pushed down."""
+    pos, vol = pd.uniform_box(nx * dx, ny * dx, nz * dx, dx)
+    body = pd.Body(pd.BBMaterial(), pos, vol)
+    pd.material(body, horizon=3.015 * dx, rho=2700.0, E=70e9)
+    x, y = pos[0], pos[1]
+    xl, xr = x.min() + 2 * dx, x.max() - 2 * dx
+    sup = np.nonzero((np.abs(y - y.min()) < dx / 2) &
+                     ((np.abs(x - xl) < dx / 2) | (np.abs(x - xr) < dx / 2)))[0]
+    top = np.nonzero((np.abs(y - y.max()) < dx / 2) & (np.abs(x) <= dx / 2 + 1e-12))[0]
+    pd.point_set(body, "support", sup)
+    pd.point_set(body, "load", top)
+    for d in ("x", "y", "z"):
+        pd.displacement_bc(lambda p: 0.0, body, "support", d)
+    pd.displacement_bc(lambda p: load, body, "load", "y")
+    return body
+
+
+@pytest.mark.parametrize("precond", ["none", "block_jacobi", "block_poly"])
+def test_oracle_beam_preconditioners_reach_relative_tolerance(precond):
+    body = small_beam()
+    ob = oracle_body(body)
+    nk = OracleNK(ob, nk_conditions(body))
+    for n in (1, 2):
+        conv, it, gm, first, last = nk.step(n, 2, maxiter=20, tol=1e-8, tol_relative=True,
+                                            rule="forward", restart=50, gmres_maxiter=5000,
+                                            precond=precond)
+        assert conv and last <= 1e-8 * first
+    # the converged state does not depend on the preconditioner
+    ref = getattr(test_oracle_beam_preconditioners_reach_relative_tolerance, "u", None)
+    if ref is None:
+        test_oracle_beam_preconditioners_reach_relative_tolerance.u = ob.u.copy()
+    else:
+        assert np.max(np.abs(ob.u - ref)) <= 1e-6 * np.max(np.abs(ref))
+
+
+def test_oracle_block_poly_is_a_better_preconditioner():
+    body = small_beam()
+    counts = {}
+    for precond in ("none", "block_jacobi", "block_poly"):
+        nk = OracleNK(oracle_body(body), nk_conditions(body))
+        _, _, gm, _, _ = nk.step(1, 1, maxiter=20, tol=1e-8, tol_relative=True, rule="forward",
+                                 restart=50, gmres_maxiter=5000, precond=precond)
+        counts[precond] = gm
+    assert counts["block_poly"] < counts["block_jacobi"] <= counts["none"]

@@ -32,6 +32,8 @@ UNIT = "bond-updates/s"
 CONFIGS = {
     # name: (nx, ny, nz, dx, material, random broken fraction, bc velocity)
     "osb8m": (400, 200, 100, 5e-4, "OSB", 0.05, 1.0),
+    # quasi-static Newton-Krylov: bond-based three-point bending beam (x span, y height)
+    "jfnk500k": (250, 50, 40, 1e-3, "BB", 0.0, 0.0),
     "osb1m": (200, 100, 50, 1e-3, "OSB", 0.0, 0.6),
     "bb1m": (200, 100, 50, 1e-3, "BB", 0.0, 0.6),
     "c1m": (200, 100, 50, 1e-3, "C", 0.0, 0.6),
@@ -189,6 +191,99 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+JFNK_WEIGHTS = os.path.join(ROOT, "peridynamics.jl_b200", "pdcuda", "weights", "beam_block_pc.npz")
+JFNK_ARMS = ("block_jacobi", "block_poly", "learned_poly")
+
+
+def jfnk_compare(device, increments, n_steps=20, weights=JFNK_WEIGHTS, arms=JFNK_ARMS):
+    """The 500k-point three-point-bending beam (250 x 50 x 40 points, dx = 1 mm, E = 70 GPa,
+    no fracture, mid-span line pushed 0.5 mm down over n_steps load increments): wall time
+    of the first `increments` increments to a 1e-8 relative nonlinear residual per increment,
+    FGMRES(50) with the forward Frechet step sqrt(eps) |u| / |v|, for each preconditioner.
+    The learned arm's time includes the network's inference on the beam."""
+    import pdcuda as pd
+    from pdcuda import mpnn
+    from pdcuda import newton_krylov as nkm
+    from pdcuda.train_preconditioner import bending_beam
+    body = bending_beam(250, 50, 40)
+    out = {}
+    for pc in arms:
+        net = None
+        if pc.startswith("learned"):
+            if not os.path.exists(weights):
+                out[pc] = None
+                continue
+            net = mpnn.BlockPreconditionerNet.load(weights, device=device)
+        dev = pd.DeviceBody(body, precision="fp64", device=device)
+        dev.autotune()
+        nk = pd.NewtonKrylov(steps=n_steps, tol=1e-8, tol_mode="relative", frechet="forward",
+                             gmres_restart=50, gmres_maxiter=50000, maxiter=20,
+                             preconditioner=pc, corrections=net)
+        t0 = time.perf_counter()
+        nkm.setup(dev, nk)
+        for n in range(1, increments + 1):
+            nkm.step(dev, nk, n)
+        t = time.perf_counter() - t0
+        st = nk.stats
+        out[pc] = {"s": t, "increments": increments,
+                   "newton_iters": sum(x["newton_iters"] for x in st),
+                   "gmres_iters": sum(x["gmres_iters"] for x in st),
+                   "force_evals": sum(x["force_evals"] for x in st),
+                   "max_rel_residual": max(x["residual"] / x["residual_first"] for x in st),
+                   "ms_per_krylov_step": 1e3 * t / max(1, sum(x["gmres_iters"] for x in st))}
+        dev.close()
+        if net is not None:
+            net.close()
+    bj = out.get("block_jacobi")
+    for pc in arms:
+        if out.get(pc) and bj:
+            out[pc]["speedup_vs_block_jacobi"] = bj["s"] / out[pc]["s"]
+    return {"workload": f"bond-based beam 250x50x40 points (500k), first {increments} of "
+                        f"{n_steps} load increments, 1e-8 relative residual, FGMRES(50)",
+            "points": body.n_points, "arms": out}
+
+
+def run_jfnk(args, rank, world):
+    """--config jfnk500k: every load increment of the quasi-static solve, per preconditioner."""
+    if rank != 0:
+        return
+    import torch  # noqa: F401  (device plumbing only)
+    res = jfnk_compare(int(os.environ.get("LOCAL_RANK", "0")), args.jfnk_increments)
+    arms = res["arms"]
+    best = arms.get("learned_poly") or arms.get("block_poly")
+    cpu = None
+    if not args.no_cpu:
+        cpu = jfnk_cpu_baseline(arms["block_jacobi"]["force_evals"])
+    line = {"metric": "JFNK wall time to 1e-8 relative residual (learned preconditioner)",
+            "value": best["s"], "unit": "s", "n_gpus": 1, "steps": args.jfnk_increments,
+            "warmup": 0, "higher_is_better": False, "scaling": "none", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic", "config": {"workload": res["workload"],
+                                                            "points": res["points"]},
+            "arms": arms, "cpu_baseline": cpu}
+    print(json.dumps(line), flush=True)
+
+
+def jfnk_cpu_baseline(force_evals, budget_s=20.0):
+    """The oracle's FP64 force evaluation (all host threads) on the same beam, timed on a few
+    evaluations; the projection multiplies by the block-Jacobi arm's force-evaluation count."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle as O
+    from helpers import oracle_body
+    from pdcuda.train_preconditioner import bending_beam
+    threads = os.cpu_count() or 1
+    O.set_threads(threads)
+    ob = oracle_body(bending_beam(250, 50, 40))
+    k, t0 = 0, time.perf_counter()
+    while k < 2 or (time.perf_counter() - t0 < budget_s and k < 20):
+        ob.force_density()
+        k += 1
+    per = (time.perf_counter() - t0) / k
+    return {"value": per, "unit": "s per force evaluation", "cores": threads, "kind": "port",
+            "sample": f"{k} FP64 force evaluations of the 500k-point beam",
+            "projected_block_jacobi_s": per * force_evals}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -200,6 +295,9 @@ def main():
     ap.add_argument("--fp64-steps", type=int, default=-1, help="steps of the FP64 comparison (0 = skip)")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--graph", type=int, default=0)
+    ap.add_argument("--jfnk-increments", type=int, default=-1,
+                    help="load increments of the JFNK comparison (default: 20 with --config "
+                         "jfnk500k, 2 in the default run, 0 = skip)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
 
@@ -214,6 +312,22 @@ def main():
         import datetime
         tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
         dist = tdist
+
+    if args.config == "jfnk500k":
+        if args.jfnk_increments < 0:
+            args.jfnk_increments = 20
+        if args.impl == "reference":
+            if rank == 0:
+                print(json.dumps({"impl": "reference", "unavailable": "the reference arm times the "
+                                  "explicit-dynamics path; the JFNK CPU baseline is in cpu_baseline"}))
+        else:
+            run_jfnk(args, rank, world)
+        if dist:
+            dist.barrier()
+            dist.destroy_process_group()
+        return
+    if args.jfnk_increments < 0:
+        args.jfnk_increments = 2
 
     if args.impl == "reference":
         run_reference(args, rank, world)
@@ -332,6 +446,10 @@ def main():
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_baseline(args.config, os.cpu_count() or 1)
+    dev.close()
+    jfnk = None
+    if rank == 0 and world == 1 and args.jfnk_increments > 0:
+        jfnk = jfnk_compare(local, args.jfnk_increments)
 
     if rank == 0:
         line = {
@@ -357,9 +475,9 @@ def main():
             "fp64_value": fp64, "fp32_over_fp64": (value / fp64) if fp64 else None,
             "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "gpu_launches": launches, "clocks": clocks, "cpu_baseline": cpu,
+            "jfnk": jfnk,
         }
         print(json.dumps(line), flush=True)
-    dev.close()
     if dist:
         dist.barrier()
         dist.destroy_process_group()

@@ -337,6 +337,36 @@ pd_status pd_nk_apply(pd_handle *h, int32_t op, const pd_nk_params *p, const dou
 pd_status pd_nk_record(pd_handle *h, int64_t capacity);
 pd_status pd_nk_recorded(pd_handle *h, int64_t *n);
 
+/* ---------------------------------------------------------------------------------------
+ * Learned block preconditioner of the Newton-Krylov solve. No counterpart in the reference
+ * (its Newton systems are solved by plain GMRES): a two-layer message-passing network over
+ * the bond graph (16 point features, hidden width 64, BF16 tensor-core layers with FP32
+ * accumulation) predicts per-point corrections D_i of the block-Jacobi blocks,
+ * B_i = P_i (I + D_i), used by PD_PC_LEARNED(_POLY). Bond-based bodies; the body's
+ * conditions (pd_nk_set_conditions) must be set before pd_mpnn_infer / pd_mpnn_loss_grad.
+ * --------------------------------------------------------------------------------------- */
+typedef struct pd_mpnn pd_mpnn;
+#define PD_MPNN_N_PARAMS 18185  /* W0[64x16] b0[64] W1[64x128] b1 W2[64x128] b2 Wo[9x64] bo[9] */
+
+pd_status pd_mpnn_create(int32_t device, pd_mpnn **out);
+pd_status pd_mpnn_destroy(pd_mpnn *net);
+/* FP32 parameter vector (row-major weights, layout above); setting resets the optimiser. */
+pd_status pd_mpnn_set_params(pd_mpnn *net, const float *theta);
+pd_status pd_mpnn_get_params(pd_mpnn *net, float *theta);
+/* Runs the network on the body and installs its corrections D (as pd_nk_set_corrections).
+ * Optional host outputs: features [n x 16], D [n x 9]. */
+pd_status pd_mpnn_infer(pd_mpnn *net, pd_handle *h, float *features, float *D);
+/* Training loss L = sum_s w_s ||(I - alpha_s K0 B)^2 r_s||^2 / S over recorded residual
+ * directions (rec_ids into pd_nk_record's store; alpha = w = 1) and host samples
+ * [n_host x 3n] (FP32; alpha = host_alpha, w = host_weight); the gradient is added to the
+ * network's accumulator (copied to grad [PD_MPNN_N_PARAMS] when not NULL). */
+pd_status pd_mpnn_loss_grad(pd_mpnn *net, pd_handle *h, int32_t n_rec, const int64_t *rec_ids,
+                            int32_t n_host, const float *host_samples, double host_alpha,
+                            double host_weight, double *loss, float *grad);
+pd_status pd_mpnn_zero_grad(pd_mpnn *net);
+/* One Adam step (beta 0.9 / 0.999) with the accumulated gradient, which is then cleared. */
+pd_status pd_mpnn_adam(pd_mpnn *net, float lr);
+
 /* Ordinary state-based force evaluation that allocates no device memory. No counterpart in
  * the reference: it exists for callers that must not let the library allocate GPU memory --
  * a host that owns every device buffer through its own pool, a time loop that must not stall

@@ -1,0 +1,801 @@
+// pd_mpnn.cu -- the learned block preconditioner of the Newton-Krylov solve: a two-layer
+// message-passing network over the bond graph that predicts per-point 3x3 corrections D_i of
+// the block-Jacobi blocks, B_i = P_i (I + D_i). No counterpart in the reference (its Newton
+// systems are solved by plain GMRES, newton_krylov.jl:448-450).
+//
+// Network (per point i; mean over the active bonds of i):
+//   x_i  16 features (k_feat_*)            h0 = relu(W0 x + b0)                     64
+//   m_l = mean_j h_{l-1,j};  h_l = h_{l-1} + relu(W_l [h_{l-1}; m_l] + b_l),  l = 1, 2
+//   D_i = Wo h2 + bo                       (9 = a 3x3 block, column-major)
+// The dense layers are BF16 tensor-core products (mma.sync m16n8k16, FP32 accumulation) with
+// the weights staged in shared memory; activations are stored as BF16, the aggregation sums
+// in FP32. Training minimises, over unit sample vectors r (recorded Krylov residual
+// directions and random probes),
+//   L = sum_s w_s || (I - alpha_s K0 B)^2 r_s ||^2 / S,
+// the residual after one application of the block polynomial M = B (2 I - K0 B) with the
+// small-strain stiffness K0 standing in for J (alpha = 1). Samples of the fast end of the
+// spectrum are given alpha = 1 / tau: their optimum is then an eigenvalue tau of K0 B (just
+// below 2, where the polynomial still maps it to a positive one) rather than 1, so the loss
+// rewards scaling the slow end up as far as the fast end allows; their weight w makes the
+// quartic, flat near its minimum, hold the fast end there. dL/dD needs four K0 sweeps per
+// sample; the backward pass runs the same products transposed and reduces the weight gradients over the
+// points per block, then in a fixed order (deterministic). Adam updates FP32 master weights.
+//
+// The dense layers move 16-128 BF16 values per point against 64 outputs: at 500k points a
+// layer is ~8 GFLOP, microseconds on the tensor cores; the network's time goes to the
+// neighbour gathers of the aggregation, which is why mma.sync fragments loaded straight from
+// shared memory are used here rather than a TMEM-resident tcgen05 pipeline.
+#include <cuda_bf16.h>
+
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "pd_nk.h"
+
+namespace pd {
+
+constexpr int NF = 16, HID = 64, NO = 9, NOP = 16;
+// parameter offsets (FP32 master vector)
+constexpr int O_W0 = 0, O_B0 = O_W0 + HID * NF, O_W1 = O_B0 + HID, O_B1 = O_W1 + HID * 2 * HID,
+              O_W2 = O_B1 + HID, O_B2 = O_W2 + HID * 2 * HID, O_WO = O_B2 + HID,
+              O_BO = O_WO + NO * HID, N_PARAMS = O_BO + NO;
+constexpr int WG_BLOCKS = 296;  // blocks of the weight-gradient reductions (148 SMs x 2)
+
+using bf16 = __nv_bfloat16;
+
+__device__ __forceinline__ void mma16816(float* c, const uint32_t* a, const uint32_t* b) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, "
+      "{%8,%9}, {%0,%1,%2,%3};\n"
+      : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
+
+__device__ __forceinline__ uint32_t pack2(float lo, float hi) {
+  __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
+  return *reinterpret_cast<uint32_t*>(&v);
+}
+__device__ __forceinline__ float2 unpack2(uint32_t u) {
+  __nv_bfloat162 v = *reinterpret_cast<__nv_bfloat162*>(&u);
+  return __bfloat1622float2(v);
+}
+__device__ __forceinline__ float bfr(float x) { return __bfloat162float(__float2bfloat16_rn(x)); }
+
+// ------------------------------------------------------------------------------------------
+// features (reference configuration; same definitions as oracle/mpnn.py)
+// ------------------------------------------------------------------------------------------
+// raw[12 i ..]: 3/tr-scaled K_ii (6), tr, n, sum xi (3), delta; cnt[i] = active bonds
+__global__ void k_feat_raw(DevBody d, float* __restrict__ raw, float* __restrict__ cnt,
+                           unsigned int* __restrict__ maxes) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= d.n) return;
+  const int nn = (int)(d.off[i + 1] - d.off[i]);
+  const double4 Xi = d.X0[i];
+  const DevParam& Pi = d.params[d.meta[i] & META_PID_MASK];
+  double K[6] = {0, 0, 0, 0, 0, 0}, sx = 0, sy = 0, sz = 0;
+  int na = 0;
+  for (int k = 0; k < nn; k++) {
+    const long long b = bond_slot(d, i, k);
+    if (!bond_bit(d.bits, b)) continue;
+    const int j = d.nbr[b];
+    const double4 Xj = d.X0[j];
+    const double L = fabs(d.len64[b]);
+    const double c = d.multi ? 0.5 * (Pi.bc + d.params[d.meta[j] & META_PID_MASK].bc) : Pi.bc;
+    const double kk = c * Xj.w * Xi.w / (L * L * L);
+    const double ex = Xj.x - Xi.x, ey = Xj.y - Xi.y, ez = Xj.z - Xi.z;
+    K[0] += kk * ex * ex; K[1] += kk * ey * ey; K[2] += kk * ez * ez;
+    K[3] += kk * ex * ey; K[4] += kk * ex * ez; K[5] += kk * ey * ez;
+    sx += ex; sy += ey; sz += ez;
+    na++;
+  }
+  const double t = K[0] + K[1] + K[2];
+  const double s = t > 0 ? 3.0 / t : 0.0;
+  float* o = raw + 12 * i;
+  o[0] = (float)(s * K[0] - 1); o[1] = (float)(s * K[1] - 1); o[2] = (float)(s * K[2] - 1);
+  o[3] = (float)(s * K[3]); o[4] = (float)(s * K[4]); o[5] = (float)(s * K[5]);
+  o[6] = (float)t; o[7] = (float)na;
+  o[8] = (float)sx; o[9] = (float)sy; o[10] = (float)sz; o[11] = (float)Pi.delta;
+  cnt[i] = (float)na;
+  atomicMax(maxes, __float_as_uint((float)t));  // non-negative floats order as integers
+  atomicMax(maxes + 1, (unsigned)na);
+}
+
+__global__ void k_feat_fin(long long n, const float* __restrict__ raw,
+                           const unsigned char* __restrict__ cmask,
+                           const unsigned int* __restrict__ maxes, bf16* __restrict__ x,
+                           float* __restrict__ xf) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float tmax = __uint_as_float(maxes[0]);
+  const float nmax = (float)maxes[1];
+  const float* r = raw + 12 * i;
+  float f[NF];
+  for (int k = 0; k < 6; k++) f[k] = r[k];
+  f[6] = tmax > 0 ? (float)((double)r[6] / (double)tmax - 1.0) : -1.f;
+  f[7] = nmax > 0 ? (float)((double)r[7] / (double)nmax - 1.0) : -1.f;
+  for (int k = 0; k < 3; k++) f[8 + k] = cmask ? (float)cmask[3 * i + k] : 0.f;
+  const double sc = nmax > 0 ? 1.0 / ((double)nmax * (double)r[11]) : 0.0;
+  const double a = r[8] * sc, b = r[9] * sc, c = r[10] * sc;
+  f[11] = (float)a; f[12] = (float)b; f[13] = (float)c;
+  f[14] = (float)sqrt(a * a + b * b + c * c);
+  f[15] = 0.f;
+  for (int k = 0; k < NF; k++) {
+    x[NF * i + k] = __float2bfloat16_rn(f[k]);
+    if (xf) xf[NF * i + k] = f[k];
+  }
+}
+
+// ------------------------------------------------------------------------------------------
+// dense layers: Y[rows x NOUT] = [in0 | in1][rows x KIN] W^T, W row-major [NOUT][KIN] (BF16)
+// one warp = 16 rows; MODE selects the epilogue
+// ------------------------------------------------------------------------------------------
+enum { D_RELU = 0, D_RESID = 1, D_OUT = 2, D_BWD = 3, D_BWD_OUT = 4 };
+
+struct DenseArgs {
+  long long n;
+  const bf16* in0; int ld0;     // first input block (columns [0, ld0))
+  const bf16* in1;              // second block (columns [ld0, KIN)), row stride KIN - ld0
+  const bf16* W;                // [NOUT][KIN]
+  const float* bias;            // [NOUT] (may be shorter: D_OUT uses 9)
+  const bf16* resid;            // D_RESID: h_{l-1}
+  bf16* out_a;                  // D_RESID: relu(z)
+  bf16* out_h;                  // D_RELU: relu(z); D_RESID: h_{l-1} + relu(z)
+  float* out_f;                 // D_OUT: D [n x 9]; D_BWD*: dh accumulate [n x 64]
+  float* out_s;                 // D_BWD: s = dm / n_i [n x 64]
+  const float* cnt;             // D_BWD: active bonds per point
+};
+
+template <int KIN>
+__device__ __forceinline__ uint32_t lda(const DenseArgs& a, long long row, int col) {
+  if (row >= a.n) return 0u;
+  if (col < a.ld0) return *reinterpret_cast<const uint32_t*>(a.in0 + row * a.ld0 + col);
+  return *reinterpret_cast<const uint32_t*>(a.in1 + row * (KIN - a.ld0) + (col - a.ld0));
+}
+
+template <int KIN, int NOUT, int MODE>
+__global__ void __launch_bounds__(128) k_dense(DenseArgs a) {
+  __shared__ __align__(16) bf16 Ws[NOUT * KIN];
+  for (int q = threadIdx.x; q < NOUT * KIN / 2; q += blockDim.x)
+    reinterpret_cast<uint32_t*>(Ws)[q] = reinterpret_cast<const uint32_t*>(a.W)[q];
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+  for (long long tile = (long long)blockIdx.x * 4 + warp; tile * 16 < a.n;
+       tile += (long long)gridDim.x * 4) {
+    const long long r0 = tile * 16;
+    float acc[NOUT / 8][4];
+#pragma unroll
+    for (int nt = 0; nt < NOUT / 8; nt++) acc[nt][0] = acc[nt][1] = acc[nt][2] = acc[nt][3] = 0.f;
+#pragma unroll
+    for (int k0 = 0; k0 < KIN; k0 += 16) {
+      uint32_t af[4];
+      af[0] = lda<KIN>(a, r0 + g, k0 + 2 * t);
+      af[1] = lda<KIN>(a, r0 + g + 8, k0 + 2 * t);
+      af[2] = lda<KIN>(a, r0 + g, k0 + 2 * t + 8);
+      af[3] = lda<KIN>(a, r0 + g + 8, k0 + 2 * t + 8);
+#pragma unroll
+      for (int nt = 0; nt < NOUT / 8; nt++) {
+        uint32_t bfm[2];
+        bfm[0] = *reinterpret_cast<const uint32_t*>(Ws + (nt * 8 + g) * KIN + k0 + 2 * t);
+        bfm[1] = *reinterpret_cast<const uint32_t*>(Ws + (nt * 8 + g) * KIN + k0 + 2 * t + 8);
+        mma16816(acc[nt], af, bfm);
+      }
+    }
+#pragma unroll
+    for (int nt = 0; nt < NOUT / 8; nt++) {
+      const int c = nt * 8 + 2 * t;
+#pragma unroll
+      for (int hf = 0; hf < 2; hf++) {
+        const long long row = r0 + g + 8 * hf;
+        if (row >= a.n) continue;
+        const float z0 = acc[nt][2 * hf], z1 = acc[nt][2 * hf + 1];
+        if (MODE == D_RELU) {
+          const float b0 = a.bias[c], b1 = a.bias[c + 1];
+          *reinterpret_cast<uint32_t*>(a.out_h + row * NOUT + c) =
+              pack2(fmaxf(z0 + b0, 0.f), fmaxf(z1 + b1, 0.f));
+        } else if (MODE == D_RESID) {
+          const float b0 = a.bias[c], b1 = a.bias[c + 1];
+          const float a0 = bfr(fmaxf(z0 + b0, 0.f)), a1 = bfr(fmaxf(z1 + b1, 0.f));
+          const float2 hp = unpack2(*reinterpret_cast<const uint32_t*>(a.resid + row * NOUT + c));
+          *reinterpret_cast<uint32_t*>(a.out_a + row * NOUT + c) = pack2(a0, a1);
+          *reinterpret_cast<uint32_t*>(a.out_h + row * NOUT + c) = pack2(hp.x + a0, hp.y + a1);
+        } else if (MODE == D_OUT) {
+          if (c < NO) a.out_f[row * NO + c] = z0 + a.bias[c];
+          if (c + 1 < NO) a.out_f[row * NO + c + 1] = z1 + a.bias[c + 1];
+        } else if (MODE == D_BWD_OUT) {
+          a.out_f[row * HID + c] = z0;
+          a.out_f[row * HID + c + 1] = z1;
+        } else {  // D_BWD: columns [0, 64) add to dh, [64, 128) become s = dm / n
+          if (c < HID) {
+            a.out_f[row * HID + c] += z0;
+            a.out_f[row * HID + c + 1] += z1;
+          } else {
+            const float nn = a.cnt[row];
+            a.out_s[row * HID + c - HID] = nn > 0 ? z0 / nn : 0.f;
+            a.out_s[row * HID + c - HID + 1] = nn > 0 ? z1 / nn : 0.f;
+          }
+        }
+      }
+    }
+  }
+}
+
+// ------------------------------------------------------------------------------------------
+// aggregation over the bonds: one warp per point, lane l owns features 2l, 2l+1
+// ------------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_agg_mean(DevBody d, const bf16* __restrict__ h,
+                                                 const float* __restrict__ cnt,
+                                                 bf16* __restrict__ m) {
+  const long long i = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (i >= d.n) return;
+  const int nn = (int)(d.off[i + 1] - d.off[i]);
+  float s0 = 0.f, s1 = 0.f;
+  for (int k = 0; k < nn; k++) {
+    const long long b = bond_slot(d, i, k);
+    if (!bond_bit(d.bits, b)) continue;
+    const int j = __ldg(d.nbr + b);
+    const float2 v = unpack2(__ldg(reinterpret_cast<const unsigned int*>(h + (long long)j * HID) + lane));
+    s0 += v.x;
+    s1 += v.y;
+  }
+  const float c = cnt[i];
+  *reinterpret_cast<uint32_t*>(m + i * HID + 2 * lane) =
+      c > 0 ? pack2(s0 / c, s1 / c) : pack2(0.f, 0.f);
+}
+
+// dh_j += sum over the active bonds j -> i of s_i (the bond graph is symmetric)
+__global__ void __launch_bounds__(256) k_agg_adj(DevBody d, const float* __restrict__ s,
+                                                float* __restrict__ dh) {
+  const long long j = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (j >= d.n) return;
+  const int nn = (int)(d.off[j + 1] - d.off[j]);
+  float a0 = 0.f, a1 = 0.f;
+  for (int k = 0; k < nn; k++) {
+    const long long b = bond_slot(d, j, k);
+    if (!bond_bit(d.bits, b)) continue;
+    const int i = __ldg(d.nbr + b);
+    const float2 v = __ldg(reinterpret_cast<const float2*>(s + (long long)i * HID) + lane);
+    a0 += v.x;
+    a1 += v.y;
+  }
+  float2* o = reinterpret_cast<float2*>(dh + j * HID) + lane;
+  float2 cur = *o;
+  cur.x += a0;
+  cur.y += a1;
+  *o = cur;
+}
+
+// dz = bf16(dh * (act > 0))
+__global__ void k_relu_grad(long long n, const float* __restrict__ dh, const bf16* __restrict__ act,
+                            bf16* __restrict__ dz) {
+  const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= n * HID) return;
+  dz[q] = __float2bfloat16_rn(__bfloat162float(act[q]) > 0.f ? dh[q] : 0.f);
+}
+
+// ------------------------------------------------------------------------------------------
+// weight gradients: part[block][MO x KIN] = sum over the block's rows of dz^T X (tensor cores)
+// X = [in0 | in1] as in DenseArgs; dz row-major [rows x MO]
+// ------------------------------------------------------------------------------------------
+template <int MO, int KIN>
+__global__ void __launch_bounds__(256) k_wgrad(long long n, const bf16* __restrict__ dz,
+                                              const bf16* __restrict__ in0, int ld0,
+                                              const bf16* __restrict__ in1,
+                                              float* __restrict__ part) {
+  __shared__ __align__(16) bf16 dzT[MO * 16];
+  __shared__ __align__(16) bf16 xT[KIN * 16];
+  constexpr int NT = KIN / 8, TILES = (MO / 16) * NT, PER = TILES / 8;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+  float acc[PER][4];
+#pragma unroll
+  for (int q = 0; q < PER; q++) acc[q][0] = acc[q][1] = acc[q][2] = acc[q][3] = 0.f;
+  const bf16 zero = __float2bfloat16_rn(0.f);
+  for (long long r0 = (long long)blockIdx.x * 16; r0 < n; r0 += (long long)gridDim.x * 16) {
+    for (int e = threadIdx.x; e < 16 * MO; e += blockDim.x) {
+      const int rr = e / MO, o = e % MO;
+      dzT[o * 16 + rr] = r0 + rr < n ? dz[(r0 + rr) * MO + o] : zero;
+    }
+    for (int e = threadIdx.x; e < 16 * KIN; e += blockDim.x) {
+      const int rr = e / KIN, k = e % KIN;
+      bf16 v = zero;
+      if (r0 + rr < n) v = k < ld0 ? in0[(r0 + rr) * ld0 + k] : in1[(r0 + rr) * (KIN - ld0) + k - ld0];
+      xT[k * 16 + rr] = v;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < PER; q++) {
+      const int tile = warp * PER + q, mt = tile / NT, nt = tile % NT;
+      uint32_t af[4], bfm[2];
+      af[0] = *reinterpret_cast<const uint32_t*>(dzT + (mt * 16 + g) * 16 + 2 * t);
+      af[1] = *reinterpret_cast<const uint32_t*>(dzT + (mt * 16 + g + 8) * 16 + 2 * t);
+      af[2] = *reinterpret_cast<const uint32_t*>(dzT + (mt * 16 + g) * 16 + 2 * t + 8);
+      af[3] = *reinterpret_cast<const uint32_t*>(dzT + (mt * 16 + g + 8) * 16 + 2 * t + 8);
+      bfm[0] = *reinterpret_cast<const uint32_t*>(xT + (nt * 8 + g) * 16 + 2 * t);
+      bfm[1] = *reinterpret_cast<const uint32_t*>(xT + (nt * 8 + g) * 16 + 2 * t + 8);
+      mma16816(acc[q], af, bfm);
+    }
+    __syncthreads();
+  }
+  float* out = part + (long long)blockIdx.x * MO * KIN;
+#pragma unroll
+  for (int q = 0; q < PER; q++) {
+    const int tile = warp * PER + q, mt = tile / NT, nt = tile % NT;
+    const int r = mt * 16 + g, c = nt * 8 + 2 * t;
+    out[r * KIN + c] = acc[q][0];
+    out[r * KIN + c + 1] = acc[q][1];
+    out[(r + 8) * KIN + c] = acc[q][2];
+    out[(r + 8) * KIN + c + 1] = acc[q][3];
+  }
+}
+
+// grad[off + e] += sum_b part[b][e] for e < rows_used * KIN (fixed order)
+__global__ void k_wgrad_reduce(const float* __restrict__ part, int nb, int size, int used,
+                               float* __restrict__ grad) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= used) return;
+  float s = 0.f;
+  for (int b = 0; b < nb; b++) s += part[(long long)b * size + e];
+  grad[e] += s;
+}
+
+// column sums of dz (bf16 values) or of dD (fp32): per-block partials, then reduced
+template <typename T>
+__global__ void k_colsum(long long n, int cols, const T* __restrict__ v, float* __restrict__ part) {
+  // block b sums rows b, b + nb, ...; thread c < cols owns column c
+  const int c = threadIdx.x;
+  if (c >= cols) return;
+  float s = 0.f;
+  for (long long r = blockIdx.x; r < n; r += gridDim.x) s += (float)v[r * cols + c];
+  part[(long long)blockIdx.x * cols + c] = s;
+}
+
+// ------------------------------------------------------------------------------------------
+// loss kernels
+// ------------------------------------------------------------------------------------------
+__global__ void k_f32_to_f64(double* dst, const float* src, long long n) {
+  const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q < n) dst[q] = (double)src[q];
+}
+
+// z_i = (I + D_i)^T P_i^T w_i (no masking: the adjoint of masked-row blocks)
+__global__ void k_blockT(long long n, const float* __restrict__ P, const float* __restrict__ D,
+                         const double* __restrict__ w, double* __restrict__ z) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float* Pi = P + 9 * i;
+  const float* Di = D + 9 * i;
+  double t[3];
+  for (int c = 0; c < 3; c++)  // (P^T w)_c = sum_r P[r, c] w_r
+    t[c] = (Pi[3 * c] * w[3 * i] + Pi[3 * c + 1] * w[3 * i + 1]) + Pi[3 * c + 2] * w[3 * i + 2];
+  for (int c = 0; c < 3; c++)
+    z[3 * i + c] = t[c] + ((Di[3 * c] * t[0] + Di[3 * c + 1] * t[1]) + Di[3 * c + 2] * t[2]);
+}
+
+// y = a - alpha b, with constrained entries 0 when cmask is given
+__global__ void k_sub(long long m, const double* a, double alpha, const double* b,
+                      const unsigned char* cmask, double* y) {
+  const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= m) return;
+  const double v = a[q] - alpha * b[q];
+  y[q] = (cmask && cmask[q]) ? 0.0 : v;
+}
+
+__global__ void k_scalev(long long m, double alpha, double* v) {
+  const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q < m) v[q] *= alpha;
+}
+
+// G_i += f (g1_i r_i^T + w_i y1_i^T) on the free rows (column-major 3x3)
+__global__ void k_acc_G(long long n, const double* __restrict__ g1, const double* __restrict__ r,
+                        const double* __restrict__ w, const double* __restrict__ y1,
+                        const unsigned char* __restrict__ cmask, double f, double* __restrict__ G) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  for (int a = 0; a < 3; a++) {
+    if (cmask[3 * i + a]) continue;
+    for (int b = 0; b < 3; b++)
+      G[9 * i + a + 3 * b] += f * (g1[3 * i + a] * r[3 * i + b] + w[3 * i + a] * y1[3 * i + b]);
+  }
+}
+
+// dD_i = P_i^T G_i (fp32, column-major) and its bf16 copy padded to 16 columns
+__global__ void k_dD(long long n, const float* __restrict__ P, const double* __restrict__ G,
+                     float* __restrict__ dD, bf16* __restrict__ dDb) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float* Pi = P + 9 * i;
+  const double* Gi = G + 9 * i;
+  for (int c = 0; c < 3; c++)
+    for (int r = 0; r < 3; r++) {
+      // (P^T G)[r, c] = sum_k P[k, r] G[k, c]
+      const double v = (Pi[3 * r] * Gi[3 * c] + Pi[3 * r + 1] * Gi[3 * c + 1]) +
+                       Pi[3 * r + 2] * Gi[3 * c + 2];
+      dD[9 * i + r + 3 * c] = (float)v;
+      dDb[NOP * i + r + 3 * c] = __float2bfloat16_rn((float)v);
+    }
+  for (int k = NO; k < NOP; k++) dDb[NOP * i + k] = __float2bfloat16_rn(0.f);
+}
+
+// ------------------------------------------------------------------------------------------
+// parameters: bf16 copies (W and W^T) and Adam
+// ------------------------------------------------------------------------------------------
+__global__ void k_weights(const float* __restrict__ th, bf16* W0, bf16* W1, bf16* W2, bf16* Wo,
+                          bf16* W1T, bf16* W2T, bf16* WoT) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e < HID * NF) W0[e] = __float2bfloat16_rn(th[O_W0 + e]);
+  if (e < HID * 2 * HID) {
+    const int o = e / (2 * HID), k = e % (2 * HID);
+    W1[e] = __float2bfloat16_rn(th[O_W1 + e]);
+    W2[e] = __float2bfloat16_rn(th[O_W2 + e]);
+    W1T[k * HID + o] = W1[e];
+    W2T[k * HID + o] = W2[e];
+  }
+  if (e < NOP * HID) {
+    const int o = e / HID, k = e % HID;
+    const bf16 v = __float2bfloat16_rn(o < NO ? th[O_WO + o * HID + k] : 0.f);
+    Wo[e] = v;
+    WoT[k * NOP + o] = v;
+  }
+}
+
+__global__ void k_adam(float* th, float* grad, float* m, float* v, int n, float lr, float b1,
+                       float b2, float eps, float c1, float c2) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= n) return;
+  const float g = grad[e];
+  const float mm = b1 * m[e] + (1 - b1) * g;
+  const float vv = b2 * v[e] + (1 - b2) * g * g;
+  m[e] = mm;
+  v[e] = vv;
+  th[e] -= lr * (mm / c1) / (sqrtf(vv / c2) + eps);
+  grad[e] = 0.f;
+}
+
+}  // namespace pd
+
+using namespace pd;
+
+// ------------------------------------------------------------------------------------------
+// host side
+// ------------------------------------------------------------------------------------------
+struct pd_mpnn {
+  int device = 0;
+  std::vector<void*> allocs;
+  float *theta = nullptr, *grad = nullptr, *am = nullptr, *av = nullptr;
+  bf16 *W0 = nullptr, *W1 = nullptr, *W2 = nullptr, *Wo = nullptr, *W1T = nullptr,
+       *W2T = nullptr, *WoT = nullptr;
+  long long adam_t = 0;
+  bool weights_dirty = true;
+  // per-body workspace (sized for the largest body seen)
+  long long cap = 0;
+  float *raw = nullptr, *cnt = nullptr, *xf = nullptr, *Dv = nullptr, *dD = nullptr,
+        *dh = nullptr, *sbuf = nullptr, *wpart = nullptr, *cpart = nullptr;
+  unsigned int* maxes = nullptr;
+  bf16 *x = nullptr, *h0 = nullptr, *m1 = nullptr, *a1 = nullptr, *h1 = nullptr, *m2 = nullptr,
+       *a2 = nullptr, *h2 = nullptr, *dz = nullptr, *dDb = nullptr;
+  double *G = nullptr, *r = nullptr, *y1 = nullptr, *y2 = nullptr, *tv = nullptr, *w = nullptr,
+         *q = nullptr, *g1 = nullptr, *red = nullptr;
+  float* hsamp = nullptr;
+};
+
+template <class T>
+static pd_status nalloc(pd_mpnn* net, T** p, size_t count) {
+  void* q = nullptr;
+  cudaError_t e = cudaMalloc(&q, sizeof(T) * (count ? count : 1));
+  if (e != cudaSuccess)
+    return pd_fail(e == cudaErrorMemoryAllocation ? PD_ERR_OOM : PD_ERR_CUDA,
+                   std::string("cudaMalloc: ") + cudaGetErrorString(e));
+  net->allocs.push_back(q);
+  *p = (T*)q;
+  return PD_OK;
+}
+
+static void nfree(pd_mpnn* net, void* p) {
+  if (!p) return;
+  for (size_t k = 0; k < net->allocs.size(); k++)
+    if (net->allocs[k] == p) { net->allocs.erase(net->allocs.begin() + k); break; }
+  cudaFree(p);
+}
+
+static pd_status ws_ensure(pd_mpnn* net, long long n) {
+  if (n <= net->cap) return PD_OK;
+  void** bufs[] = {(void**)&net->raw, (void**)&net->cnt, (void**)&net->xf, (void**)&net->Dv,
+                   (void**)&net->dD, (void**)&net->dh, (void**)&net->sbuf, (void**)&net->x,
+                   (void**)&net->h0, (void**)&net->m1, (void**)&net->a1, (void**)&net->h1,
+                   (void**)&net->m2, (void**)&net->a2, (void**)&net->h2, (void**)&net->dz,
+                   (void**)&net->dDb, (void**)&net->G, (void**)&net->r, (void**)&net->y1,
+                   (void**)&net->y2, (void**)&net->tv, (void**)&net->w, (void**)&net->q,
+                   (void**)&net->g1, (void**)&net->hsamp};
+  for (void** b : bufs) { nfree(net, *b); *b = nullptr; }
+  PD_TRY(nalloc(net, &net->raw, 12 * n));
+  PD_TRY(nalloc(net, &net->cnt, n));
+  PD_TRY(nalloc(net, &net->xf, NF * n));
+  PD_TRY(nalloc(net, &net->Dv, NO * n));
+  PD_TRY(nalloc(net, &net->dD, NO * n));
+  PD_TRY(nalloc(net, &net->dh, HID * n));
+  PD_TRY(nalloc(net, &net->sbuf, HID * n));
+  PD_TRY(nalloc(net, &net->x, NF * n));
+  bf16** acts[] = {&net->h0, &net->m1, &net->a1, &net->h1, &net->m2, &net->a2, &net->h2, &net->dz};
+  for (bf16** a : acts) PD_TRY(nalloc(net, a, HID * n));
+  PD_TRY(nalloc(net, &net->dDb, NOP * n));
+  PD_TRY(nalloc(net, &net->G, 9 * n));
+  double** vecs[] = {&net->r, &net->y1, &net->y2, &net->tv, &net->w, &net->q, &net->g1};
+  for (double** v : vecs) PD_TRY(nalloc(net, v, 3 * n));
+  PD_TRY(nalloc(net, &net->hsamp, 3 * n));
+  net->cap = n;
+  return PD_OK;
+}
+
+static int grid1(long long n, int t) {
+  long long b = (n + t - 1) / t;
+  return (int)(b < 1 ? 1 : b);
+}
+
+static void refresh_weights(pd_mpnn* net, cudaStream_t s) {
+  if (!net->weights_dirty) return;
+  k_weights<<<grid1(HID * 2 * HID, 256), 256, 0, s>>>(net->theta, net->W0, net->W1, net->W2, net->Wo,
+                                                      net->W1T, net->W2T, net->WoT);
+  net->weights_dirty = false;
+}
+
+static int dense_grid(long long n) {
+  long long tiles = (n + 15) / 16;
+  long long b = (tiles + 3) / 4;
+  if (b > 148LL * 8) b = 148LL * 8;
+  return (int)(b < 1 ? 1 : b);
+}
+
+// features and forward pass on body h; D in net->Dv
+static pd_status net_forward(pd_mpnn* net, pd_handle* h) {
+  const long long n = h->n;
+  cudaStream_t s = h->stream;
+  PD_TRY(ws_ensure(net, n));
+  refresh_weights(net, s);
+  PD_CUDA(cudaMemsetAsync(net->maxes, 0, 2 * sizeof(unsigned), s));
+  k_feat_raw<<<grid1(n, 128), 128, 0, s>>>(h->d, net->raw, net->cnt, net->maxes);
+  k_feat_fin<<<grid1(n, 256), 256, 0, s>>>(n, net->raw, h->nk->cmask, net->maxes, net->x, net->xf);
+  const float* th = net->theta;
+  DenseArgs a{};
+  a.n = n;
+  a.in0 = net->x; a.ld0 = NF; a.W = net->W0; a.bias = th + O_B0; a.out_h = net->h0;
+  k_dense<NF, HID, D_RELU><<<dense_grid(n), 128, 0, s>>>(a);
+  const int ag = grid1(n * 32, 256);
+  bf16* hp = net->h0;
+  bf16* ms[2] = {net->m1, net->m2};
+  bf16* as[2] = {net->a1, net->a2};
+  bf16* hs[2] = {net->h1, net->h2};
+  const bf16* Ws[2] = {net->W1, net->W2};
+  const int ob[2] = {O_B1, O_B2};
+  for (int l = 0; l < 2; l++) {
+    k_agg_mean<<<ag, 256, 0, s>>>(h->d, hp, net->cnt, ms[l]);
+    DenseArgs b{};
+    b.n = n; b.in0 = hp; b.ld0 = HID; b.in1 = ms[l]; b.W = Ws[l]; b.bias = th + ob[l];
+    b.resid = hp; b.out_a = as[l]; b.out_h = hs[l];
+    k_dense<2 * HID, HID, D_RESID><<<dense_grid(n), 128, 0, s>>>(b);
+    hp = hs[l];
+  }
+  DenseArgs o{};
+  o.n = n; o.in0 = net->h2; o.ld0 = HID; o.W = net->Wo; o.bias = th + O_BO; o.out_f = net->Dv;
+  k_dense<HID, NOP, D_OUT><<<dense_grid(n), 128, 0, s>>>(o);
+  h->launches += 9;
+  PD_CUDA(cudaGetLastError());
+  return PD_OK;
+}
+
+// backward pass from net->dD / net->dDb into net->grad
+static pd_status net_backward(pd_mpnn* net, pd_handle* h) {
+  const long long n = h->n;
+  cudaStream_t s = h->stream;
+  // output layer: dWo = dDb^T h2 (16 x 64, rows 0..8 used), dbo = colsum dD, dh2 = dDb Wo
+  k_wgrad<NOP, HID><<<WG_BLOCKS, 256, 0, s>>>(n, net->dDb, net->h2, HID, nullptr, net->wpart);
+  k_wgrad_reduce<<<grid1(NO * HID, 256), 256, 0, s>>>(net->wpart, WG_BLOCKS, NOP * HID, NO * HID,
+                                                     net->grad + O_WO);
+  k_colsum<float><<<WG_BLOCKS, 32, 0, s>>>(n, NO, net->dD, net->cpart);
+  k_wgrad_reduce<<<1, 64, 0, s>>>(net->cpart, WG_BLOCKS, NO, NO, net->grad + O_BO);
+  DenseArgs o{};
+  o.n = n; o.in0 = net->dDb; o.ld0 = NOP; o.W = net->WoT; o.out_f = net->dh;
+  k_dense<NOP, HID, D_BWD_OUT><<<dense_grid(n), 128, 0, s>>>(o);
+  const bf16* hprev[2] = {net->h0, net->h1};
+  const bf16* ms[2] = {net->m1, net->m2};
+  const bf16* as[2] = {net->a1, net->a2};
+  const bf16* WT[2] = {net->W1T, net->W2T};
+  const int ow[2] = {O_W1, O_W2}, ob[2] = {O_B1, O_B2};
+  const int eg = grid1(n * HID, 256), ag = grid1(n * 32, 256);
+  for (int l = 1; l >= 0; l--) {
+    k_relu_grad<<<eg, 256, 0, s>>>(n, net->dh, as[l], net->dz);
+    k_wgrad<HID, 2 * HID><<<WG_BLOCKS, 256, 0, s>>>(n, net->dz, hprev[l], HID, ms[l], net->wpart);
+    k_wgrad_reduce<<<grid1(HID * 2 * HID, 256), 256, 0, s>>>(net->wpart, WG_BLOCKS, HID * 2 * HID,
+                                                            HID * 2 * HID, net->grad + ow[l]);
+    k_colsum<bf16><<<WG_BLOCKS, 64, 0, s>>>(n, HID, net->dz, net->cpart);
+    k_wgrad_reduce<<<1, 64, 0, s>>>(net->cpart, WG_BLOCKS, HID, HID, net->grad + ob[l]);
+    DenseArgs b{};
+    b.n = n; b.in0 = net->dz; b.ld0 = HID; b.W = WT[l]; b.out_f = net->dh; b.out_s = net->sbuf;
+    b.cnt = net->cnt;
+    k_dense<HID, 2 * HID, D_BWD><<<dense_grid(n), 128, 0, s>>>(b);
+    k_agg_adj<<<ag, 256, 0, s>>>(h->d, net->sbuf, net->dh);
+  }
+  k_relu_grad<<<eg, 256, 0, s>>>(n, net->dh, net->h0, net->dz);
+  k_wgrad<HID, NF><<<WG_BLOCKS, 256, 0, s>>>(n, net->dz, net->x, NF, nullptr, net->wpart);
+  k_wgrad_reduce<<<grid1(HID * NF, 256), 256, 0, s>>>(net->wpart, WG_BLOCKS, HID * NF, HID * NF,
+                                                     net->grad + O_W0);
+  k_colsum<bf16><<<WG_BLOCKS, 64, 0, s>>>(n, HID, net->dz, net->cpart);
+  k_wgrad_reduce<<<1, 64, 0, s>>>(net->cpart, WG_BLOCKS, HID, HID, net->grad + O_B0);
+  h->launches += 26;
+  PD_CUDA(cudaGetLastError());
+  return PD_OK;
+}
+
+extern "C" pd_status pd_mpnn_create(int32_t device, pd_mpnn** out) {
+  if (!out) return pd_fail(PD_ERR_ARG, "out is NULL");
+  *out = nullptr;
+  PD_CUDA(cudaSetDevice(device));
+  pd_mpnn* net = new pd_mpnn();
+  net->device = device;
+  pd_status st = PD_OK;
+  auto a = [&](pd_status x) { if (st == PD_OK) st = x; };
+  a(nalloc(net, &net->theta, N_PARAMS));
+  a(nalloc(net, &net->grad, N_PARAMS));
+  a(nalloc(net, &net->am, N_PARAMS));
+  a(nalloc(net, &net->av, N_PARAMS));
+  a(nalloc(net, &net->W0, HID * NF));
+  a(nalloc(net, &net->W1, HID * 2 * HID));
+  a(nalloc(net, &net->W2, HID * 2 * HID));
+  a(nalloc(net, &net->Wo, NOP * HID));
+  a(nalloc(net, &net->W1T, HID * 2 * HID));
+  a(nalloc(net, &net->W2T, HID * 2 * HID));
+  a(nalloc(net, &net->WoT, NOP * HID));
+  a(nalloc(net, &net->maxes, 2));
+  a(nalloc(net, &net->wpart, (size_t)WG_BLOCKS * HID * 2 * HID));
+  a(nalloc(net, &net->cpart, (size_t)WG_BLOCKS * HID));
+  a(nalloc(net, &net->red, 4));
+  if (st == PD_OK) {
+    cudaMemset(net->theta, 0, sizeof(float) * N_PARAMS);
+    cudaMemset(net->grad, 0, sizeof(float) * N_PARAMS);
+    cudaMemset(net->am, 0, sizeof(float) * N_PARAMS);
+    cudaMemset(net->av, 0, sizeof(float) * N_PARAMS);
+  }
+  if (st != PD_OK) {
+    for (void* p : net->allocs) cudaFree(p);
+    delete net;
+    return st;
+  }
+  *out = net;
+  return PD_OK;
+}
+
+extern "C" pd_status pd_mpnn_destroy(pd_mpnn* net) {
+  if (!net) return PD_OK;
+  cudaSetDevice(net->device);
+  cudaDeviceSynchronize();
+  for (void* p : net->allocs) cudaFree(p);
+  delete net;
+  return PD_OK;
+}
+
+extern "C" pd_status pd_mpnn_set_params(pd_mpnn* net, const float* theta) {
+  if (!net || !theta) return pd_fail(PD_ERR_ARG, "NULL argument");
+  PD_CUDA(cudaSetDevice(net->device));
+  PD_CUDA(cudaMemcpy(net->theta, theta, sizeof(float) * N_PARAMS, cudaMemcpyHostToDevice));
+  PD_CUDA(cudaMemset(net->grad, 0, sizeof(float) * N_PARAMS));
+  PD_CUDA(cudaMemset(net->am, 0, sizeof(float) * N_PARAMS));
+  PD_CUDA(cudaMemset(net->av, 0, sizeof(float) * N_PARAMS));
+  net->adam_t = 0;
+  net->weights_dirty = true;
+  return PD_OK;
+}
+
+extern "C" pd_status pd_mpnn_get_params(pd_mpnn* net, float* theta) {
+  if (!net || !theta) return pd_fail(PD_ERR_ARG, "NULL argument");
+  PD_CUDA(cudaSetDevice(net->device));
+  PD_CUDA(cudaMemcpy(theta, net->theta, sizeof(float) * N_PARAMS, cudaMemcpyDeviceToHost));
+  return PD_OK;
+}
+
+static pd_status check_pair(pd_mpnn* net, pd_handle* h) {
+  if (!net || !h) return pd_fail(PD_ERR_ARG, "NULL argument");
+  if (net->device != h->device) return pd_fail(PD_ERR_ARG, "network and body on different devices");
+  if (h->material != PD_MAT_BB)
+    return pd_fail(PD_ERR_UNSUPPORTED, "the learned preconditioner needs the bond-based material");
+  PD_CUDA(cudaSetDevice(h->device));
+  return nk_ensure(h, 1);
+}
+
+extern "C" pd_status pd_mpnn_infer(pd_mpnn* net, pd_handle* h, float* features, float* D) {
+  PD_TRY(check_pair(net, h));
+  PD_TRY(net_forward(net, h));
+  NKState* S = h->nk;
+  if (!S->D) PD_TRY(dalloc(h, &S->D, 9 * h->n));
+  PD_CUDA(cudaMemcpyAsync(S->D, net->Dv, sizeof(float) * 9 * h->n, cudaMemcpyDeviceToDevice, h->stream));
+  S->have_D = true;
+  if (features)
+    PD_CUDA(cudaMemcpyAsync(features, net->xf, sizeof(float) * NF * h->n, cudaMemcpyDeviceToHost, h->stream));
+  if (D)
+    PD_CUDA(cudaMemcpyAsync(D, net->Dv, sizeof(float) * 9 * h->n, cudaMemcpyDeviceToHost, h->stream));
+  PD_CUDA(cudaStreamSynchronize(h->stream));
+  return PD_OK;
+}
+
+extern "C" pd_status pd_mpnn_loss_grad(pd_mpnn* net, pd_handle* h, int32_t n_rec,
+                                       const int64_t* rec_ids, int32_t n_host,
+                                       const float* host_samples, double host_alpha,
+                                       double host_weight, double* loss, float* grad) {
+  PD_TRY(check_pair(net, h));
+  NKState* S = h->nk;
+  if (n_rec < 0 || n_host < 0 || n_rec + n_host == 0 || (n_rec > 0 && !rec_ids) ||
+      (n_host > 0 && !host_samples))
+    return pd_fail(PD_ERR_ARG, "no samples");
+  for (int k = 0; k < n_rec; k++)
+    if (rec_ids[k] < 0 || rec_ids[k] >= S->rec_n) return pd_fail(PD_ERR_ARG, "recorded index out of range");
+  const long long n = h->n, nd = 3 * n;
+  cudaStream_t s = h->stream;
+  PD_TRY(net_forward(net, h));
+  nk_compute_blocks(h);  // P at the current state
+  PD_CUDA(cudaMemsetAsync(net->G, 0, sizeof(double) * 9 * n, s));
+  if (!(host_weight >= 0)) return pd_fail(PD_ERR_ARG, "host_weight < 0");
+  const int S_n = n_rec + n_host;
+  const int vg = grid1(nd, 256), pg = grid1(n, 256);
+  std::vector<double> losses(S_n, 0.0);
+  double* lsum = net->red;
+  double Ltot = 0.0;
+  for (int k = 0; k < S_n; k++) {
+    if (k < n_rec) {
+      k_f32_to_f64<<<vg, 256, 0, s>>>(net->r, S->rec + rec_ids[k] * nd, nd);
+    } else {
+      PD_CUDA(cudaMemcpyAsync(net->hsamp, host_samples + (size_t)(k - n_rec) * nd, sizeof(float) * nd,
+                              cudaMemcpyHostToDevice, s));
+      k_f32_to_f64<<<vg, 256, 0, s>>>(net->r, net->hsamp, nd);
+    }
+    // with K = alpha K0: y1 = r - K B r;  y2 = y1 - K B y1;  w = K y2;  g1 = K mask(y2 - B^T w)
+    const double al = k < n_rec ? 1.0 : host_alpha;
+    const double wt = (k < n_rec ? 1.0 : host_weight) / S_n;
+    nk_apply_blocks(h, net->Dv, net->r, 1.0, nullptr, 0.0, net->tv);
+    nk_apply_k0(h, net->tv, net->q);
+    k_sub<<<vg, 256, 0, s>>>(nd, net->r, al, net->q, nullptr, net->y1);
+    nk_apply_blocks(h, net->Dv, net->y1, 1.0, nullptr, 0.0, net->tv);
+    nk_apply_k0(h, net->tv, net->q);
+    k_sub<<<vg, 256, 0, s>>>(nd, net->y1, al, net->q, nullptr, net->y2);
+    nk_apply_k0(h, net->y2, net->w);
+    k_scalev<<<vg, 256, 0, s>>>(nd, al, net->w);
+    k_blockT<<<pg, 256, 0, s>>>(n, S->P, net->Dv, net->w, net->tv);
+    k_sub<<<vg, 256, 0, s>>>(nd, net->y2, 1.0, net->tv, S->cmask, net->q);
+    nk_apply_k0(h, net->q, net->g1);
+    k_scalev<<<vg, 256, 0, s>>>(nd, al, net->g1);
+    k_acc_G<<<pg, 256, 0, s>>>(n, net->g1, net->r, net->w, net->y1, S->cmask, -2.0 * wt, net->G);
+    nk_dots_dev(h, net->y2, 1, net->y2, lsum);
+    double l2 = 0.0;
+    PD_CUDA(cudaMemcpyAsync(&l2, lsum, sizeof(double), cudaMemcpyDeviceToHost, s));
+    PD_CUDA(cudaStreamSynchronize(s));
+    Ltot += wt * l2;
+    h->launches += 9;
+  }
+  k_dD<<<pg, 256, 0, s>>>(n, S->P, net->G, net->dD, net->dDb);
+  h->launches++;
+  PD_TRY(net_backward(net, h));
+  if (grad) PD_CUDA(cudaMemcpyAsync(grad, net->grad, sizeof(float) * N_PARAMS, cudaMemcpyDeviceToHost, s));
+  PD_CUDA(cudaStreamSynchronize(s));
+  if (loss) *loss = Ltot;
+  return PD_OK;
+}
+
+extern "C" pd_status pd_mpnn_zero_grad(pd_mpnn* net) {
+  if (!net) return pd_fail(PD_ERR_ARG, "NULL argument");
+  PD_CUDA(cudaSetDevice(net->device));
+  PD_CUDA(cudaMemset(net->grad, 0, sizeof(float) * N_PARAMS));
+  return PD_OK;
+}
+
+extern "C" pd_status pd_mpnn_adam(pd_mpnn* net, float lr) {
+  if (!net || !(lr > 0)) return pd_fail(PD_ERR_ARG, "invalid argument");
+  PD_CUDA(cudaSetDevice(net->device));
+  net->adam_t++;
+  const float b1 = 0.9f, b2 = 0.999f;
+  const float c1 = 1.f - std::pow(b1, (float)net->adam_t), c2 = 1.f - std::pow(b2, (float)net->adam_t);
+  k_adam<<<grid1(N_PARAMS, 256), 256>>>(net->theta, net->grad, net->am, net->av, N_PARAMS, lr, b1, b2,
+                                        1e-8f, c1, c2);
+  PD_CUDA(cudaGetLastError());
+  PD_CUDA(cudaDeviceSynchronize());
+  net->weights_dirty = true;
+  return PD_OK;
+}

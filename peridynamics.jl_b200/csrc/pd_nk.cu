@@ -27,37 +27,9 @@
 #include <cstring>
 #include <vector>
 
-#include "pd_handle.h"
+#include "pd_nk.h"
 
 namespace pd {
-
-constexpr int NK_NB = 592;   // blocks of the reduction kernels: 148 SMs x 4
-constexpr int NK_TPB = 256;
-
-// device scalars (doubles) of the solver
-enum { SC_WW = 0, SC_UU = 1, SC_VV = 2, SC_EPS = 3, SC_RR = 4, SC_N = 8 };
-
-struct NKState {
-  long long ndof = 0, ld = 0;   // 3 n and the padded stride of the basis vectors
-  int m = 0;                    // basis capacity (restart length)
-  bool zbasis = false;
-  int n_cond = 0;
-  long long* cdof = nullptr;
-  double* cval = nullptr;
-  int* cfield = nullptr;
-  unsigned char* cmask = nullptr;  // [3n] 1: dof carries a displacement condition
-  double *Fu = nullptr, *Fp = nullptr, *r = nullptr, *x = nullptr, *t = nullptr, *s = nullptr;
-  double *V = nullptr, *Z = nullptr;
-  float* P = nullptr;           // [9n] block-Jacobi inverse blocks (column-major)
-  float* D = nullptr;           // [9n] learned corrections
-  bool have_D = false;
-  float4* vf = nullptr;         // [n] FP32 copy of the vector that K0 gathers
-  double *part = nullptr, *h1 = nullptr, *h2 = nullptr, *hc = nullptr, *sc = nullptr,
-         *y = nullptr;
-  double* hpin = nullptr;       // pinned host copy of hc
-  float* rec = nullptr;         // recorded residual directions
-  long long rec_cap = 0, rec_n = 0;
-};
 
 void nk_release(pd_handle* h) {
   if (!h->nk) return;
@@ -838,3 +810,21 @@ extern "C" pd_status pd_nk_step(pd_handle* h, int64_t step, double beta, const p
                                   "Consider increasing `maxiter` or `tol`.");
   return PD_OK;
 }
+
+// helpers shared with pd_mpnn.cu
+namespace pd {
+pd_status nk_ensure(pd_handle* h, int m) { return nk_state(h, m); }
+void nk_dots_dev(pd_handle* h, const double* V, int k, const double* w, double* out) {
+  nk_dots(h, V, k, w, out);
+}
+void nk_apply_k0(pd_handle* h, const double* v, double* out) { nk_k0(h, v, out); }
+void nk_compute_blocks(pd_handle* h) {
+  k_bj_blocks<<<nk_grid(h->n, 128), 128, 0, h->stream>>>(h->d, h->nk->cmask, h->nk->P);
+  h->launches++;
+}
+void nk_apply_blocks(pd_handle* h, const float* D, const double* v, double a, const double* s,
+                     double b, double* z) {
+  k_block<<<nk_grid(h->n, 256), 256, 0, h->stream>>>(h->nk->P, D, v, a, s, b, h->nk->cmask, z, h->n);
+  h->launches++;
+}
+}  // namespace pd

@@ -31,6 +31,7 @@ BC_KIND_TIME, BC_KIND_POINT_TIME, BC_KIND_DATA = 0, 1, 2
 NK_CENTRAL, NK_FORWARD = 0, 1
 PC_NONE, PC_BLOCK_JACOBI, PC_BLOCK_POLY, PC_LEARNED_POLY, PC_LEARNED = range(5)
 NKC_DISPLACEMENT, NKC_B_EXT = 0, 1
+MPNN_N_PARAMS = 18185
 
 # every symbol that include/pdcuda.h declares
 EXPORTS = (
@@ -41,6 +42,8 @@ EXPORTS = (
     "pd_set_graph", "pd_set_pipeline", "pd_info", "pd_launch_count", "pd_stream",
     "pd_nk_set_conditions", "pd_nk_step", "pd_nk_set_corrections", "pd_nk_apply",
     "pd_nk_record", "pd_nk_recorded",
+    "pd_mpnn_create", "pd_mpnn_destroy", "pd_mpnn_set_params", "pd_mpnn_get_params",
+    "pd_mpnn_infer", "pd_mpnn_loss_grad", "pd_mpnn_zero_grad", "pd_mpnn_adam",
     "pd_osb_force_static", "pd_static_last_error",
 )
 
@@ -149,6 +152,14 @@ def lib():
         "pd_nk_apply": [vp, i32, vp, vp, vp],
         "pd_nk_record": [vp, i64],
         "pd_nk_recorded": [vp, vp],
+        "pd_mpnn_create": [i32, vp],
+        "pd_mpnn_destroy": [vp],
+        "pd_mpnn_set_params": [vp, vp],
+        "pd_mpnn_get_params": [vp, vp],
+        "pd_mpnn_infer": [vp, vp, vp, vp],
+        "pd_mpnn_loss_grad": [vp, vp, i32, vp, i32, vp, dbl, dbl, vp, vp],
+        "pd_mpnn_zero_grad": [vp],
+        "pd_mpnn_adam": [vp, C.c_float],
     }
     for name, args in sig.items():
         f = getattr(L, name)

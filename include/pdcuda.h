@@ -336,6 +336,8 @@ pd_status pd_nk_apply(pd_handle *h, int32_t op, const pd_nk_params *p, const dou
  * recorded vectors are the training data of the learned preconditioner. */
 pd_status pd_nk_record(pd_handle *h, int64_t capacity);
 pd_status pd_nk_recorded(pd_handle *h, int64_t *n);
+/* Recorded direction k as 3n floats (host). */
+pd_status pd_nk_recorded_vector(pd_handle *h, int64_t k, float *out);
 
 /* ---------------------------------------------------------------------------------------
  * Learned block preconditioner of the Newton-Krylov solve. No counterpart in the reference
@@ -363,6 +365,12 @@ pd_status pd_mpnn_infer(pd_mpnn *net, pd_handle *h, float *features, float *D);
 pd_status pd_mpnn_loss_grad(pd_mpnn *net, pd_handle *h, int32_t n_rec, const int64_t *rec_ids,
                             int32_t n_host, const float *host_samples, double host_alpha,
                             double host_weight, double *loss, float *grad);
+/* Spectral training loss L = -mean_rec rho(r) + weight mean_host max(rho(q) - tau, 0)^2 with
+ * rho(v) = v . K0 B v: recorded residual directions (the slow end) are pulled up, host samples
+ * (top eigenvectors of K0 B) are held below tau. Gradient handling as pd_mpnn_loss_grad. */
+pd_status pd_mpnn_spectral_grad(pd_mpnn *net, pd_handle *h, int32_t n_rec, const int64_t *rec_ids,
+                                int32_t n_host, const float *host_samples, double tau,
+                                double weight, double *loss, float *grad);
 pd_status pd_mpnn_zero_grad(pd_mpnn *net);
 /* One Adam step (beta 0.9 / 0.999) with the accumulated gradient, which is then cleared. */
 pd_status pd_mpnn_adam(pd_mpnn *net, float lr);

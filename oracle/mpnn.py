@@ -10,8 +10,10 @@ Network (per point i, bonds j of i that are active):
   x_i  16 features of the point (``features``)
   h0 = relu(W0 x + b0)                                  64
   m_l = mean_j h_{l-1, j};  h_l = h_{l-1} + relu(W_l [h_{l-1}; m_l] + b_l),  l = 1, 2
-  D_i = Wo h2 + bo                                      9 = 3x3 column-major
-The preconditioner blocks are B_i = P_i (I + D_i) with P_i the block-Jacobi inverse.
+  D_i = iso(Wo h2 + bo)     3x3 column-major; iso: every block s I, s = mean_j tr(A_j) / 3
+The preconditioner blocks are B_i = P_i (I + D_i) = (1 + s) P_i with P_i the block-Jacobi
+inverse: one learned scale per body keeps the blocks symmetric positive definite and K0 B
+similar to a symmetric operator.
 
 Loss over unit sample vectors r (recorded Krylov residual directions, alpha = 1, and top
 eigenvectors of K0 P, alpha = 1 / tau):
@@ -140,8 +142,17 @@ def forward(theta, x, g, exact=False):
         hn = rd(h + a)
         act[f"m{l}"], act[f"a{l}"], act[f"h{l}"] = m, a, hn
         h = hn
-    act["D"] = h @ W["Wo"].T + p["bo"]
+    act["D"] = iso(h @ W["Wo"].T + p["bo"])
     return act
+
+
+def iso(D):
+    """Body-wide isotropic readout of n x 9 blocks: every block becomes s I with
+    s = mean tr / 3. Applied to a gradient it gives the adjoint (sum tr / (3 n)) I."""
+    t = (D[:, 0] + D[:, 4] + D[:, 8]).mean() / 3
+    out = np.zeros_like(D)
+    out[:, 0] = out[:, 4] = out[:, 8] = t
+    return out
 
 
 def _mean64(g, h):
@@ -164,6 +175,7 @@ def backward(theta, act, dD, g, exact=False):
     W = {k: rd(np.asarray(v, np.float64 if exact else np.float32)) for k, v in p.items()
          if k.startswith("W")}
     grads = {}
+    dD = iso(dD)
     dDb = rd(dD)
     grads["Wo"] = dDb.T @ act["h2"]
     grads["bo"] = dD.sum(axis=0)
@@ -219,6 +231,39 @@ def loss_and_dD(onk, P, D, samples, alphas=None):
         a[cm.reshape(-1, 3)] = 0.0  # rows of constrained dofs do not reach B v
         G += a
     dDm = np.einsum("nba,nbc->nac", P, G)  # P^T G
+    return L, dDm.transpose(0, 2, 1).reshape(n, 9)
+
+
+def spectral_loss_and_dD(onk, P, D, slow, fast, tau, weight):
+    """L = -mean_slow rho(r) + weight mean_fast max(rho(q) - tau, 0)^2, rho(v) = v . K0 B v,
+    and its gradient with respect to D (n x 9, column-major)."""
+    n = onk.n
+    Dm = D.reshape(n, 3, 3).transpose(0, 2, 1)
+    B = np.einsum("nab,nbc->nac", P, np.eye(3) + Dm)
+    cm = onk.cmask
+
+    def Bm(w):
+        z = np.einsum("nab,nb->na", B, w.reshape(-1, 3)).reshape(-1)
+        z[cm] = 0.0
+        return z
+
+    G = np.zeros((n, 3, 3))
+    L = 0.0
+    for v, f_of in [(r, None) for r in slow] + [(q, True) for q in fast]:
+        v = np.asarray(v, np.float64)
+        rho = float(v @ onk.k0(Bm(v)))
+        if f_of is None:
+            L -= rho / len(slow)
+            f = -1.0 / len(slow)
+        elif rho > tau:
+            L += weight * (rho - tau) ** 2 / len(fast)
+            f = weight * 2.0 * (rho - tau) / len(fast)
+        else:
+            continue
+        a = f * onk.k0(v).reshape(-1, 3)[:, :, None] * v.reshape(-1, 3)[:, None, :]
+        a[cm.reshape(-1, 3)] = 0.0
+        G += a
+    dDm = np.einsum("nba,nbc->nac", P, G)
     return L, dDm.transpose(0, 2, 1).reshape(n, 9)
 
 

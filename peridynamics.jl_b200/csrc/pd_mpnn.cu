@@ -1,12 +1,16 @@
 // pd_mpnn.cu -- the learned block preconditioner of the Newton-Krylov solve: a two-layer
 // message-passing network over the bond graph that predicts per-point 3x3 corrections D_i of
-// the block-Jacobi blocks, B_i = P_i (I + D_i). No counterpart in the reference (its Newton
+// the block-Jacobi blocks, B_i = P_i (I + D_i). The readout makes D_i = s I the same for every
+// point: scalings that vary from point to point (full 3x3 corrections, or isotropic ones per
+// point) made the Krylov solves slower, the slow end of the spectrum following the weakest
+// points; one scale per body keeps the blocks symmetric positive definite and the
+// preconditioned operator similar to a symmetric one. No counterpart in the reference (its Newton
 // systems are solved by plain GMRES, newton_krylov.jl:448-450).
 //
 // Network (per point i; mean over the active bonds of i):
 //   x_i  16 features (k_feat_*)            h0 = relu(W0 x + b0)                     64
 //   m_l = mean_j h_{l-1,j};  h_l = h_{l-1} + relu(W_l [h_{l-1}; m_l] + b_l),  l = 1, 2
-//   D_i = Wo h2 + bo                       (9 = a 3x3 block, column-major)
+//   A_i = Wo h2 + bo (3x3, column-major);  D_i = s I,  s = mean_j tr(A_j) / 3 (body readout)
 // The dense layers are BF16 tensor-core products (mma.sync m16n8k16, FP32 accumulation) with
 // the weights staged in shared memory; activations are stored as BF16, the aggregation sums
 // in FP32. Training minimises, over unit sample vectors r (recorded Krylov residual
@@ -400,6 +404,58 @@ __global__ void k_acc_G(long long n, const double* __restrict__ g1, const double
   }
 }
 
+// body-wide isotropic readout of the per-point outputs A_i (3x3, column-major):
+// D_i = s I for every point, s = mean_j tr(A_j) / 3. The same map, self-adjoint up to the
+// 1 / n of the mean, turns a gradient dD into d A_i = (sum_j tr(dD_j) / (3 n)) I.
+// part: per-block partial sums of the traces (fixed partition and order)
+__global__ void k_trace_part(long long n, const float* __restrict__ D, double* __restrict__ part) {
+  __shared__ double red[8];
+  double acc = 0.0;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    acc += (double)D[9 * i] + (double)D[9 * i + 4] + (double)D[9 * i + 8];
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); w++) t += red[w];
+    part[blockIdx.x] = t;
+  }
+}
+
+// D_i = c I with c = scale * sum(part); bf16 copy padded to 16 columns when Db is given
+__global__ void k_iso_write(long long n, const double* __restrict__ part, int nb, double scale,
+                            float* __restrict__ D, bf16* __restrict__ Db) {
+  __shared__ float c;
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int b = 0; b < nb; b++) t += part[b];
+    c = (float)(t * scale);
+  }
+  __syncthreads();
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    for (int k = 0; k < 9; k++) D[9 * i + k] = (k % 4) == 0 ? c : 0.f;
+    if (Db)
+      for (int k = 0; k < NOP; k++)
+        Db[NOP * i + k] = __float2bfloat16_rn(k < 9 && (k % 4) == 0 ? c : 0.f);
+  }
+}
+
+constexpr int ISO_BLOCKS = 148;
+
+// G_i += f a_i b_i^T on the free rows
+__global__ void k_acc_outer(long long n, const double* __restrict__ a, const double* __restrict__ b,
+                            const unsigned char* __restrict__ cmask, double f, double* __restrict__ G) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  for (int r = 0; r < 3; r++) {
+    if (cmask[3 * i + r]) continue;
+    for (int c = 0; c < 3; c++) G[9 * i + r + 3 * c] += f * a[3 * i + r] * b[3 * i + c];
+  }
+}
+
 // dD_i = P_i^T G_i (fp32, column-major) and its bf16 copy padded to 16 columns
 __global__ void k_dD(long long n, const float* __restrict__ P, const double* __restrict__ G,
                      float* __restrict__ dD, bf16* __restrict__ dDb) {
@@ -579,7 +635,9 @@ static pd_status net_forward(pd_mpnn* net, pd_handle* h) {
   DenseArgs o{};
   o.n = n; o.in0 = net->h2; o.ld0 = HID; o.W = net->Wo; o.bias = th + O_BO; o.out_f = net->Dv;
   k_dense<HID, NOP, D_OUT><<<dense_grid(n), 128, 0, s>>>(o);
-  h->launches += 9;
+  k_trace_part<<<ISO_BLOCKS, 256, 0, s>>>(n, net->Dv, net->red + 4);
+  k_iso_write<<<ISO_BLOCKS, 256, 0, s>>>(n, net->red + 4, ISO_BLOCKS, 1.0 / (3.0 * n), net->Dv, nullptr);
+  h->launches += 11;
   PD_CUDA(cudaGetLastError());
   return PD_OK;
 }
@@ -649,7 +707,7 @@ extern "C" pd_status pd_mpnn_create(int32_t device, pd_mpnn** out) {
   a(nalloc(net, &net->maxes, 2));
   a(nalloc(net, &net->wpart, (size_t)WG_BLOCKS * HID * 2 * HID));
   a(nalloc(net, &net->cpart, (size_t)WG_BLOCKS * HID));
-  a(nalloc(net, &net->red, 4));
+  a(nalloc(net, &net->red, 4 + ISO_BLOCKS));
   if (st == PD_OK) {
     cudaMemset(net->theta, 0, sizeof(float) * N_PARAMS);
     cudaMemset(net->grad, 0, sizeof(float) * N_PARAMS);
@@ -771,7 +829,9 @@ extern "C" pd_status pd_mpnn_loss_grad(pd_mpnn* net, pd_handle* h, int32_t n_rec
     h->launches += 9;
   }
   k_dD<<<pg, 256, 0, s>>>(n, S->P, net->G, net->dD, net->dDb);
-  h->launches++;
+  k_trace_part<<<ISO_BLOCKS, 256, 0, s>>>(n, net->dD, net->red + 4);
+  k_iso_write<<<ISO_BLOCKS, 256, 0, s>>>(n, net->red + 4, ISO_BLOCKS, 1.0 / (3.0 * n), net->dD, net->dDb);
+  h->launches += 3;
   PD_TRY(net_backward(net, h));
   if (grad) PD_CUDA(cudaMemcpyAsync(grad, net->grad, sizeof(float) * N_PARAMS, cudaMemcpyDeviceToHost, s));
   PD_CUDA(cudaStreamSynchronize(s));
@@ -797,5 +857,68 @@ extern "C" pd_status pd_mpnn_adam(pd_mpnn* net, float lr) {
   PD_CUDA(cudaGetLastError());
   PD_CUDA(cudaDeviceSynchronize());
   net->weights_dirty = true;
+  return PD_OK;
+}
+
+// Spectral loss: L = -mean_slow rho(r) + w mean_fast max(rho(q) - tau, 0)^2 with the Rayleigh
+// quotient rho(v) = v . K0 B v of unit vectors. The slow samples (recorded Krylov residual
+// directions) pull the preconditioned spectrum up; the fast samples (top eigenvectors of
+// K0 B) hold its top below tau. d rho / d B_i = (K0 v)_i v_i^T on the free rows.
+extern "C" pd_status pd_mpnn_spectral_grad(pd_mpnn* net, pd_handle* h, int32_t n_rec,
+                                           const int64_t* rec_ids, int32_t n_host,
+                                           const float* host_samples, double tau, double weight,
+                                           double* loss, float* grad) {
+  PD_TRY(check_pair(net, h));
+  NKState* S = h->nk;
+  if (n_rec < 0 || n_host < 0 || n_rec + n_host == 0 || (n_rec > 0 && !rec_ids) ||
+      (n_host > 0 && !host_samples) || !(weight >= 0))
+    return pd_fail(PD_ERR_ARG, "invalid samples");
+  for (int k = 0; k < n_rec; k++)
+    if (rec_ids[k] < 0 || rec_ids[k] >= S->rec_n) return pd_fail(PD_ERR_ARG, "recorded index out of range");
+  const long long n = h->n, nd = 3 * n;
+  cudaStream_t s = h->stream;
+  PD_TRY(net_forward(net, h));
+  nk_compute_blocks(h);
+  PD_CUDA(cudaMemsetAsync(net->G, 0, sizeof(double) * 9 * n, s));
+  const int vg = grid1(nd, 256), pg = grid1(n, 256);
+  double Ltot = 0.0;
+  for (int k = 0; k < n_rec + n_host; k++) {
+    if (k < n_rec) {
+      k_f32_to_f64<<<vg, 256, 0, s>>>(net->r, S->rec + rec_ids[k] * nd, nd);
+    } else {
+      PD_CUDA(cudaMemcpyAsync(net->hsamp, host_samples + (size_t)(k - n_rec) * nd, sizeof(float) * nd,
+                              cudaMemcpyHostToDevice, s));
+      k_f32_to_f64<<<vg, 256, 0, s>>>(net->r, net->hsamp, nd);
+    }
+    // rho = r . K0 B r  (r is zero at the constrained dofs)
+    nk_apply_blocks(h, net->Dv, net->r, 1.0, nullptr, 0.0, net->tv);
+    nk_apply_k0(h, net->tv, net->q);
+    nk_dots_dev(h, net->r, 1, net->q, net->red);
+    double rho = 0.0;
+    PD_CUDA(cudaMemcpyAsync(&rho, net->red, sizeof(double), cudaMemcpyDeviceToHost, s));
+    PD_CUDA(cudaStreamSynchronize(s));
+    double f = 0.0;
+    if (k < n_rec) {
+      Ltot -= rho / n_rec;
+      f = -1.0 / n_rec;
+    } else if (rho > tau) {
+      Ltot += weight * (rho - tau) * (rho - tau) / n_host;
+      f = weight * 2.0 * (rho - tau) / n_host;
+    }
+    if (f != 0.0) {
+      nk_apply_k0(h, net->r, net->w);
+      k_acc_outer<<<pg, 256, 0, s>>>(n, net->w, net->r, S->cmask, f, net->G);
+      h->launches++;
+    }
+    h->launches += 3;
+  }
+  k_dD<<<pg, 256, 0, s>>>(n, S->P, net->G, net->dD, net->dDb);
+  k_trace_part<<<ISO_BLOCKS, 256, 0, s>>>(n, net->dD, net->red + 4);
+  k_iso_write<<<ISO_BLOCKS, 256, 0, s>>>(n, net->red + 4, ISO_BLOCKS, 1.0 / (3.0 * n), net->dD, net->dDb);
+  h->launches += 3;
+  PD_TRY(net_backward(net, h));
+  if (grad) PD_CUDA(cudaMemcpyAsync(grad, net->grad, sizeof(float) * N_PARAMS, cudaMemcpyDeviceToHost, s));
+  PD_CUDA(cudaStreamSynchronize(s));
+  if (loss) *loss = Ltot;
   return PD_OK;
 }

@@ -730,6 +730,16 @@ extern "C" pd_status pd_nk_recorded(pd_handle* h, int64_t* n) {
   return PD_OK;
 }
 
+extern "C" pd_status pd_nk_recorded_vector(pd_handle* h, int64_t k, float* out) {
+  if (!h || !out) return pd_fail(PD_ERR_ARG, "NULL argument");
+  if (!h->nk || k < 0 || k >= h->nk->rec_n) return pd_fail(PD_ERR_ARG, "recorded index out of range");
+  PD_CUDA(cudaSetDevice(h->device));
+  PD_CUDA(cudaMemcpyAsync(out, h->nk->rec + k * h->nk->ndof, sizeof(float) * h->nk->ndof,
+                          cudaMemcpyDeviceToHost, h->stream));
+  PD_CUDA(cudaStreamSynchronize(h->stream));
+  return PD_OK;
+}
+
 extern "C" pd_status pd_nk_apply(pd_handle* h, int32_t op, const pd_nk_params* p, const double* v,
                                  double* out) {
   if (!h || !out || (op != 3 && !v)) return pd_fail(PD_ERR_ARG, "NULL argument");

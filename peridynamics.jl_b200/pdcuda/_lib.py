@@ -41,9 +41,10 @@ EXPORTS = (
     "pd_force", "pd_run_vv", "pd_nan_step", "pd_run_vv_timed", "pd_autotune", "pd_set_mapping",
     "pd_set_graph", "pd_set_pipeline", "pd_info", "pd_launch_count", "pd_stream",
     "pd_nk_set_conditions", "pd_nk_step", "pd_nk_set_corrections", "pd_nk_apply",
-    "pd_nk_record", "pd_nk_recorded",
+    "pd_nk_record", "pd_nk_recorded", "pd_nk_recorded_vector",
     "pd_mpnn_create", "pd_mpnn_destroy", "pd_mpnn_set_params", "pd_mpnn_get_params",
-    "pd_mpnn_infer", "pd_mpnn_loss_grad", "pd_mpnn_zero_grad", "pd_mpnn_adam",
+    "pd_mpnn_infer", "pd_mpnn_loss_grad", "pd_mpnn_spectral_grad", "pd_mpnn_zero_grad",
+    "pd_mpnn_adam",
     "pd_osb_force_static", "pd_static_last_error",
 )
 
@@ -152,12 +153,14 @@ def lib():
         "pd_nk_apply": [vp, i32, vp, vp, vp],
         "pd_nk_record": [vp, i64],
         "pd_nk_recorded": [vp, vp],
+        "pd_nk_recorded_vector": [vp, i64, vp],
         "pd_mpnn_create": [i32, vp],
         "pd_mpnn_destroy": [vp],
         "pd_mpnn_set_params": [vp, vp],
         "pd_mpnn_get_params": [vp, vp],
         "pd_mpnn_infer": [vp, vp, vp, vp],
         "pd_mpnn_loss_grad": [vp, vp, i32, vp, i32, vp, dbl, dbl, vp, vp],
+        "pd_mpnn_spectral_grad": [vp, vp, i32, vp, i32, vp, dbl, dbl, vp, vp],
         "pd_mpnn_zero_grad": [vp],
         "pd_mpnn_adam": [vp, C.c_float],
     }

@@ -3,17 +3,19 @@
 ``BlockPreconditionerNet`` holds a two-layer message-passing network on the device
 (``pd_mpnn_*`` of libpdcuda): 16 features per point, hidden width 64, BF16 tensor-core
 layers with FP32 accumulation. It predicts per-point corrections D_i of the block-Jacobi
-blocks, B_i = P_i (I + D_i), which ``NewtonKrylov(preconditioner="learned_poly")`` applies
+blocks, B_i = P_i (I + D_i), read out over the body as one isotropic scale (D_i = s I; full
+3x3 corrections and per-point scalings made the Krylov solves slower), which ``NewtonKrylov(preconditioner="learned_poly")`` applies
 inside FGMRES as z = B (2 v - K0 B v). The untrained network (zero output layer) is the
 block-Jacobi polynomial.
 
 With the polynomial the preconditioned spectrum is mu = lambda (2 - lambda) for the
 eigenvalues lambda of K0 B: the slow end gains from scaling B up, until the fast end reaches 2
-and the polynomial turns it negative. Training therefore works on the fast end: the samples
-are top eigenvectors of K0 B under the current network (power iteration) and the loss
-||(I - K0 B / tau)^2 q||^2 places them at tau < 2; Adam minimises it with the device's own
-forward and backward kernels (``train``). ``collect`` records the Krylov residual directions
-of plain block-Jacobi runs (``pd_nk_record``), the data that shows where plain runs stall.
+and the polynomial turns it negative. Training (``train``) uses the spectral loss
+-mean rho(r) + w mean max(rho(q) - tau, 0)^2 with rho(v) = v . K0 B v: r are the Krylov
+residual directions recorded at every restart of plain block-Jacobi runs (``collect``,
+``pd_nk_record``: the slow end, where those runs stall), q the top eigenvectors of K0 B under
+the current network (power iteration). Adam minimises it with the device's own forward and
+backward kernels.
 """
 from __future__ import annotations
 
@@ -98,6 +100,20 @@ class BlockPreconditionerNet:
                 "pd_mpnn_loss_grad")
         return loss.value, grad
 
+    def spectral_grad(self, dev, rec_ids=(), fast=None, tau=1.85, weight=100.0):
+        """Spectral loss over recorded directions (the slow end, pulled up) and fast samples
+        [k x 3n] (held below tau); the gradient is accumulated on the device and returned."""
+        ids = np.ascontiguousarray(rec_ids, np.int64)
+        smp = None if fast is None else np.ascontiguousarray(fast, np.float32).reshape(-1, 3 * dev.n)
+        n_host = 0 if smp is None else smp.shape[0]
+        loss = C.c_double()
+        grad = np.empty(N_PARAMS, np.float32)
+        L.check(L.lib().pd_mpnn_spectral_grad(self.h, dev.h, len(ids), L.ptr(ids) if len(ids) else None,
+                                              n_host, L.ptr(smp), float(tau), float(weight),
+                                              C.byref(loss), L.ptr(grad)),
+                "pd_mpnn_spectral_grad")
+        return loss.value, grad
+
     def zero_grad(self):
         L.check(L.lib().pd_mpnn_zero_grad(self.h), "pd_mpnn_zero_grad")
 
@@ -168,17 +184,21 @@ def collect(dev, nk, increments, capacity):
     nkm.record(dev, capacity)
     nkm.setup(dev, nk)
     for n in range(1, increments + 1):
-        nkm.step(dev, nk, n)
+        try:
+            nkm.step(dev, nk, n)
+        except L.NotConvergedError:
+            break  # the directions recorded so far are the data
     return nkm.recorded(dev)
 
 
-def train(net, devs, steps, lr=1e-3, n_fast=4, tau=1.9, refresh=10, power_iters=6, seed=0,
-          log=None):
-    """Adam on the bodies in turn. The samples are the top eigenvectors of K0 B for the current
-    network (recomputed by a few power iterations every `refresh` visits of a body) with the
-    target eigenvalue tau: the loss ||(I - K0 B / tau)^2 q||^2 asks the blocks to scale the
-    preconditioned operator up until its fast end sits at tau < 2, the widest range that the
-    polynomial z = B (2 v - K0 B v) still maps to positive values. Returns the loss history."""
+def train(net, devs, steps, lr=1e-3, batch=16, n_fast=8, tau=1.85, weight=100.0, refresh=5,
+          power_iters=6, seed=0, log=None):
+    """Adam on the bodies in turn with the spectral loss: every step takes `batch` recorded
+    Krylov directions of one body (the slow end of its preconditioned spectrum, pulled up) and
+    its `n_fast` top eigenvectors of K0 B under the current network (recomputed by a few power
+    iterations every `refresh` visits), held below tau. Returns the loss history."""
+    rng = np.random.default_rng(seed)
+    counts = [nkm.recorded(d) for d in devs]
     fast = [top_modes(d, n_fast, seed=seed + k) for k, d in enumerate(devs)]
     hist = []
     for s in range(steps):
@@ -187,9 +207,10 @@ def train(net, devs, steps, lr=1e-3, n_fast=4, tau=1.9, refresh=10, power_iters=
         if visit > 0 and visit % refresh == 0:
             net.infer(devs[k])
             fast[k] = top_modes(devs[k], n_fast, iters=power_iters, start=fast[k], learned=True)
-        loss, _ = net.loss_grad(devs[k], (), fast[k], 1.0 / tau, 1.0)
+        ids = rng.choice(counts[k], size=min(batch, counts[k]), replace=False)
+        loss, _ = net.spectral_grad(devs[k], ids, fast[k], tau, weight)
         net.adam(lr)
         hist.append(loss)
         if log and (s % 20 == 0 or s == steps - 1):
-            log(f"step {s:4d} body {k} loss {loss:.3e}")
+            log(f"step {s:4d} body {k} loss {loss:.4e}")
     return hist

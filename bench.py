@@ -195,7 +195,8 @@ JFNK_WEIGHTS = os.path.join(ROOT, "peridynamics.jl_b200", "pdcuda", "weights", "
 JFNK_ARMS = ("block_jacobi", "block_poly", "learned_poly")
 
 
-def jfnk_compare(device, increments, n_steps=20, weights=JFNK_WEIGHTS, arms=JFNK_ARMS):
+def jfnk_compare(device, increments, n_steps=20, weights=JFNK_WEIGHTS, arms=JFNK_ARMS,
+                 gmres_maxiter=8000, newton_maxiter=12):
     """The 500k-point three-point-bending beam (250 x 50 x 40 points, dx = 1 mm, E = 70 GPa,
     no fracture, mid-span line pushed 0.5 mm down over n_steps load increments): wall time
     of the first `increments` increments to a 1e-8 relative nonlinear residual per increment,
@@ -218,8 +219,8 @@ def jfnk_compare(device, increments, n_steps=20, weights=JFNK_WEIGHTS, arms=JFNK
         dev = pd.DeviceBody(body, precision="fp64", device=device)
         dev.autotune()
         nk = pd.NewtonKrylov(steps=n_steps, tol=1e-8, tol_mode="relative", frechet="forward",
-                             gmres_restart=50, gmres_maxiter=8000, maxiter=12,
-                             preconditioner=pc, corrections=net)
+                             gmres_restart=50, gmres_maxiter=gmres_maxiter,
+                             maxiter=newton_maxiter, preconditioner=pc, corrections=net)
         t0 = time.perf_counter()
         nkm.setup(dev, nk)
         done = 0
@@ -263,13 +264,18 @@ def run_jfnk(args, rank, world):
     if rank != 0:
         return
     import torch  # noqa: F401  (device plumbing only)
-    res = jfnk_compare(int(os.environ.get("LOCAL_RANK", "0")), args.jfnk_increments)
+    res = jfnk_compare(int(os.environ.get("LOCAL_RANK", "0")), args.jfnk_increments,
+                       arms=tuple(args.jfnk_arms.split(",")),
+                       gmres_maxiter=args.jfnk_gmres_maxiter,
+                       newton_maxiter=args.jfnk_newton_maxiter)
     arms = res["arms"]
     ok = lambda a: a is not None and a.get("converged", True)
-    best = arms["learned_poly"] if ok(arms.get("learned_poly")) else arms["block_poly"]
+    ran = [arms[k] for k in ("learned_poly", "block_poly", "block_jacobi") if arms.get(k)]
+    best = next((a for a in ran if ok(a)), ran[0])
     cpu = None
     if not args.no_cpu:
-        cpu = jfnk_cpu_baseline(arms["block_jacobi"]["force_evals"])
+        bj = arms.get("block_jacobi") or {}
+        cpu = jfnk_cpu_baseline(bj.get("force_evals", 0))
     line = {"metric": "JFNK wall time to 1e-8 relative residual (learned preconditioner)",
             "value": best["s"], "unit": "s", "n_gpus": 1, "steps": args.jfnk_increments,
             "warmup": 0, "higher_is_better": False, "scaling": "none", "vs_baseline": None,
@@ -314,6 +320,9 @@ def main():
     ap.add_argument("--jfnk-increments", type=int, default=-1,
                     help="load increments of the JFNK comparison (default: 20 with --config "
                          "jfnk500k, 2 in the default run, 0 = skip)")
+    ap.add_argument("--jfnk-arms", default=",".join(JFNK_ARMS))
+    ap.add_argument("--jfnk-gmres-maxiter", type=int, default=8000)
+    ap.add_argument("--jfnk-newton-maxiter", type=int, default=12)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
 

@@ -370,13 +370,10 @@ def main():
             dist.barrier()
             torch.cuda.synchronize()
 
+    from pdcuda.replicas import reduce_max
+
     def max_over_ranks(x):
-        if not dist:
-            return x
-        import torch
-        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{local}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return reduce_max(x, dist, device=f"cuda:{local}")
 
     def build(prec):
         body, frac_ = make_body(args.config)

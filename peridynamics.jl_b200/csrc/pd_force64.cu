@@ -119,8 +119,12 @@ __device__ __forceinline__ void commit_row64(unsigned int* bits, long long word_
 // -------------------------------------------------------------------------------------------
 // BB: bond_based.jl:125-180 (calc_failure! storing the bond length, force_density_point!)
 // -------------------------------------------------------------------------------------------
-template <int G, bool MULTI>
-__global__ void PD_LB64 k_bb64(DevBody d, int kstep) {
+// FAST (mappings other than the serial order): the force uses one division per bond,
+// (l - L) / (L l), in place of the reference's (l - L) / L and three divisions by l; the
+// forces differ from the serial order by a few units in the last place, as the lane-group sums
+// already do. The failure decision keeps the reference's expression.
+template <int G, bool MULTI, bool FAST>
+__global__ void __launch_bounds__(256, FAST ? 4 : 2) k_bb64(DevBody d, int kstep) {
   if (d.ctrl->err) return;
   PD_SLICE_LOOP(G) {
     PD_SLICE_SETUP
@@ -141,19 +145,31 @@ __global__ void PD_LB64 k_bb64(DevBody d, int kstep) {
         const double4 xj = ld4(d.cur + j);
         const double dx = xj.x - xi.x, dy = xj.y - xi.y, dz = xj.z - xi.z;
         const double l = sqrt((dx * dx + dy * dy) + dz * dz);
-        const double eps = (l - L) / L;
-        act = ((word >> lane) & 1u) && !(eps > P.epsc && Ls > 0);
-        const double om = act ? 1.0 : 0.0;
-        double sc;
-        if (MULTI) {
-          const double bcj = d.params[d.meta[j] & META_PID_MASK].bc;
-          sc = om * (P.bc + bcj) / 2 * eps * xj.w;
+        if (FAST) {
+          // the failure test keeps the reference's eps = (l - L) / L (bonds that may fail only)
+          const bool brk = Ls > 0 && (l - L) / L > P.epsc;
+          act = ((word >> lane) & 1u) && !brk;
+          const double q = (l - L) / (L * l);  // eps / l
+          const double bcb = MULTI ? 0.5 * (P.bc + d.params[d.meta[j] & META_PID_MASK].bc) : P.bc;
+          const double sc = act ? bcb * q * xj.w : 0.0;
+          bx += sc * dx;
+          by += sc * dy;
+          bz += sc * dz;
         } else {
-          sc = om * P.bc * eps * xj.w;
+          const double eps = (l - L) / L;
+          act = ((word >> lane) & 1u) && !(eps > P.epsc && Ls > 0);
+          const double om = act ? 1.0 : 0.0;
+          double sc;
+          if (MULTI) {
+            const double bcj = d.params[d.meta[j] & META_PID_MASK].bc;
+            sc = om * (P.bc + bcj) / 2 * eps * xj.w;
+          } else {
+            sc = om * P.bc * eps * xj.w;
+          }
+          bx += sc * dx / l;
+          by += sc * dy / l;
+          bz += sc * dz / l;
         }
-        bx += sc * dx / l;
-        by += sc * dy / l;
-        bz += sc * dz / l;
       }
       na += act;
       commit_row64(d.bits, wi, word, act, lane);
@@ -554,8 +570,14 @@ int launch_force64(const DevBody& d, const LaunchCfg& c, int kstep, int phase, c
   int launches = 0;
   if (d.material == MAT_BB) {
     if (!A) return 0;
-    if (d.multi) { PD_DISPATCH_G(G, (k_bb64<GG, true><<<grid, c.block, 0, s>>>(d, kstep))); }
-    else { PD_DISPATCH_G(G, (k_bb64<GG, false><<<grid, c.block, 0, s>>>(d, kstep))); }
+    if (c.exact) {
+      if (d.multi) k_bb64<1, true, false><<<grid, c.block, 0, s>>>(d, kstep);
+      else k_bb64<1, false, false><<<grid, c.block, 0, s>>>(d, kstep);
+    } else if (d.multi) {
+      PD_DISPATCH_G(G, (k_bb64<GG, true, true><<<grid, c.block, 0, s>>>(d, kstep)));
+    } else {
+      PD_DISPATCH_G(G, (k_bb64<GG, false, true><<<grid, c.block, 0, s>>>(d, kstep)));
+    }
     return 1;
   }
   if (d.material == MAT_OSB) {

@@ -307,36 +307,45 @@ __global__ void k_block(const float* __restrict__ P, const float* __restrict__ D
   }
 }
 
-__global__ void k_pack4(float4* __restrict__ vf, const double* __restrict__ v, long long n) {
+__global__ void k_init_kx(DevBody d, float4* __restrict__ kx) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= d.n) return;
+  const double4 X = d.X0[i];
+  kx[2 * i] = make_float4((float)X.x, (float)X.y, (float)X.z, (float)X.w);
+}
+
+__global__ void k_pack4(float4* __restrict__ kx, const double* __restrict__ v, long long n) {
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  vf[i] = make_float4((float)v[3 * i], (float)v[3 * i + 1], (float)v[3 * i + 2], 0.f);
+  kx[2 * i + 1] = make_float4((float)v[3 * i], (float)v[3 * i + 1], (float)v[3 * i + 2], 0.f);
 }
 
 // out_i = V_i sum_j c V_j / L^3 (xi . (v_j - v_i)) xi over the active bonds: the small-strain
-// stiffness K0 of the reference configuration (xi = X_j - X_i), FP32 bond arithmetic;
-// constrained rows 0
+// stiffness K0 of the reference configuration, in FP32 from FP32 copies of the reference
+// positions (xi = X_j - X_i, L = |xi|: the bond arrays are read for the neighbour and the
+// bond bit only, one 32-byte gather per bond); constrained rows 0
 template <int G>
-__global__ void __launch_bounds__(256) k_k0(DevBody d, const float4* __restrict__ vf,
+__global__ void __launch_bounds__(256) k_k0(DevBody d, const float4* __restrict__ kx,
                                             const unsigned char* __restrict__ cmask,
                                             double* __restrict__ out) {
   PD_SLICE_LOOP(G) {
     PD_SLICE_SETUP
     float ax = 0.f, ay = 0.f, az = 0.f;
-    const double4 Xi = valid ? d.X0[i] : make_double4(0, 0, 0, 0);
-    const float4 vi = valid ? vf[i] : make_float4(0, 0, 0, 0);
+    const float4 Xi = valid ? kx[2 * i] : make_float4(0, 0, 0, 0);
+    const float4 vi = valid ? kx[2 * i + 1] : make_float4(0, 0, 0, 0);
     const DevParam& Pi = d.params[valid ? (d.meta[i] & META_PID_MASK) : 0];
+    const float ci = (float)Pi.bc;
     for (int r = 0; r < rows; r++) {
       const int k = r * G + gl;
       if (k < cnt) {
         const long long b = sbase + (long long)r * 32 + lane;
         if (bond_bit(d.bits, b)) {
           const int j = __ldg(d.nbr + b);
-          const double4 Xj = d.X0[j];
-          const float L = (float)fabs(__ldg(d.len64 + b));
-          const float ex = (float)(Xj.x - Xi.x), ey = (float)(Xj.y - Xi.y), ez = (float)(Xj.z - Xi.z);
-          const float4 vj = vf[j];
-          const float kk = (float)(bb_c(d, Pi, j) * Xj.w) / (L * L * L);
+          const float4 Xj = __ldg(kx + 2 * j), vj = __ldg(kx + 2 * j + 1);
+          const float ex = Xj.x - Xi.x, ey = Xj.y - Xi.y, ez = Xj.z - Xi.z;
+          const float L2 = (ex * ex + ey * ey) + ez * ez;
+          const float c = d.multi ? (float)bb_c(d, Pi, j) : ci;
+          const float kk = c * Xj.w / (L2 * sqrtf(L2));
           const float pr = kk * (ex * (vj.x - vi.x) + ey * (vj.y - vi.y) + ez * (vj.z - vi.z));
           ax += pr * ex; ay += pr * ey; az += pr * ez;
         }
@@ -385,7 +394,8 @@ static pd_status nk_state(pd_handle* h, int m) {
     PD_TRY(dalloc(h, &S->t, nd));
     PD_TRY(dalloc(h, &S->s, nd));
     PD_TRY(dalloc(h, &S->P, 9 * h->n));
-    PD_TRY(dalloc(h, &S->vf, h->n));
+    PD_TRY(dalloc(h, &S->kx, 2 * h->n));
+    k_init_kx<<<nk_grid(h->n, 256), 256, 0, h->stream>>>(h->d, S->kx);
     PD_TRY(dalloc(h, &S->sc, SC_N));
     PD_CUDA(cudaMemsetAsync(S->sc, 0, SC_N * sizeof(double), h->stream));
   }
@@ -463,18 +473,18 @@ static void nk_matvec(pd_handle* h, const pd_nk_params& p, const double* v, doub
 
 static void nk_k0(pd_handle* h, const double* v, double* out) {
   NKState* S = h->nk;
-  k_pack4<<<nk_grid(h->n, 256), 256, 0, h->stream>>>(S->vf, v, h->n);
+  k_pack4<<<nk_grid(h->n, 256), 256, 0, h->stream>>>(S->kx, v, h->n);
   long long blocks = (h->d.nslices + 7) / 8;
   if (blocks < 1) blocks = 1;
   if (blocks > 148LL * 64) blocks = 148LL * 64;
   const int grid = (int)blocks;
   switch (h->d.lg) {
-    case 1: k_k0<1><<<grid, 256, 0, h->stream>>>(h->d, S->vf, S->cmask, out); break;
-    case 2: k_k0<2><<<grid, 256, 0, h->stream>>>(h->d, S->vf, S->cmask, out); break;
-    case 4: k_k0<4><<<grid, 256, 0, h->stream>>>(h->d, S->vf, S->cmask, out); break;
-    case 8: k_k0<8><<<grid, 256, 0, h->stream>>>(h->d, S->vf, S->cmask, out); break;
-    case 16: k_k0<16><<<grid, 256, 0, h->stream>>>(h->d, S->vf, S->cmask, out); break;
-    default: k_k0<32><<<grid, 256, 0, h->stream>>>(h->d, S->vf, S->cmask, out); break;
+    case 1: k_k0<1><<<grid, 256, 0, h->stream>>>(h->d, S->kx, S->cmask, out); break;
+    case 2: k_k0<2><<<grid, 256, 0, h->stream>>>(h->d, S->kx, S->cmask, out); break;
+    case 4: k_k0<4><<<grid, 256, 0, h->stream>>>(h->d, S->kx, S->cmask, out); break;
+    case 8: k_k0<8><<<grid, 256, 0, h->stream>>>(h->d, S->kx, S->cmask, out); break;
+    case 16: k_k0<16><<<grid, 256, 0, h->stream>>>(h->d, S->kx, S->cmask, out); break;
+    default: k_k0<32><<<grid, 256, 0, h->stream>>>(h->d, S->kx, S->cmask, out); break;
   }
   h->launches += 2;
 }

@@ -25,7 +25,8 @@ struct NKState {
   float* P = nullptr;           // [9n] block-Jacobi inverse blocks (column-major)
   float* D = nullptr;           // [9n] learned corrections
   bool have_D = false;
-  float4* vf = nullptr;         // [n] FP32 copy of the vector that K0 gathers
+  float4* kx = nullptr;         // [2n] per point {X, Y, Z, V} (FP32 reference position) and
+                                //      {v_x, v_y, v_z, 0}: the vector K0 is applied to
   double *part = nullptr, *h1 = nullptr, *h2 = nullptr, *hc = nullptr, *sc = nullptr,
          *y = nullptr;
   double* hpin = nullptr;       // pinned host copy of hc

@@ -195,13 +195,56 @@ JFNK_WEIGHTS = os.path.join(ROOT, "peridynamics.jl_b200", "pdcuda", "weights", "
 JFNK_ARMS = ("block_jacobi", "block_poly", "learned_poly")
 
 
+def _jfnk_arm(pd, mpnn, nkm, body, device, pc, G, increments, n_steps, weights, gmres_maxiter,
+              newton_maxiter, budget):
+    net = None
+    if pc.startswith("learned"):
+        if not os.path.exists(weights):
+            return None
+        net = mpnn.BlockPreconditionerNet.load(weights, device=device)
+    dev = pd.DeviceBody(body, precision="fp64", device=device)
+    dev.set_mapping(G, 256)
+    nk = pd.NewtonKrylov(steps=n_steps, tol=1e-8, tol_mode="relative", frechet="forward",
+                         gmres_restart=50, gmres_maxiter=gmres_maxiter,
+                         maxiter=newton_maxiter, preconditioner=pc, corrections=net)
+    t0 = time.perf_counter()
+    nkm.setup(dev, nk)
+    done = 0
+    try:
+        for n in range(1, increments + 1):
+            nkm.step(dev, nk, n)
+            done = n
+            if budget and time.perf_counter() - t0 > budget:
+                break
+    except pd.NotConvergedError:
+        pass
+    t = time.perf_counter() - t0
+    st = nk.stats
+    dev.close()
+    if net is not None:
+        net.close()
+    if done < increments:
+        return {"s": t, "converged": False, "increments_done": done,
+                "gmres_iters": sum(x["gmres_iters"] for x in st), "group": G}
+    return {"s": t, "increments": increments, "group": G,
+            "newton_iters": sum(x["newton_iters"] for x in st),
+            "gmres_iters": sum(x["gmres_iters"] for x in st),
+            "force_evals": sum(x["force_evals"] for x in st),
+            "max_rel_residual": max(x["residual"] / x["residual_first"] for x in st),
+            "ms_per_krylov_step": 1e3 * t / max(1, sum(x["gmres_iters"] for x in st))}
+
+
 def jfnk_compare(device, increments, n_steps=20, weights=JFNK_WEIGHTS, arms=JFNK_ARMS,
-                 gmres_maxiter=8000, newton_maxiter=12):
+                 gmres_maxiter=8000, newton_maxiter=12, groups=(4,)):
     """The 500k-point three-point-bending beam (250 x 50 x 40 points, dx = 1 mm, E = 70 GPa,
     no fracture, mid-span line pushed 0.5 mm down over n_steps load increments): wall time
     of the first `increments` increments to a 1e-8 relative nonlinear residual per increment,
     FGMRES(50) with the forward Frechet step sqrt(eps) |u| / |v|, for each preconditioner.
-    The learned arm's time includes the network's inference on the beam."""
+    The learned arm's time includes the network's inference on the beam. Each arm runs with
+    every lane mapping in `groups` (lanes per point of the force kernels): the mapping sets the
+    FP64 summation order, and the finite-difference products carry that rounding into the
+    Krylov counts, so several mappings give the spread of a count; the first one is the
+    reported run."""
     import pdcuda as pd
     from pdcuda import mpnn
     from pdcuda import newton_krylov as nkm
@@ -210,46 +253,17 @@ def jfnk_compare(device, increments, n_steps=20, weights=JFNK_WEIGHTS, arms=JFNK
     out = {}
     budget = None  # other arms stop (reported as not converged) past 3x the block-Jacobi time
     for pc in arms:
-        net = None
-        if pc.startswith("learned"):
-            if not os.path.exists(weights):
-                out[pc] = None
-                continue
-            net = mpnn.BlockPreconditionerNet.load(weights, device=device)
-        dev = pd.DeviceBody(body, precision="fp64", device=device)
-        dev.autotune()
-        nk = pd.NewtonKrylov(steps=n_steps, tol=1e-8, tol_mode="relative", frechet="forward",
-                             gmres_restart=50, gmres_maxiter=gmres_maxiter,
-                             maxiter=newton_maxiter, preconditioner=pc, corrections=net)
-        t0 = time.perf_counter()
-        nkm.setup(dev, nk)
-        done = 0
-        try:
-            for n in range(1, increments + 1):
-                nkm.step(dev, nk, n)
-                done = n
-                if budget and time.perf_counter() - t0 > budget:
-                    break
-        except pd.NotConvergedError:
-            pass
-        t = time.perf_counter() - t0
-        st = nk.stats
-        if done < increments:
-            out[pc] = {"s": t, "converged": False, "increments_done": done,
-                       "gmres_iters": sum(x["gmres_iters"] for x in st)}
-            dev.close()
-            continue
-        if pc == "block_jacobi":
-            budget = 3.0 * t
-        out[pc] = {"s": t, "increments": increments,
-                   "newton_iters": sum(x["newton_iters"] for x in st),
-                   "gmres_iters": sum(x["gmres_iters"] for x in st),
-                   "force_evals": sum(x["force_evals"] for x in st),
-                   "max_rel_residual": max(x["residual"] / x["residual_first"] for x in st),
-                   "ms_per_krylov_step": 1e3 * t / max(1, sum(x["gmres_iters"] for x in st))}
-        dev.close()
-        if net is not None:
-            net.close()
+        runs = []
+        for G in groups:
+            runs.append(_jfnk_arm(pd, mpnn, nkm, body, device, pc, G, increments, n_steps, weights,
+                                  gmres_maxiter, newton_maxiter, budget))
+        r0 = runs[0]
+        if r0 is not None and len(runs) > 1:
+            r0["spread"] = {str(G): (None if r is None else {"s": r["s"], "gmres_iters": r["gmres_iters"]})
+                            for G, r in zip(groups, runs)}
+        out[pc] = r0
+        if pc == "block_jacobi" and r0 is not None and r0.get("converged", True):
+            budget = 3.0 * r0["s"]
     bj = out.get("block_jacobi")
     for pc in arms:
         if out.get(pc) and bj and out[pc].get("converged", True):
@@ -267,7 +281,8 @@ def run_jfnk(args, rank, world):
     res = jfnk_compare(int(os.environ.get("LOCAL_RANK", "0")), args.jfnk_increments,
                        arms=tuple(args.jfnk_arms.split(",")),
                        gmres_maxiter=args.jfnk_gmres_maxiter,
-                       newton_maxiter=args.jfnk_newton_maxiter)
+                       newton_maxiter=args.jfnk_newton_maxiter,
+                       groups=tuple(int(g) for g in args.jfnk_groups.split(",")))
     arms = res["arms"]
     ok = lambda a: a is not None and a.get("converged", True)
     ran = [arms[k] for k in ("learned_poly", "block_poly", "block_jacobi") if arms.get(k)]
@@ -323,6 +338,8 @@ def main():
     ap.add_argument("--jfnk-arms", default=",".join(JFNK_ARMS))
     ap.add_argument("--jfnk-gmres-maxiter", type=int, default=8000)
     ap.add_argument("--jfnk-newton-maxiter", type=int, default=12)
+    ap.add_argument("--jfnk-groups", default="4",
+                    help="lane mappings per arm (the first is reported, the others give the spread)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
 

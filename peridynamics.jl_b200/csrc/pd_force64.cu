@@ -124,7 +124,7 @@ __device__ __forceinline__ void commit_row64(unsigned int* bits, long long word_
 // forces differ from the serial order by a few units in the last place, as the lane-group sums
 // already do. The failure decision keeps the reference's expression.
 template <int G, bool MULTI, bool FAST>
-__global__ void __launch_bounds__(256, FAST ? 4 : 2) k_bb64(DevBody d, int kstep) {
+__global__ void __launch_bounds__(256, FAST ? 3 : 2) k_bb64(DevBody d, int kstep) {
   if (d.ctrl->err) return;
   PD_SLICE_LOOP(G) {
     PD_SLICE_SETUP
@@ -132,6 +132,46 @@ __global__ void __launch_bounds__(256, FAST ? 4 : 2) k_bb64(DevBody d, int kstep
     int na = 0;
     const double4 xi = valid ? ld4(d.cur + i) : make_double4(0, 0, 0, 0);
     const DevParam& P = d.params[valid ? (d.meta[i] & META_PID_MASK) : 0];
+    if (FAST) {
+      // two rows per iteration: two independent neighbour gathers in flight per lane
+      const int self = valid ? (int)i : 0;
+      for (int r = 0; r < rows; r += 2) {
+        const bool two = r + 1 < rows;
+        const long long wi = (sbase >> 5) + r;
+        const unsigned w0 = d.bits[wi], w1 = two ? d.bits[wi + 1] : 0u;
+        const int k0 = r * G + gl, k1 = k0 + G;
+        const bool h0 = k0 < cnt, h1 = two && k1 < cnt;
+        const long long b0 = sbase + (long long)r * 32 + lane, b1 = b0 + 32;
+        const int j0 = h0 ? __ldg(d.nbr + b0) : self, j1 = h1 ? __ldg(d.nbr + b1) : self;
+        const double Ls0 = h0 ? __ldg(d.len64 + b0) : 1.0, Ls1 = h1 ? __ldg(d.len64 + b1) : 1.0;
+        const double4 x0 = ld4(d.cur + j0), x1 = ld4(d.cur + j1);
+        bool act0 = false, act1 = false;
+#pragma unroll
+        for (int u = 0; u < 2; u++) {
+          const bool h = u ? h1 : h0;
+          if (!h) continue;
+          const double4 xj = u ? x1 : x0;
+          const double Ls = u ? Ls1 : Ls0;
+          const double L = fabs(Ls);
+          const double dx = xj.x - xi.x, dy = xj.y - xi.y, dz = xj.z - xi.z;
+          const double l = sqrt((dx * dx + dy * dy) + dz * dz);
+          // the failure test keeps the reference's eps = (l - L) / L (bonds that may fail only)
+          const bool brk = Ls > 0 && (l - L) / L > P.epsc;
+          const bool act = (((u ? w1 : w0) >> lane) & 1u) && !brk;
+          const double q = (l - L) / (L * l);  // eps / l
+          const double bcb =
+              MULTI ? 0.5 * (P.bc + d.params[d.meta[u ? j1 : j0] & META_PID_MASK].bc) : P.bc;
+          const double sc = act ? bcb * q * xj.w : 0.0;
+          bx += sc * dx;
+          by += sc * dy;
+          bz += sc * dz;
+          if (u) act1 = act; else act0 = act;
+        }
+        na += act0 + act1;
+        commit_row64(d.bits, wi, w0, act0, lane);
+        if (two) commit_row64(d.bits, wi + 1, w1, act1, lane);
+      }
+    } else
     for (int r = 0; r < rows; r++) {
       const long long wi = (sbase >> 5) + r;
       const unsigned word = d.bits[wi];
@@ -145,17 +185,7 @@ __global__ void __launch_bounds__(256, FAST ? 4 : 2) k_bb64(DevBody d, int kstep
         const double4 xj = ld4(d.cur + j);
         const double dx = xj.x - xi.x, dy = xj.y - xi.y, dz = xj.z - xi.z;
         const double l = sqrt((dx * dx + dy * dy) + dz * dz);
-        if (FAST) {
-          // the failure test keeps the reference's eps = (l - L) / L (bonds that may fail only)
-          const bool brk = Ls > 0 && (l - L) / L > P.epsc;
-          act = ((word >> lane) & 1u) && !brk;
-          const double q = (l - L) / (L * l);  // eps / l
-          const double bcb = MULTI ? 0.5 * (P.bc + d.params[d.meta[j] & META_PID_MASK].bc) : P.bc;
-          const double sc = act ? bcb * q * xj.w : 0.0;
-          bx += sc * dx;
-          by += sc * dy;
-          bz += sc * dz;
-        } else {
+        {
           const double eps = (l - L) / L;
           act = ((word >> lane) & 1u) && !(eps > P.epsc && Ls > 0);
           const double om = act ? 1.0 : 0.0;

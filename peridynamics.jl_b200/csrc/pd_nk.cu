@@ -335,20 +335,28 @@ __global__ void __launch_bounds__(256) k_k0(DevBody d, const float4* __restrict_
     const float4 vi = valid ? kx[2 * i + 1] : make_float4(0, 0, 0, 0);
     const DevParam& Pi = d.params[valid ? (d.meta[i] & META_PID_MASK) : 0];
     const float ci = (float)Pi.bc;
-    for (int r = 0; r < rows; r++) {
-      const int k = r * G + gl;
-      if (k < cnt) {
-        const long long b = sbase + (long long)r * 32 + lane;
-        if (bond_bit(d.bits, b)) {
-          const int j = __ldg(d.nbr + b);
-          const float4 Xj = __ldg(kx + 2 * j), vj = __ldg(kx + 2 * j + 1);
-          const float ex = Xj.x - Xi.x, ey = Xj.y - Xi.y, ez = Xj.z - Xi.z;
-          const float L2 = (ex * ex + ey * ey) + ez * ez;
-          const float c = d.multi ? (float)bb_c(d, Pi, j) : ci;
-          const float kk = c * Xj.w / (L2 * sqrtf(L2));
-          const float pr = kk * (ex * (vj.x - vi.x) + ey * (vj.y - vi.y) + ez * (vj.z - vi.z));
-          ax += pr * ex; ay += pr * ey; az += pr * ez;
-        }
+    const int self = valid ? (int)i : 0;
+    // two rows per iteration: two independent neighbour gathers in flight per lane
+    for (int r = 0; r < rows; r += 2) {
+      const int k0 = r * G + gl, k1 = k0 + G;
+      const long long b0 = sbase + (long long)r * 32 + lane, b1 = b0 + 32;
+      const bool a0 = k0 < cnt && bond_bit(d.bits, b0);
+      const bool a1 = r + 1 < rows && k1 < cnt && bond_bit(d.bits, b1);
+      const int j0 = a0 ? __ldg(d.nbr + b0) : self;
+      const int j1 = a1 ? __ldg(d.nbr + b1) : self;
+      const float4 X0 = __ldg(kx + 2 * j0), v0 = __ldg(kx + 2 * j0 + 1);
+      const float4 X1 = __ldg(kx + 2 * j1), v1 = __ldg(kx + 2 * j1 + 1);
+#pragma unroll
+      for (int u = 0; u < 2; u++) {
+        const bool a = u ? a1 : a0;
+        if (!a) continue;
+        const float4 Xj = u ? X1 : X0, vj = u ? v1 : v0;
+        const float ex = Xj.x - Xi.x, ey = Xj.y - Xi.y, ez = Xj.z - Xi.z;
+        const float L2 = (ex * ex + ey * ey) + ez * ez;
+        const float c = d.multi ? (float)bb_c(d, Pi, u ? j1 : j0) : ci;
+        const float kk = c * Xj.w / (L2 * sqrtf(L2));
+        const float pr = kk * (ex * (vj.x - vi.x) + ey * (vj.y - vi.y) + ez * (vj.z - vi.z));
+        ax += pr * ex; ay += pr * ey; az += pr * ez;
       }
     }
     if (G > 1) { ax = group_sum<G>(ax); ay = group_sum<G>(ay); az = group_sum<G>(az); }

@@ -404,6 +404,7 @@ def main():
     body, dev, dt = build(args.precision)
     n_pts, n_bonds, sym = dev.info()
     group, block = dev.autotune()
+    dev_mapping = dev.mapping()
     dev.set_graph(args.graph)
     step = 1
     dev.run(step, args.warmup, dt)
@@ -499,7 +500,8 @@ def main():
             "config": {"workload": f"{args.config}: {mat} {nx}x{ny}x{nz} points, dx={dx}, "
                                    f"horizon 3.015dx, {frac:.0%} pairs broken, VV step",
                        "points": n_pts, "bonds": n_bonds, "precision": prec,
-                       "mapping": {"group": group, "block": block}, "symmetric_pairs": bool(sym),
+                       "mapping": dict(zip(("group", "block", "pipe"), dev_mapping)),
+                       "symmetric_pairs": bool(sym),
                        "l2": "inputs larger than L2 (bond arrays of ~19 GB)",
                        "parallelism": f"replicas x{world}"},
             "roofline": {"bound": "hbm", "kernel": f"{mat.lower()} force {dom}",

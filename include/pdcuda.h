@@ -243,8 +243,13 @@ pd_status pd_set_mapping(pd_handle *h, int32_t group, int32_t block);
 
 /* How the FP32 force kernels read the bond stream: 0 = direct loads; 1, 2, 3 = chunks of
  * the sliced bond arrays staged in shared memory by TMA bulk copies (4 rows x 3 stages,
- * 4 rows x 4 stages, 8 rows x 3 stages per warp). Needs one lane per point and BB or OSB. */
+ * 4 rows x 4 stages, 8 rows x 3 stages per warp; one lane per point, BB or OSB); 4 = direct
+ * loads two rows at a time, all their neighbour gathers in flight together (OSB; results
+ * identical to 0). pd_autotune times all that apply. */
 pd_status pd_set_pipeline(pd_handle *h, int32_t pipe);
+
+/* The current mapping (group 0 = serial order), block size and bond-stream variant. */
+pd_status pd_get_mapping(pd_handle *h, int32_t *group, int32_t *block, int32_t *pipe);
 
 /* Enables CUDA-graph capture of blocks of `steps_per_graph` steps (0 disables). */
 pd_status pd_set_graph(pd_handle *h, int32_t steps_per_graph);

@@ -868,7 +868,7 @@ extern "C" pd_status pd_set_param_timesteps(pd_handle* h, const double* dtp) {
 static int launch_force(pd_handle* h, int kstep, int phase) {
   int k;
   if (h->precision == PD_PREC_FP64) k = launch_force64(h->d, h->cfg, kstep, phase, h->stream);
-  else if (h->cfg.pipe > 0 && tma_supported(h->d)) k = launch_force32_tma(h->d, h->cfg.pipe, kstep, phase, h->stream);
+  else if (h->cfg.pipe >= 1 && h->cfg.pipe <= 3 && tma_supported(h->d)) k = launch_force32_tma(h->d, h->cfg.pipe, kstep, phase, h->stream);
   else k = launch_force32(h->d, h->cfg, kstep, phase, h->stream);
   h->launches += k;
   return k;
@@ -1066,13 +1066,18 @@ extern "C" pd_status pd_autotune(pd_handle* h, int32_t* group_out, int32_t* bloc
     if (st == PD_ERR_OOM) { cudaGetLastError(); continue; }  // no room for a second layout
     if (st != PD_OK) { cudaEventDestroy(e0); cudaEventDestroy(e1); return st; }
     const bool tma = h->precision == PD_PREC_FP32_KAHAN && G == 1 && tma_supported(h->d);
-    for (int v = 0; v < (tma ? 5 : 2); v++) {
-      const int B = v < 2 ? blocks[v] : 128;
+    const bool two = h->precision == PD_PREC_FP32_KAHAN && h->material == PD_MAT_OSB;
+    // candidates: blocks of 128 / 256 with plain loads, then (FP32 OSB) the two-row kernels,
+    // then (one lane per point) the TMA-staged bond stream
+    for (int v = 0; v < 7; v++) {
+      if ((v == 2 || v == 3) && !two) continue;
+      if (v >= 4 && !tma) continue;
+      const int B = v < 4 ? blocks[v % 2] : 128;
       h->cfg.group = G; h->cfg.block = B; h->cfg.exact = false;
-      h->cfg.pipe = v < 2 ? 0 : v - 1;
+      h->cfg.pipe = v < 2 ? 0 : v < 4 ? 4 : v - 3;
       launch_force(h, 0, 0);
       cudaEventRecord(e0, h->stream);
-      for (int r = 0; r < 3; r++) launch_force(h, 0, 0);
+      for (int r = 0; r < 5; r++) launch_force(h, 0, 0);
       cudaEventRecord(e1, h->stream);
       cudaError_t e = cudaEventSynchronize(e1);
       if (e != cudaSuccess) { cudaEventDestroy(e0); cudaEventDestroy(e1); return fail(PD_ERR_CUDA, cudaGetErrorString(e)); }
@@ -1156,10 +1161,20 @@ extern "C" pd_status pd_break_random_pairs(pd_handle* h, double fraction, uint64
   return PD_OK;
 }
 
+extern "C" pd_status pd_get_mapping(pd_handle* h, int32_t* group, int32_t* block, int32_t* pipe) {
+  if (!h) return fail(PD_ERR_ARG, "handle is NULL");
+  if (group) *group = h->cfg.exact ? 0 : h->cfg.group;
+  if (block) *block = h->cfg.block;
+  if (pipe) *pipe = h->cfg.pipe;
+  return PD_OK;
+}
+
 extern "C" pd_status pd_set_pipeline(pd_handle* h, int32_t pipe) {
   if (!h) return fail(PD_ERR_ARG, "handle is NULL");
-  if (pipe < 0 || pipe > 3) return fail(PD_ERR_ARG, "pipe must be 0, 1, 2 or 3");
-  if (pipe > 0 && (h->precision != PD_PREC_FP32_KAHAN || !tma_supported(h->d)))
+  if (pipe < 0 || pipe > 4) return fail(PD_ERR_ARG, "pipe must be 0 to 4");
+  if (pipe == 4 && (h->precision != PD_PREC_FP32_KAHAN || h->material != PD_MAT_OSB))
+    return fail(PD_ERR_ARG, "the two-row kernels are the FP32 OSB ones");
+  if (pipe >= 1 && pipe <= 3 && (h->precision != PD_PREC_FP32_KAHAN || !tma_supported(h->d)))
     return fail(PD_ERR_ARG, "the staged bond stream needs the FP32 path, one lane per point and BB or OSB");
   h->cfg.pipe = pipe;
   destroy_graph(h);

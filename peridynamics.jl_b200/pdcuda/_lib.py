@@ -39,7 +39,7 @@ EXPORTS = (
     "pd_destroy", "pd_set_state", "pd_break_bonds", "pd_break_random_pairs", "pd_get_field",
     "pd_set_bcs", "pd_set_bc_values", "pd_stable_timestep", "pd_set_param_timesteps",
     "pd_force", "pd_run_vv", "pd_nan_step", "pd_run_vv_timed", "pd_autotune", "pd_set_mapping",
-    "pd_set_graph", "pd_set_pipeline", "pd_info", "pd_launch_count", "pd_stream",
+    "pd_set_graph", "pd_set_pipeline", "pd_get_mapping", "pd_info", "pd_launch_count", "pd_stream",
     "pd_nk_set_conditions", "pd_nk_step", "pd_nk_set_corrections", "pd_nk_apply",
     "pd_nk_record", "pd_nk_recorded", "pd_nk_recorded_vector",
     "pd_mpnn_create", "pd_mpnn_destroy", "pd_mpnn_set_params", "pd_mpnn_get_params",
@@ -143,6 +143,7 @@ def lib():
         "pd_set_mapping": [vp, i32, i32],
         "pd_set_graph": [vp, i32],
         "pd_set_pipeline": [vp, i32],
+        "pd_get_mapping": [vp, vp, vp, vp],
         "pd_info": [vp, vp, vp, vp],
         "pd_launch_count": [vp, vp],
         "pd_stream": [vp, vp],

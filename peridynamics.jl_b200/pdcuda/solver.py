@@ -279,6 +279,12 @@ class DeviceBody:
     def set_pipeline(self, pipe):
         L.check(L.lib().pd_set_pipeline(self.h, pipe), "pd_set_pipeline")
 
+    def mapping(self):
+        """(lanes per point, block size, bond-stream variant); 0 lanes = serial order."""
+        g, b, p = C.c_int32(), C.c_int32(), C.c_int32()
+        L.check(L.lib().pd_get_mapping(self.h, C.byref(g), C.byref(b), C.byref(p)), "pd_get_mapping")
+        return g.value, b.value, p.value
+
     def autotune(self):
         g, b = C.c_int32(), C.c_int32()
         L.check(L.lib().pd_autotune(self.h, C.byref(g), C.byref(b)), "pd_autotune")

@@ -304,3 +304,22 @@ def test_staged_bond_stream_matches_direct_loads(name):
     # the same FP32 arithmetic; FMA contraction may differ between the two kernels
     for b, na in res[1:]:
         assert rel_err(b, res[0][0]) < 1e-6 and np.array_equal(na, res[0][1])
+
+
+@pytest.mark.parametrize("group", [1, 4, 32])
+def test_two_row_osb_kernels_equal_one_row(group):
+    """Pipeline 4 (two rows of gathers in flight) adds every lane's bonds in the same order as
+    the one-row OSB kernels: identical forces, bond states and damage, also with fracture."""
+    body = cube_body(pd.OSBMaterial(), n=9, fracture=True)
+    u = deform(body._pos, amplitude=0.002)
+    out = []
+    for pipe in (0, 4):
+        dev = pd.DeviceBody(body, precision="fp32")
+        dev.set_mapping(group, 256)
+        dev.set_pipeline(pipe)
+        assert dev.mapping() == (group, 256, pipe)
+        dev.set_state(displacement=u)
+        dev.force()
+        out.append([dev.field(f) for f in ("b_int", "n_active_bonds", "bond_active", "damage")])
+    for a, b in zip(*out):
+        assert np.array_equal(a, b)

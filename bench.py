@@ -146,15 +146,16 @@ def oracle_sample(cfg, threads):
     return b, dt, (sx, sy, sz)
 
 
-def cpu_baseline(cfg, threads, budget_s=20.0):
-    """bond-updates/s of the oracle sample over whole Velocity Verlet steps (bounded run)."""
+def cpu_baseline(cfg, threads, budget_s=15.0):
+    """bond-updates/s of the oracle sample over whole Velocity Verlet steps (a run of about
+    budget_s seconds)."""
     b, dt, (sx, sy, sz) = oracle_sample(cfg, threads)
     steps, t0 = 0, time.perf_counter()
     while True:
         b.run_vv(steps + 1, 1, dt)
         steps += 1
         el = time.perf_counter() - t0
-        if el > budget_s or steps >= 50:
+        if el > budget_s or steps >= 5000:
             break
     return {"value": b.n_bonds * steps / el, "unit": UNIT, "cores": threads, "kind": "port",
             "sample": f"{sx}x{sy}x{sz} sub-block ({b.n} points, {b.n_bonds} bonds) of the same "

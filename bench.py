@@ -37,6 +37,8 @@ CONFIGS = {
     "osb1m": (200, 100, 50, 1e-3, "OSB", 0.0, 0.6),
     "bb1m": (200, 100, 50, 1e-3, "BB", 0.0, 0.6),
     "c1m": (200, 100, 50, 1e-3, "C", 0.0, 0.6),
+    # 64 CMat NeoHooke specimens of 20k-200k points in one device body (see make_ensemble)
+    "ens64": (0, 0, 0, 1e-3, "C", 0.0, 0.6),
 }
 # algorithmic bytes (FP32-compensated form): per directed bond nbr 4 + xi 12 + L 4 + 1/8 bit;
 # per point 140 (u, v FP64 read+write, own u, b_ext/BC, parameter id, damage) + 8 for OSB
@@ -73,6 +75,77 @@ def make_body(cfg, jitter_seed=None):
     pd.velocity_bc(lambda t: -vbc, body, "ymin", "y")
     pd.velocity_bc(lambda t: vbc, body, "ymax", "y")
     return body, frac
+
+
+def make_ensemble(n=64, seed=0xE45, dx=1e-3, vbc=0.6):
+    """Specimens of the ensemble workload: cuboids of aspect 4:2:1 with a seeded point count
+    in [20k, 200k] at dx = 1 mm, horizon 3.015 dx, CMaterial (NeoHooke, ZEM Cs = 0.5),
+    E ~ U[50, 200] GPa, nu = 0.3, rho ~ U[2000, 8000] kg/m^3, Gc = 100 J/m^2, an edge crack on
+    the plane y = 0 from the x-min face of length ~ U[0.1, 0.4] of the specimen length
+    (precrack! filter), +-vbc m/s on the outermost y layers."""
+    import pdcuda as pd
+    rng = np.random.default_rng(seed)
+    bodies = []
+    for _ in range(n):
+        m = max(3, int(round((rng.uniform(20e3, 200e3) / 8.0) ** (1.0 / 3.0))))
+        E, rho, a = rng.uniform(50e9, 200e9), rng.uniform(2000.0, 8000.0), rng.uniform(0.1, 0.4)
+        pos, vol = pd.uniform_box(4 * m * dx, 2 * m * dx, m * dx, dx)
+        body = pd.Body(pd.CMaterial(model=pd.NeoHooke()), pos, vol)
+        pd.material(body, horizon=3.015 * dx, rho=rho, E=E, nu=0.3, Gc=100.0)
+        x, y = pos[0], pos[1]
+        tip = x.min() + a * (x.max() - x.min())
+        pd.point_set(body, "crack_a", np.nonzero((y < 0) & (x <= tip))[0])
+        pd.point_set(body, "crack_b", np.nonzero((y >= 0) & (x <= tip))[0])
+        pd.precrack(body, "crack_a", "crack_b", update_dmg=False)
+        pd.point_set(body, "ymin", np.nonzero(y < y.min() + 0.5 * dx)[0])
+        pd.point_set(body, "ymax", np.nonzero(y > y.max() - 0.5 * dx)[0])
+        pd.velocity_bc(lambda t: -vbc, body, "ymin", "y")
+        pd.velocity_bc(lambda t: vbc, body, "ymax", "y")
+        bodies.append(body)
+    return bodies
+
+
+def run_ensemble(args, rank, world, local, dist):
+    """--config ens64: all specimens advanced together, every one with its own CFL step; one
+    step = one Velocity Verlet step of every specimen. Ranks own disjoint specimen sets
+    (replicas: no exchange)."""
+    import pdcuda as pd
+    from pdcuda.replicas import partition_specimens, reduce_max, reduce_sum
+    bodies = make_ensemble()
+    mine = partition_specimens([b.n_points for b in bodies], world)[rank]
+    t0 = time.perf_counter()
+    ens = pd.Ensemble([bodies[k] for k in mine], precision=args.precision, device=local,
+                      graph_steps=args.graph if args.graph else 50)
+    setup_s = time.perf_counter() - t0
+    g, b = ens.dev.autotune()
+    mapping = ens.dev.mapping()
+    if args.graph:
+        ens.dev.set_graph(args.graph)
+    ens.run(args.warmup)
+    n_pts, n_bonds, _ = ens.dev.info()
+    if dist:
+        dist.barrier()
+    with ClockSampler(local) as clk:
+        ms, a, bph, integ = ens.run_timed(args.warmup + 1, args.steps)
+    ms_max = reduce_max(ms, dist, f"cuda:{local}")
+    bonds_all = reduce_sum(n_bonds, dist, f"cuda:{local}")
+    value = bonds_all * args.steps / (ms_max / 1e3)
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None,
+                "dtype": "f32" if args.precision == "fp32" else "f64", "data": "synthetic",
+                "config": {"workload": "ens64: 64 CMat NeoHooke specimens of 20k-200k points (seeded), "
+                                       "edge cracks, +-0.6 m/s, own CFL step each, one device body",
+                           "specimens": len(mine), "points": n_pts, "bonds": n_bonds,
+                           "mapping": dict(zip(("group", "block", "pipe"), mapping)),
+                           "graph_steps": args.graph if args.graph else 50,
+                           "setup_s": setup_s, "parallelism": f"replicas x{world}"},
+                "ms": {"phase_a": a / args.steps, "phase_b": bph / args.steps,
+                       "integrate": integ / args.steps},
+                "clocks": clk.summary()}
+        print(json.dumps(line), flush=True)
+    ens.close()
 
 
 class ClockSampler:
@@ -371,6 +444,12 @@ def main():
         return
     if args.jfnk_increments < 0:
         args.jfnk_increments = 2
+    if args.config == "ens64" and args.impl == "ours":
+        run_ensemble(args, rank, world, local, dist)
+        if dist:
+            dist.barrier()
+            dist.destroy_process_group()
+        return
 
     if args.impl == "reference":
         run_reference(args, rank, world)

@@ -481,8 +481,14 @@ __device__ void pk1_32(int cmodel, const DevParam& p, const float* H, float* P) 
 // -------------------------------------------------------------------------------------------
 // CMat phase A (correspondence.jl:193-224, 288-298; bond_system.jl:309-327)
 // -------------------------------------------------------------------------------------------
+// the correspondence phase A keeps 15 compensated 3x3 sums per point: it gets its own
+// occupancy bound (PD_MINB_CA resident blocks per SM). Measured on the 1M-point CMat block:
+// 1.50 / 1.44 / 1.49 ms at 2 / 3 / 4 blocks (109 / 80 / 64 registers).
+#ifndef PD_MINB_CA
+#define PD_MINB_CA 3
+#endif
 template <int G>
-__global__ void PD_LB k_c_a32(DevBody d, int kstep) {
+__global__ void __launch_bounds__(256, PD_MINB_CA) k_c_a32(DevBody d, int kstep) {
   if (d.ctrl->err) return;
   PD_SLICE_LOOP(G) {
     PD_SLICE_SETUP

@@ -76,7 +76,22 @@ class Ensemble:
                 body.data_bcs.append(cc)
             body.single_dim_ics += [ren(c) for c in b.single_dim_ics]
             body.posdep_single_dim_ics += [ren(c) for c in b.posdep_single_dim_ics]
-            body.point_sets_precracks += [(f"s{k}:{a}", f"s{k}:{c}", f) for a, c, f in b.point_sets_precracks]
+        # pre-cracks: the c-th crack of every specimen (of one mode) becomes one crack of the
+        # ensemble. No bond joins two specimens, so the union of the a-sets against the union
+        # of the b-sets selects exactly the bonds each specimen's own crack selects.
+        for mode in (True, False):
+            per = [[(a, c) for a, c, f in b.point_sets_precracks if f == mode] for b in self.bodies]
+            for c in range(max((len(p) for p in per), default=0)):
+                sa, sb = [], []
+                for k, p in enumerate(per):
+                    if c < len(p):
+                        o = self.offsets[k]
+                        sa.append(np.asarray(self.bodies[k].point_sets[p[c][0]]) + o)
+                        sb.append(np.asarray(self.bodies[k].point_sets[p[c][1]]) + o)
+                tag = "filter" if mode else "damage"
+                body.point_sets[f"{tag}{c}:a"] = np.concatenate(sa)
+                body.point_sets[f"{tag}{c}:b"] = np.concatenate(sb)
+                body.point_sets_precracks.append((f"{tag}{c}:a", f"{tag}{c}:b", mode))
         return body
 
     def run(self, n_steps, first_step=1):
@@ -85,6 +100,10 @@ class Ensemble:
         if first_step == 1:
             self.dev.force(0.0, float(self.dt.min()))
         self.dev.run(first_step, n_steps, -1.0)
+
+    def run_timed(self, first_step, n_steps):
+        """run() with CUDA events: (total, force phase A, phase B, integration) ms."""
+        return self.dev.run_timed(first_step, n_steps, -1.0)
 
     def field(self, name, k):
         """Storage field of specimen k: 3 x n_k (9 x n_k) point vectors (tensors), n_k point

@@ -10,7 +10,7 @@ from helpers import oracle_bcs, oracle_body
 pytestmark = pytest.mark.gpu
 
 
-def specimen(mat_factory, nx, ny, nz, E, rho, crack_frac, seed, dx=1e-3):
+def specimen(mat_factory, nx, ny, nz, E, rho, crack_frac, seed, dx=1e-3, filt=False):
     lx, ly, lz = nx * dx, ny * dx, nz * dx
     pos, vol = pd.uniform_box(lx, ly, lz, dx, center=(lx / 2, ly / 2, lz / 2))
     mat = mat_factory()
@@ -22,7 +22,7 @@ def specimen(mat_factory, nx, ny, nz, E, rho, crack_frac, seed, dx=1e-3):
     a = crack_frac * lx
     pd.point_set(body, "ca", where=lambda p: (p[1] <= ly / 2) & (p[0] < a))
     pd.point_set(body, "cb", where=lambda p: (p[1] > ly / 2) & (p[0] < a))
-    pd.precrack(body, "ca", "cb")
+    pd.precrack(body, "ca", "cb", update_dmg=not filt)
     pd.point_set(body, "left", where=lambda p: p[0] < 1.5 * dx)
     pd.point_set(body, "right", where=lambda p: p[0] > lx - 1.5 * dx)
     pd.velocity_bc(lambda t: -0.6, body, "left", "x")
@@ -31,14 +31,14 @@ def specimen(mat_factory, nx, ny, nz, E, rho, crack_frac, seed, dx=1e-3):
     return body
 
 
-def build(mat_factory):
+def build(mat_factory, filt=False):
     rng = np.random.default_rng(7)
     bodies = []
     for k in range(3):
         nx, ny, nz = int(rng.integers(10, 16)), int(rng.integers(6, 10)), 3
         bodies.append(specimen(mat_factory, nx, ny, nz, E=float(rng.uniform(50e9, 200e9)),
                                rho=float(rng.uniform(2000, 8000)),
-                               crack_frac=float(rng.uniform(0.1, 0.4)), seed=k))
+                               crack_frac=float(rng.uniform(0.1, 0.4)), seed=k, filt=filt))
     return bodies
 
 
@@ -74,3 +74,21 @@ def test_ensemble_rejects_mixed_materials():
     b = specimen(pd.OSBMaterial, 8, 6, 3, 70e9, 2700, 0.2, 0)
     with pytest.raises(ValueError):
         pd.Ensemble([a, b])
+
+
+def test_ensemble_with_filter_cracks_matches_specimens_run_alone():
+    """precrack!(...; update_dmg=false) of every specimen: the ensemble merges the k-th crack of
+    all specimens into one filter (no bond joins two specimens); bonds and trajectories equal
+    those of each specimen alone, bit for bit in serial FP64 order."""
+    bodies = build(pd.BBMaterial, filt=True)
+    ens = pd.Ensemble(bodies, precision="fp64")
+    ens.dev.set_mapping(0)
+    ens.run(40)
+    for k, b in enumerate(bodies):
+        ob = oracle_body(b)
+        dt = ob.stable_timestep(0.7)
+        ob.force_density(0.0, dt)
+        assert ob.run_vv(1, 40, dt, oracle_bcs(b, 1, 40, dt)) == 0
+        assert np.array_equal(ens.field("n_neighbors", k), ob.n_neighbors)
+        assert np.array_equal(ens.field("displacement", k).T, ob.u)
+    ens.close()

@@ -61,15 +61,20 @@ class VelocityVerlet:
 
 
 class Job:
-    """A simulation job (src/core/job.jl:45-62). ``export`` replaces the VTK writer: it is
-    called as export(step, t, sim) every ``freq`` steps and at step 0 when given."""
+    """A simulation job (src/core/job.jl:45-62). With a ``path`` the fields are written as VTK
+    files in the reference's layout (``pdcuda.vtk``: `<path>/vtk/timestep_<n>.pvtu` at step 0
+    and every ``freq`` steps); ``export`` (a callable export(step, t, sim)) replaces the writer."""
 
     def __init__(self, body, solver, path="", freq=10, fields=None, export=None,
                  precision="fp64", graph_steps=0, mapping=None, device=0):
         if freq < 0:
             raise ValueError("`freq` should be larger than zero!")
         self.body, self.solver = body, solver
-        self.path, self.freq, self.fields, self.export = path, int(freq), fields, export
+        self.path, self.freq, self.fields = path, int(freq), fields
+        if export is None and path:
+            from .vtk import VtkExport
+            export = VtkExport(path, freq, fields)
+        self.export = export
         self.precision, self.graph_steps, self.mapping, self.device = precision, graph_steps, mapping, device
 
 

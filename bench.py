@@ -41,13 +41,28 @@ CONFIGS = {
     "pulse1m": (200, 100, 50, 1e-3, "OSB", 0.0, 0.0),
     # 64 CMat NeoHooke specimens of 20k-200k points in one device body (see make_ensemble)
     "ens64": (0, 0, 0, 1e-3, "C", 0.0, 0.6),
+    # dynamic relaxation of an OSB block in uniform tension (see make_dr_block)
+    "dr1m": (200, 100, 50, 1e-3, "OSB", 0.0, 0.0),
 }
+DR_STRAIN = 5e-5
+# algorithmic bytes per point of the damping and velocity-update kernels of one relaxation step
+# (damping: u, v_half, b_int, b_int_old, v_half_old, Lambda; update: Lambda, b_int, b_ext,
+# v_half_old read, v_half, v, v_half_old, b_int_old written)
+B_DR_POINT = {"fp64": 328.0, "fp32": 304.0}
 # algorithmic bytes (FP32-compensated form): per directed bond nbr 4 + xi 12 + L 4 + 1/8 bit;
 # per point 140 (u, v FP64 read+write, own u, b_ext/BC, parameter id, damage) + 8 for OSB
 # (m, theta) + 72 for CMat (F, P K^-1)
 B_BOND = {"fp32": 20.125, "fp64": 36.125}
 B_POINT = {"fp32": 140.0, "fp64": 184.0}
 B_POINT_EXTRA = {"BB": 0.0, "OSB": 8.0, "C": 72.0}
+
+
+def pinned(*shape):
+    """A zeroed float64 host array in page-locked memory (torch owns the allocation; the
+    returned tensor keeps it alive)."""
+    import torch
+    t = torch.zeros(shape, dtype=torch.float64, pin_memory=True)
+    return t, t.numpy()
 
 
 def load_peaks():
@@ -77,6 +92,30 @@ def make_body(cfg, jitter_seed=None):
     pd.velocity_bc(lambda t: -vbc, body, "ymin", "y")
     pd.velocity_bc(lambda t: vbc, body, "ymax", "y")
     return body, frac
+
+
+def make_dr_block(nx, ny, nz, dx, mat="OSB"):
+    """A block in uniform tension for dynamic relaxation (the reference's relaxation bar at
+    scale): the two x = min layers held by zero velocity conditions, a force density on the
+    x = max layer that gives the strain DR_STRAIN, no pre-damage."""
+    import pdcuda as pd
+    pos, vol = pd.uniform_box(nx * dx, ny * dx, nz * dx, dx)
+    material = {"OSB": pd.OSBMaterial, "BB": pd.BBMaterial,
+                "C": lambda: pd.CMaterial(model=pd.NeoHooke())}[mat]()
+    body = pd.Body(material, pos, vol)
+    kw = dict(horizon=3.015 * dx, rho=2700.0, E=70e9, Gc=100.0)
+    if mat != "BB":
+        kw["nu"] = 0.25
+    pd.material(body, **kw)
+    x = body._pos[:, 0]
+    pd.point_set(body, "left", np.nonzero(x < x.min() + 1.5 * dx)[0])
+    right = np.nonzero(x > x.max() - 0.5 * dx)[0]
+    pd.point_set(body, "right", right)
+    b_right = DR_STRAIN * 70e9 * (ny * dx) * (nz * dx) / vol[right].sum()
+    for d in ("x", "y", "z"):
+        pd.velocity_bc(lambda t: 0.0, body, "left", d)
+    pd.forcedensity_bc(lambda t: b_right, body, "right", "x")
+    return body
 
 
 def make_ensemble(n=64, seed=0xE45, dx=1e-3, vbc=0.6):
@@ -305,24 +344,165 @@ def cpu_baseline(cfg, threads, budget_s=15.0):
                       f"lattice and parameters, {steps} FP64 VV steps in {el:.1f} s"}
 
 
+def dr_oracle_sample(cfg, threads):
+    """The FP64 oracle with its dynamic relaxation on a 64x64x40 sub-block of the dr1m block
+    (same spacing, parameters and loading), initialised and ready to step."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    from dr import OracleDR
+    nx, ny, nz, dx, mat, frac, vbc = CONFIGS[cfg]
+    sx, sy, sz = min(nx, 64), min(ny, 64), min(nz, 40)
+    g = lambda n: (np.arange(n) - (n - 1) / 2) * dx
+    X = np.array(np.meshgrid(g(sx), g(sy), g(sz), indexing="ij")).reshape(3, -1).T
+    X = np.ascontiguousarray(X[np.lexsort((X[:, 0], X[:, 1], X[:, 2]))])
+    V = np.full(len(X), dx ** 3)
+    om = {"OSB": O.OSB, "BB": O.BB, "C": O.CMAT}[mat]
+    kw = {} if mat == "BB" else {"nu": 0.25}
+    p = O.point_params(om, 3.015 * dx, 2700.0, E=70e9, Gc=100.0, **kw)
+    O.set_threads(threads)
+    b = O.OracleBody(om, X, V, [p], cmodel=O.NEOHOOKE)
+    left = np.nonzero(X[:, 0] < X[:, 0].min() + 1.5 * dx)[0]
+    right = np.nonzero(X[:, 0] > X[:, 0].max() - 0.5 * dx)[0]
+    b_right = DR_STRAIN * 70e9 * (sy * dx) * (sz * dx) / V[right].sum()
+    bcs = [dict(field=0, dim=d, kind=2, pts=left, values=np.zeros(len(left))) for d in range(3)]
+    bcs.append(dict(field=1, dim=0, kind=2, pts=right, values=np.full(len(right), b_right)))
+    dr = OracleDR(b, 1.0, fast=True)
+    b.force_density(0.0, 1.0)
+    return b, dr, bcs, (sx, sy, sz)
+
+
+def dr_cpu_baseline(cfg, threads, budget_s=15.0):
+    """bond-updates/s of the oracle sample over whole relaxation steps (about budget_s s)."""
+    b, dr, bcs, (sx, sy, sz) = dr_oracle_sample(cfg, threads)
+    steps, t0 = 0, time.perf_counter()
+    while True:
+        steps += 1
+        dr.step(steps, bcs)
+        el = time.perf_counter() - t0
+        if el > budget_s or steps >= 5000:
+            break
+    return {"value": b.n_bonds * steps / el, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"{sx}x{sy}x{sz} sub-block ({b.n} points, {b.n_bonds} bonds) of the same "
+                      f"lattice, parameters and loading, {steps} FP64 relaxation steps in {el:.1f} s "
+                      f"(force on all threads, damping sums in numpy)"}
+
+
+def run_dr(args, rank, world, local, dist):
+    """--config dr1m: dynamic relaxation of a 1M-point OSB block in uniform tension; one step =
+    one relaxation step (conditions and drift, force density, damping, velocity update).
+    Ranks run independent replicas."""
+    import pdcuda as pd
+    from pdcuda import dynamic_relaxation as drm
+    from pdcuda.replicas import reduce_max
+    nx, ny, nz, dx, mat, _, _ = CONFIGS[args.config]
+    prec = args.precision
+    body = make_dr_block(nx, ny, nz, dx, mat)
+    dev = pd.DeviceBody(body, precision=prec, device=local)
+    n_pts, n_bonds, _ = dev.info()
+    dev.autotune()
+    mapping = dev.mapping()
+    dr = pd.DynamicRelaxation(steps=args.warmup + args.steps)
+    drm.init(dev, dr)
+    drm.run(dev, dr, 1, args.warmup)
+    launches0 = dev.launch_count()
+
+    def barrier():
+        if dist:
+            import torch
+            dist.barrier()
+            torch.cuda.synchronize()
+
+    barrier()
+    with ClockSampler(local) as clk:
+        ms, ms_drift, ms_force, ms_relax = drm.run_timed(dev, dr, args.warmup + 1, args.steps)
+    launches = dev.launch_count() - launches0
+    barrier()
+    ms_max = reduce_max(ms, dist, f"cuda:{local}")
+    value = n_bonds * args.steps * world / (ms_max / 1e3)
+    right = body.point_sets["right"]
+    u = dev.field("displacement")
+    exact = DR_STRAIN * (body._pos[right, 0].mean() - body._pos[body.point_sets["left"], 0].max())
+    progress = float(u[0, right].mean() / exact)
+    # roofline: the force kernels of a step (OSB: phases A and B each stream every bond once)
+    n_phase = 1 if mat == "BB" else 2
+    pt = {"fp32": 64 + 8 + 16 + 4 + 4, "fp64": 128 + 8 + 32 + 4 + 4}[prec]
+    force_bytes = n_phase * (n_bonds * B_BOND[prec] + n_pts * pt)
+    peak, peak_kind = load_peaks()
+    force_ms = ms_force / args.steps
+    achieved = force_bytes / (force_ms / 1e3) / 1e9
+    relax_ms = ms_relax / args.steps
+    relax_gbs = n_pts * B_DR_POINT[prec] / (relax_ms / 1e3) / 1e9
+
+    # end to end through the public API with host buffers: upload the state, restart the
+    # relaxation, run, read back
+    # (page-locked host buffers)
+    bufs = [pinned(n_pts, 3), pinned(n_pts, 3), pinned(n_pts, 3), pinned(n_pts)]
+    h_u, h_v, out_u, out_d = (b[1] for b in bufs)
+    barrier()
+    t0 = time.perf_counter()
+    dev.set_state(displacement=h_u, velocity=h_v)
+    drm.init(dev, dr)
+    drm.run(dev, dr, 1, args.steps)
+    dev.field("displacement", out=out_u)
+    dev.field("damage", out=out_d)
+    e2e_s = reduce_max(time.perf_counter() - t0, dist, f"cuda:{local}")
+    e2e = n_bonds * args.steps * world / e2e_s
+    dev.close()
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu = dr_cpu_baseline(args.config, os.cpu_count() or 1)
+    if rank == 0:
+        line = {
+            "metric": "bond-updates/s per relaxation step", "value": value, "unit": UNIT,
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32" if prec == "fp32" else "f64", "data": "synthetic",
+            "config": {"workload": f"dr1m: {mat} {nx}x{ny}x{nz} points, dx={dx}, horizon 3.015dx, "
+                                   f"uniform tension (strain {DR_STRAIN}), dynamic relaxation step",
+                       "points": n_pts, "bonds": n_bonds, "precision": prec,
+                       "mapping": dict(zip(("group", "block", "pipe"), mapping)),
+                       "l2": "inputs larger than L2 (bond arrays of ~2.5 GB)",
+                       "parallelism": f"replicas x{world}"},
+            "roofline": {"bound": "hbm", "kernel": f"{mat.lower()} force (all phases of a step)",
+                         "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": None, "peak_kind": peak_kind,
+                         "alg_bytes_per_step": force_bytes, "ms_per_step": force_ms},
+            "relax_kernels": {"ms_per_step": relax_ms, "alg_bytes_per_step": n_pts * B_DR_POINT[prec],
+                              "achieved_gbs": relax_gbs, "frac": relax_gbs / peak},
+            "ms": {"drift": ms_drift / args.steps, "force": force_ms, "relax": relax_ms},
+            "relaxation": {"steps": args.warmup + args.steps, "elongation_over_exact": progress},
+            "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": (h_u.nbytes + h_v.nbytes) / args.steps,
+                    "d2h_bytes_per_step": (out_u.nbytes + out_d.nbytes) / args.steps},
+            "gpu_launches": launches, "clocks": clk.summary(), "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+
+
 def run_reference(args, rank, world):
     """The reference arm: the CPU restatement of the reference (Julia is not installed) on all
     host threads; every step is one Velocity Verlet step of the bounded sample."""
     if rank != 0:
         return
     threads = os.cpu_count() or 1
-    b, dt, (sx, sy, sz) = oracle_sample(args.config, threads)
+    if args.config == "dr1m":
+        b, dr, bcs, (sx, sy, sz) = dr_oracle_sample(args.config, threads)
+        step = lambda n: dr.step(n, bcs)
+    else:
+        b, dt, (sx, sy, sz) = oracle_sample(args.config, threads)
+        step = lambda n: b.run_vv(n, 1, dt)
     for k in range(max(args.warmup, 0)):
-        b.run_vv(k + 1, 1, dt)
+        step(k + 1)
     t0 = time.perf_counter()
     for k in range(args.steps):
-        b.run_vv(args.warmup + k + 1, 1, dt)
+        step(args.warmup + k + 1)
     el = time.perf_counter() - t0
     v = b.n_bonds * args.steps / el
     nx, ny, nz, dx, mat, frac, vbc = CONFIGS[args.config]
+    kind = "relaxation" if args.config == "dr1m" else "VV"
     sample = (f"{sx}x{sy}x{sz} sub-block ({b.n} points, {b.n_bonds} bonds) of the {args.config} "
-              f"lattice and parameters, {args.steps} FP64 VV steps in {el:.2f} s")
-    line = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+              f"lattice and parameters, {args.steps} FP64 {kind} steps in {el:.2f} s")
+    metric = "bond-updates/s per relaxation step" if args.config == "dr1m" else METRIC
+    line = {"metric": metric, "value": v, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1e3 * el / max(args.steps, 1),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic", "impl": "reference",
@@ -521,6 +701,12 @@ def main():
             dist.barrier()
             dist.destroy_process_group()
         return
+    if args.config == "dr1m" and args.impl == "ours":
+        run_dr(args, rank, world, local, dist)
+        if dist:
+            dist.barrier()
+            dist.destroy_process_group()
+        return
     if args.config == "ens64" and args.impl == "ours":
         run_ensemble(args, rank, world, local, dist)
         if dist:
@@ -625,15 +811,15 @@ def main():
         dev.set_graph(args.graph)
 
     # end to end through the public API with host buffers: upload the state, run, read back
-    h_u = np.ascontiguousarray(np.zeros((n_pts, 3)))
-    h_v = np.ascontiguousarray(np.zeros((n_pts, 3)))
-    h_v[:, 1] = 0.0
+    # (page-locked host buffers)
+    bufs = [pinned(n_pts, 3), pinned(n_pts, 3), pinned(n_pts, 3), pinned(n_pts)]
+    h_u, h_v, out_u, out_d = (b[1] for b in bufs)
     barrier()
     t0 = time.perf_counter()
     dev.set_state(displacement=h_u, velocity=h_v)
     dev.run(1, args.steps, dt)
-    out_u = dev.field("displacement")
-    out_d = dev.field("damage")
+    dev.field("displacement", out=out_u)
+    dev.field("damage", out=out_d)
     e2e_s = time.perf_counter() - t0
     e2e_s = max_over_ranks(e2e_s)
     h2d = (h_u.nbytes + h_v.nbytes) / args.steps

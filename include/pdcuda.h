@@ -264,6 +264,31 @@ pd_status pd_launch_count(pd_handle *h, int64_t *count);
 pd_status pd_stream(pd_handle *h, void **stream);
 
 /* ---------------------------------------------------------------------------------------
+ * Dynamic relaxation (src/time_solvers/dynamic_relaxation.jl): adaptive-damping explicit
+ * steps towards a static state on the same force kernels as Velocity Verlet.
+ * --------------------------------------------------------------------------------------- */
+
+/* init_density_matrix! (dynamic_relaxation.jl:109-164): the fictitious density
+ * Lambda_i = damping_factor / 4 dt^2 n_i 5 pi delta^2 bc of every point, v_half_old and
+ * b_int_old cleared. dt is the relaxation step (DynamicRelaxation stepsize). */
+pd_status pd_dr_init(pd_handle *h, double dt, double damping_factor);
+
+/* relaxation_timestep! (:191-211, 269-370) for steps first_step .. first_step + n_steps - 1:
+ * conditions and drift, force density, damping coefficient (steps > 1), velocity update.
+ * Boundary values come from pd_set_bc_values as for pd_run_vv. PD_ERR_NAN as pd_run_vv. With
+ * the serial mapping (pd_set_mapping group 0) the damping sums follow the reference's order. */
+pd_status pd_run_dr(pd_handle *h, int64_t first_step, int64_t n_steps);
+
+/* pd_run_dr with CUDA events around every phase: elapsed milliseconds of the whole run, of the
+ * conditions and drift kernels, of the force kernels and of the damping and velocity-update
+ * kernels, summed over the steps. Same effect on the state as pd_run_dr. */
+pd_status pd_run_dr_timed(pd_handle *h, int64_t first_step, int64_t n_steps, double *ms_total,
+                          double *ms_drift, double *ms_force, double *ms_relax);
+
+/* Lambda of every point (n doubles, host). */
+pd_status pd_dr_density_matrix(pd_handle *h, double *out);
+
+/* ---------------------------------------------------------------------------------------
  * Quasi-static Jacobian-free Newton-Krylov solve (src/time_solvers/newton_krylov.jl).
  * Needs a PD_PREC_FP64 handle without fracture (validate_chunk_for_newton_krylov!,
  * newton_krylov.jl:219-253). Position-dependent conditions f(p) are evaluated by the host at

@@ -546,6 +546,7 @@ extern "C" pd_status pd_destroy(pd_handle* h) {
   if (h->stream) cudaStreamSynchronize(h->stream);
   destroy_graph(h);
   pd::nk_release(h);
+  pd::dr_release(h);
   for (void* p : h->allocs) cudaFree(p);
   h->allocs.clear();
   if (h->stream) cudaStreamDestroy(h->stream);
@@ -560,6 +561,23 @@ static pd_status clear_error(pd_handle* h) {
   return PD_OK;
 }
 
+// cur[i].xyz = in[3i..3i+2] (- X0[i].xyz with sub_x0); the fourth component is kept
+__global__ void k_set_cur(double4* cur, const double4* X0, const double* in, long long n, int sub_x0) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double4 c = cur[i];
+  c.x = in[3 * i];
+  c.y = in[3 * i + 1];
+  c.z = in[3 * i + 2];
+  if (sub_x0) {
+    const double4 x = X0[i];
+    c.x = c.x - x.x;
+    c.y = c.y - x.y;
+    c.z = c.z - x.z;
+  }
+  cur[i] = c;
+}
+
 extern "C" pd_status pd_set_state(pd_handle* h, const double* position, const double* displacement,
                                   const double* velocity, const double* velocity_half,
                                   const double* acceleration, const double* b_ext,
@@ -569,30 +587,30 @@ extern "C" pd_status pd_set_state(pd_handle* h, const double* position, const do
   PD_CUDA(cudaStreamSynchronize(h->stream));
   const long long n = h->n, nb = h->nb;
   if (n == 0) return PD_OK;
-  std::vector<double4> cur(n);
-  PD_CUDA(cudaMemcpy(cur.data(), h->d.cur, sizeof(double4) * n, cudaMemcpyDeviceToHost));
-  std::vector<double4> X0(n);
-  PD_CUDA(cudaMemcpy(X0.data(), h->d.X0, sizeof(double4) * n, cudaMemcpyDeviceToHost));
-  bool cur_changed = false;
+  // the packed point state (FP64: current position; FP32: displacement) from a 3n host array,
+  // packed on the device
+  const double* src = nullptr;
+  int sub_x0 = 0;
   if (h->precision == PD_PREC_FP64) {
-    if (position) {
-      for (long long i = 0; i < n; i++) { cur[i].x = position[3 * i]; cur[i].y = position[3 * i + 1]; cur[i].z = position[3 * i + 2]; }
-      cur_changed = true;
-    }
+    src = position;
     if (displacement) PD_CUDA(cudaMemcpy(h->g.u, displacement, sizeof(double) * 3 * n, cudaMemcpyHostToDevice));
-  } else {
-    if (displacement) {
-      for (long long i = 0; i < n; i++) { cur[i].x = displacement[3 * i]; cur[i].y = displacement[3 * i + 1]; cur[i].z = displacement[3 * i + 2]; }
-      cur_changed = true;
-    } else if (position) {
-      for (long long i = 0; i < n; i++) {
-        cur[i].x = position[3 * i] - X0[i].x; cur[i].y = position[3 * i + 1] - X0[i].y; cur[i].z = position[3 * i + 2] - X0[i].z;
-      }
-      cur_changed = true;
-    }
+  } else if (displacement) {
+    src = displacement;
+  } else if (position) {
+    src = position;
+    sub_x0 = 1;
   }
-  if (cur_changed) {
-    PD_CUDA(cudaMemcpy(h->d.cur, cur.data(), sizeof(double4) * n, cudaMemcpyHostToDevice));
+  if (src) {
+    double* tmp = nullptr;
+    PD_CUDA(cudaMalloc(&tmp, sizeof(double) * 3 * n));
+    cudaError_t e = cudaMemcpy(tmp, src, sizeof(double) * 3 * n, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) {
+      k_set_cur<<<(unsigned)((n + 255) / 256), 256, 0, h->stream>>>(h->d.cur, h->d.X0, tmp, n, sub_x0);
+      e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    cudaFree(tmp);
+    if (e != cudaSuccess) return fail(PD_ERR_CUDA, cudaGetErrorString(e));
     launch_split_u(h->d, h->stream);
     PD_CUDA(cudaGetLastError());
   }

@@ -12,6 +12,8 @@
 namespace pd {
 struct NKState;  // quasi-static Newton-Krylov solver state (pd_nk.cu)
 void nk_release(pd_handle* h);
+struct DRState;  // dynamic relaxation state (pd_dr.cu)
+void dr_release(pd_handle* h);
 }
 
 // sets the thread's last error message and returns code
@@ -84,6 +86,7 @@ struct pd_handle {
   long long nan_step = -1;
   long long nslots = 0;
   pd::NKState* nk = nullptr;  // created by the first pd_nk_* call
+  pd::DRState* dr = nullptr;  // created by pd_dr_init
 };
 
 template <class T>

@@ -57,6 +57,10 @@ __global__ void k_kick_drift(DevBody d, IntDev g, int mode, double dt_override, 
   double vh[3];
   for (int k = 0; k < 3; k++) {
     const long long q = 3 * i + k;
+    if (mode == 2) {  // dynamic relaxation: drift with the stored v_half
+      vh[k] = g.vh[q];
+      continue;
+    }
     if (mode == 1) {
       double b = bint(d, g, q);
       if (meta & META_HAS_BEXT) b = b + g.bext[q];

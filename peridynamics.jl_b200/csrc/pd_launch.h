@@ -9,7 +9,8 @@ struct LaunchCfg {
   int group;  // lanes per point: 1, 2, 4, 8, 16, 32
   int block;  // threads per block
   bool exact; // FP64: one lane per point in the reference's serial summation order
-  int pipe;   // FP32: 0 = plain loads, > 0 = TMA-staged bond stream (pd_force32_tma.cu)
+  int pipe;   // FP32: 0 = plain loads, 1-3 = TMA-staged bond stream (pd_force32_tma.cu),
+              // 4 = two rows of neighbour gathers in flight (OSB)
 };
 
 // boundary conditions as the integration kernels see them
@@ -52,7 +53,8 @@ bool tma_supported(const DevBody& d);
 int launch_force32_tma(const DevBody& d, int pipe, int kstep, int phase, cudaStream_t s);
 void launch_cauchy64(const DevBody& d, const double* F, int from_h32, double* out, cudaStream_t s);
 
-// integration: mode 0 = kick from the stored (v, a), mode 1 = kick from the last force
+// integration: mode 0 = kick from the stored (v, a), mode 1 = kick from the last force,
+// mode 2 = no kick (dynamic relaxation: drift with the stored v_half)
 void launch_kick_drift(const DevBody& d, const IntDev& g, int mode, double dt_override, int kstep,
                        cudaStream_t s);
 void launch_bc(const DevBody& d, const IntDev& g, const BCDev& bc, double dt_override, int kstep,

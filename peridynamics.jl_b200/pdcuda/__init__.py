@@ -16,6 +16,7 @@ from .body import (Body, point_set, material, failure_permit, no_failure, veloci
 from .solver import VelocityVerlet, Job, DeviceBody, submit
 from .ensemble import Ensemble
 from .newton_krylov import NewtonKrylov
+from .dynamic_relaxation import DynamicRelaxation
 from . import mpnn
 from ._lib import NotConvergedError
 

@@ -40,6 +40,7 @@ EXPORTS = (
     "pd_set_bcs", "pd_set_bc_values", "pd_stable_timestep", "pd_set_param_timesteps",
     "pd_force", "pd_run_vv", "pd_nan_step", "pd_run_vv_timed", "pd_autotune", "pd_set_mapping",
     "pd_set_graph", "pd_set_pipeline", "pd_get_mapping", "pd_info", "pd_launch_count", "pd_stream",
+    "pd_dr_init", "pd_run_dr", "pd_run_dr_timed", "pd_dr_density_matrix",
     "pd_nk_set_conditions", "pd_nk_step", "pd_nk_set_corrections", "pd_nk_apply",
     "pd_nk_record", "pd_nk_recorded", "pd_nk_recorded_vector",
     "pd_mpnn_create", "pd_mpnn_destroy", "pd_mpnn_set_params", "pd_mpnn_get_params",
@@ -148,6 +149,10 @@ def lib():
         "pd_launch_count": [vp, vp],
         "pd_stream": [vp, vp],
         "pd_osb_force_static": [i64] + [vp] * 8 + [vp, i32, vp, vp, vp],
+        "pd_dr_init": [vp, dbl, dbl],
+        "pd_run_dr": [vp, i64, i64],
+        "pd_run_dr_timed": [vp, i64, i64, vp, vp, vp, vp],
+        "pd_dr_density_matrix": [vp, vp],
         "pd_nk_set_conditions": [vp, i32, vp],
         "pd_nk_step": [vp, i64, dbl, vp, vp],
         "pd_nk_set_corrections": [vp, vp],

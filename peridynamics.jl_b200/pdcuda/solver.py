@@ -220,16 +220,17 @@ class DeviceBody:
         self._keep = args + [ba]
         L.check(L.lib().pd_set_state(self.h, *[L.ptr(a) for a in args], L.ptr(ba)), "pd_set_state")
 
-    def field(self, name):
+    def field(self, name, out=None):
         """A storage field: point vectors / tensors as 3 x N / 9 x N views (the reference's
-        layout), scalars as N, bond_active as n_bonds bytes."""
+        layout), scalars as N, bond_active as n_bonds bytes. out: a C-contiguous array of the
+        field's size and type to read into (pinned host memory makes the copy faster)."""
         fid, comp, dt = _FIELDS[name]
-        if comp == 0:
-            out = np.empty(self.n_bonds, dt)
-        elif comp == 1:
-            out = np.empty(self.n, dt)
-        else:
-            out = np.empty((self.n, comp), dt)
+        shape = (self.n_bonds,) if comp == 0 else (self.n,) if comp == 1 else (self.n, comp)
+        if out is None:
+            out = np.empty(shape, dt)
+        elif out.dtype != dt or out.size != int(np.prod(shape)) or not out.flags.c_contiguous:
+            raise ValueError(f"out must be a C-contiguous {np.dtype(dt).name} array of {np.prod(shape)} elements")
+        out = out.reshape(shape)
         L.check(L.lib().pd_get_field(self.h, fid, L.ptr(out), out.nbytes), f"pd_get_field({name})")
         return out.T if comp > 1 else out
 
@@ -341,7 +342,13 @@ def submit(job: Job, quiet=True):
         if job.mapping is not None:
             dev.set_mapping(*job.mapping)
         return nk_solve(dev, job.solver, job.export, job.freq if job.export is not None else 0)
+    from .dynamic_relaxation import DynamicRelaxation, solve as dr_solve
     check_conditions_applicable(job.body, job.solver)
+    if isinstance(job.solver, DynamicRelaxation):
+        dev = DeviceBody(job.body, precision=job.precision, device=job.device)
+        if job.mapping is not None:
+            dev.set_mapping(*job.mapping)
+        return dr_solve(dev, job.solver, job.export, job.freq if job.export is not None else 0)
     vv = job.solver
     dev = DeviceBody(job.body, precision=job.precision, device=job.device)
     if job.mapping is not None:

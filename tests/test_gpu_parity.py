@@ -323,3 +323,25 @@ def test_two_row_osb_kernels_equal_one_row(group):
         out.append([dev.field(f) for f in ("b_int", "n_active_bonds", "bond_active", "damage")])
     for a, b in zip(*out):
         assert np.array_equal(a, b)
+
+
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+def test_set_state_round_trip(prec):
+    """Positions and displacements set from host arrays read back unchanged (FP64 keeps the
+    position, FP32 the displacement: the other is derived), also into a caller's buffer."""
+    body = cube_body(pd.OSBMaterial(), n=5)
+    dev = pd.DeviceBody(body, precision=prec)
+    X = body._pos
+    u = deform(X)
+    key = "position" if prec == "fp64" else "displacement"
+    val = X + u if prec == "fp64" else u
+    dev.set_state(**{key: val})
+    buf = np.full((dev.n, 3), np.nan)
+    got = dev.field(key, out=buf)
+    assert np.shares_memory(got, buf) and np.array_equal(got.T, val)
+    if prec == "fp32":
+        dev.set_state(position=X + 2 * u)
+        assert np.array_equal(dev.field("displacement").T, (X + 2 * u) - X)
+    with pytest.raises(ValueError):
+        dev.field(key, out=np.empty((dev.n, 2)))
+    dev.close()

@@ -182,6 +182,12 @@ pd_status pd_break_bonds(pd_handle *h, const uint8_t *set_a, const uint8_t *set_
  * `fraction`, decided by a hash of (min(i,j), max(i,j), seed), so both directions agree. */
 pd_status pd_break_random_pairs(pd_handle *h, double fraction, uint64_t seed);
 
+/* pd_break_random_pairs hashing point_ids[i] (n int64, host) instead of the row numbers: a
+ * partition passes the body's point numbers of its rows and breaks the same pairs as the
+ * undivided body. */
+pd_status pd_break_random_pairs_ids(pd_handle *h, double fraction, uint64_t seed,
+                                    const int64_t *point_ids);
+
 /* Copies one storage field to host memory of `bytes` bytes (export_results,
  * threads_body_data_handler.jl:197-212). */
 pd_status pd_get_field(pd_handle *h, int32_t field, void *out, size_t bytes);
@@ -262,6 +268,57 @@ pd_status pd_launch_count(pd_handle *h, int64_t *count);
 
 /* The cudaStream_t of the handle, as an opaque pointer. */
 pd_status pd_stream(pd_handle *h, void **stream);
+
+/* ---------------------------------------------------------------------------------------
+ * Partitioned bodies: one partition per GPU with halo exchange between the stages of a
+ * step (the reference's MPI data handler, src/core/mpi_body_data_handler.jl: chop_body_mpi
+ * :102-109, exchange_loc_to_halo! :239-318, calc_force_density! :400-409; decomposition
+ * PointDecomposition / distribute_equally, src/discretization/decomposition.jl:32-63).
+ * --------------------------------------------------------------------------------------- */
+
+/* A partition of a body: desc holds its rows (owned points and halo points, in the body's
+ * point order) and owned[i] != 0 marks the owned rows. The search gives every owned row all
+ * its bonds and every halo row only its bonds to owned rows; halo rows take no part in the
+ * stable time step and leave the killed-point decision of CMaterial to their owner. Other
+ * arguments as pd_create_search. */
+pd_status pd_create_partition(const pd_body_desc *desc, const double *search_position,
+                              const uint8_t *fp_point, int32_t n_filters, const uint8_t *filter_a,
+                              const uint8_t *filter_b, const uint8_t *owned, pd_handle **out);
+
+/* Issues all further work of the handle on `stream` (a cudaStream_t of the same device; NULL
+ * returns to the handle's own stream), so that a communication library's transfers on that
+ * stream order with the kernels. Waits for the work issued so far. */
+pd_status pd_set_stream(pd_handle *h, void *stream);
+
+/* Velocity Verlet in stages (verlet_timestep!, velocity_verlet.jl:181-237, with the force
+ * density split at its halo exchanges): pd_vv_begin(first_step, n_steps, dt) opens a run
+ * (boundary values from pd_set_bc_values as for pd_run_vv); for kstep = 0 .. n_steps - 1 the
+ * caller issues stage 0 (half kick, conditions, drift), stage 1 (the first force kernel; BB:
+ * the whole force) and stage 2 (the second force kernel of OSB / CMat; nothing for BB);
+ * pd_vv_end issues the closing half kick, waits and reports PD_ERR_NAN as pd_run_vv. The
+ * sequence has the effect of pd_run_vv(first_step, n_steps, dt). Asynchronous except
+ * pd_vv_begin / pd_vv_end. */
+pd_status pd_vv_begin(pd_handle *h, int64_t first_step, int64_t n_steps, double dt);
+/* pd_force split like the stages: phase 1 issues the first force kernel, phase 2 the second
+ * one, then waits and reports PD_ERR_NAN (initialize! of a partition, with the kind-1
+ * exchange between the phases). */
+pd_status pd_force_phase(pd_handle *h, int32_t phase, double t, double dt);
+pd_status pd_vv_stage(pd_handle *h, int32_t stage, int64_t kstep);
+pd_status pd_vv_end(pd_handle *h);
+
+/* Halo data (exchange_loc_to_halo!): kind 0 = the point state the force kernels gather from
+ * neighbours, exchanged after stage 0; kind 1 = the per-point state of the first force kernel
+ * that the second one gathers (OSB, CMat; nothing for BB), exchanged after stage 1. Every row
+ * is pd_halo_row_bytes bytes. pd_halo_pack gathers rows d_rows[0 .. n_rows) (int32, device)
+ * into d_buf (device); pd_halo_unpack writes d_buf into rows row0 .. row0 + n_rows - 1 and
+ * finishes them (FP32: the split displacement; CMat with directed bond states: the bonds of
+ * killed rows). Both are asynchronous on the handle's stream; a row index outside the body
+ * is reported by the next pd_vv_end. */
+pd_status pd_halo_row_bytes(pd_handle *h, int32_t kind, int64_t *bytes);
+pd_status pd_halo_pack(pd_handle *h, int32_t kind, const int32_t *d_rows, int64_t n_rows,
+                       void *d_buf);
+pd_status pd_halo_unpack(pd_handle *h, int32_t kind, int64_t row0, int64_t n_rows,
+                         const void *d_buf);
 
 /* ---------------------------------------------------------------------------------------
  * Dynamic relaxation (src/time_solvers/dynamic_relaxation.jl): adaptive-damping explicit

@@ -307,6 +307,7 @@ static pd_status begin_create(const pd_body_desc* desc, pd_handle** out, pd_hand
   h->maxdmg = desc->maxdmg;
   h->multi = desc->multi_params ? 1 : 0;
   PD_CUDA(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+  h->own_stream = h->stream;
   for (int k = 0; k < desc->n_params; k++) h->hp.push_back(make_param(desc->params[k], h->cs));
   PD_TRY(dalloc(h, &h->dparams, h->hp.size()));
   PD_TRY(upload_params(h));
@@ -450,7 +451,7 @@ extern "C" pd_status pd_find_bonds(int64_t n, const double* position, const doub
     ok(cudaMemcpy(dd, delta, sizeof(double) * n, cudaMemcpyHostToDevice));
     if (dm) ok(cudaMemcpy(dm, mask.data(), sizeof(unsigned short) * n, cudaMemcpyHostToDevice));
   }
-  if (e == cudaSuccess) ok(device_find_bonds_grid(n, dX, dd, dm, lo, hc, nc, doff, &dnbr, &nb, &dup, s));
+  if (e == cudaSuccess) ok(device_find_bonds_grid(n, dX, dd, dm, nullptr, lo, hc, nc, doff, &dnbr, &nb, &dup, s));
   if (e == cudaSuccess && dup) st = fail(PD_ERR_ARG, "point duplicate found!");
   if (e == cudaSuccess && st == PD_OK) {
     *n_bonds = nb;
@@ -480,10 +481,11 @@ extern "C" pd_status pd_find_bonds(int64_t n, const double* position, const doub
   return st;
 }
 
-extern "C" pd_status pd_create_search(const pd_body_desc* desc, const double* search_position,
-                                      const uint8_t* fp_point, int32_t n_filters,
-                                      const uint8_t* filter_a, const uint8_t* filter_b,
-                                      pd_handle** out) {
+// the body's own neighbour search on the device; owned (may be null) restricts the bonds of
+// the points outside it to owned neighbours and marks them halo rows
+static pd_status create_search(const pd_body_desc* desc, const double* search_position,
+                               const uint8_t* fp_point, int32_t n_filters, const uint8_t* filter_a,
+                               const uint8_t* filter_b, const uint8_t* owned, pd_handle** out) {
   PD_TRY(validate_desc(desc, false));
   const long long n = desc->n_points;
   const double* spos = search_position ? search_position : desc->position;
@@ -497,10 +499,16 @@ extern "C" pd_status pd_create_search(const pd_body_desc* desc, const double* se
   pd_handle* h = nullptr;
   pd_status st = begin_create(desc, out, &h);
   if (st != PD_OK) { if (h) pd_destroy(h); return st; }
+  if (owned) {
+    for (long long i = 0; i < n; i++)
+      if (!owned[i]) h->hmeta[i] |= pd::META_HALO;
+    st = upload_meta(h);
+    if (st != PD_OK) { std::string m = g_err; pd_destroy(h); return fail(st, m); }
+  }
   double *dX = nullptr, *dXs = nullptr, *dd = nullptr;
   unsigned short* dm = nullptr;
   long long* doff = nullptr;
-  unsigned char *dfp = nullptr, *dfpb = nullptr;
+  unsigned char *dfp = nullptr, *dfpb = nullptr, *down = nullptr;
   std::vector<double> X(desc->position, desc->position + 3 * n);
   st = dalloc(h, &dX, 3 * n);
   if (st == PD_OK && search_position) st = dalloc(h, &dXs, 3 * n);
@@ -508,6 +516,7 @@ extern "C" pd_status pd_create_search(const pd_body_desc* desc, const double* se
   if (st == PD_OK) st = dalloc(h, &doff, n + 1);
   if (st == PD_OK && n_filters > 0) st = dalloc(h, &dm, n);
   if (st == PD_OK) st = dalloc(h, &dfp, n);
+  if (st == PD_OK && owned) st = dalloc(h, &down, n);
   if (st != PD_OK) { std::string m = g_err; pd_destroy(h); return fail(st, m); }
   std::vector<unsigned char> fp(n, 1);
   if (fp_point) std::copy(fp_point, fp_point + n, fp.begin());
@@ -516,11 +525,12 @@ extern "C" pd_status pd_create_search(const pd_body_desc* desc, const double* se
   if (e == cudaSuccess) e = cudaMemcpy(dd, delta.data(), sizeof(double) * n, cudaMemcpyHostToDevice);
   if (e == cudaSuccess && dm) e = cudaMemcpy(dm, mask.data(), sizeof(unsigned short) * n, cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMemcpy(dfp, fp.data(), n, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess && down) e = cudaMemcpy(down, owned, n, cudaMemcpyHostToDevice);
   int* dnbr = nullptr;
   long long nb = 0;
   int dup = 0;
   if (e == cudaSuccess)
-    e = device_find_bonds_grid(n, dXs ? dXs : dX, dd, dm, lo, hc, nc, doff, &dnbr, &nb, &dup, h->stream);
+    e = device_find_bonds_grid(n, dXs ? dXs : dX, dd, dm, down, lo, hc, nc, doff, &dnbr, &nb, &dup, h->stream);
   if (e != cudaSuccess) { pd_destroy(h); return fail(PD_ERR_CUDA, cudaGetErrorString(e)); }
   if (dup) { pd_destroy(h); return fail(PD_ERR_ARG, "point duplicate found!"); }
   h->allocs.push_back(dnbr);
@@ -532,12 +542,27 @@ extern "C" pd_status pd_create_search(const pd_body_desc* desc, const double* se
   if (st == PD_OK) st = dalloc(h, &dfpb, nb);
   if (st != PD_OK) { std::string m = g_err; pd_destroy(h); return fail(st, m); }
   if (nb) launch_bond_props(n, dX, dfp, doff, dnbr, dL, dfpb, h->stream);
-  dfree(h, dX); dfree(h, dXs); dfree(h, dd); dfree(h, dm); dfree(h, dfp);
+  dfree(h, dX); dfree(h, dXs); dfree(h, dd); dfree(h, dm); dfree(h, dfp); dfree(h, down);
   st = finish_create(h, dnbr, dL, dfpb);
   dfree(h, dnbr); dfree(h, dL); dfree(h, dfpb);
   if (st != PD_OK) { std::string m = g_err; pd_destroy(h); return fail(st, m); }
   *out = h;
   return PD_OK;
+}
+
+extern "C" pd_status pd_create_search(const pd_body_desc* desc, const double* search_position,
+                                      const uint8_t* fp_point, int32_t n_filters,
+                                      const uint8_t* filter_a, const uint8_t* filter_b,
+                                      pd_handle** out) {
+  return create_search(desc, search_position, fp_point, n_filters, filter_a, filter_b, nullptr, out);
+}
+
+extern "C" pd_status pd_create_partition(const pd_body_desc* desc, const double* search_position,
+                                         const uint8_t* fp_point, int32_t n_filters,
+                                         const uint8_t* filter_a, const uint8_t* filter_b,
+                                         const uint8_t* owned, pd_handle** out) {
+  if (!owned) return fail(PD_ERR_ARG, "owned is NULL");
+  return create_search(desc, search_position, fp_point, n_filters, filter_a, filter_b, owned, out);
 }
 
 extern "C" pd_status pd_destroy(pd_handle* h) {
@@ -549,7 +574,7 @@ extern "C" pd_status pd_destroy(pd_handle* h) {
   pd::dr_release(h);
   for (void* p : h->allocs) cudaFree(p);
   h->allocs.clear();
-  if (h->stream) cudaStreamDestroy(h->stream);
+  if (h->own_stream) cudaStreamDestroy(h->own_stream);
   delete h;
   return PD_OK;
 }
@@ -901,6 +926,7 @@ static pd_status check_err(pd_handle* h) {
     return fail(PD_ERR_NAN, "NaN values detected in force density field! step: " + std::to_string(c.err_step));
   }
   if (c.err == 3) return fail(PD_ERR_TIMEOUT, "a bounded wait of a force kernel gave up");
+  if (c.err == 4) return fail(PD_ERR_ARG, "a halo row index outside the body (pd_halo_pack)");
   if (c.err == 2)
     return fail(PD_ERR_ARG, "boundary condition values missing for step " + std::to_string(c.err_step) +
                                 " (call pd_set_bc_values)");
@@ -1166,13 +1192,24 @@ extern "C" pd_status pd_break_bonds(pd_handle* h, const uint8_t* set_a, const ui
 }
 
 extern "C" pd_status pd_break_random_pairs(pd_handle* h, double fraction, uint64_t seed) {
+  return pd_break_random_pairs_ids(h, fraction, seed, nullptr);
+}
+
+extern "C" pd_status pd_break_random_pairs_ids(pd_handle* h, double fraction, uint64_t seed,
+                                               const int64_t* point_ids) {
   if (!h) return fail(PD_ERR_ARG, "handle is NULL");
   if (!(fraction >= 0 && fraction <= 1)) return fail(PD_ERR_ARG, "fraction must be in [0, 1]");
   PD_CUDA(cudaSetDevice(h->device));
   if (h->n == 0) return PD_OK;
-  launch_break_random(h->d, fraction, (unsigned long long)seed, h->stream);
+  long long* gid = nullptr;
+  if (point_ids) {
+    PD_TRY(dalloc(h, &gid, h->n));
+    PD_CUDA(cudaMemcpy(gid, point_ids, sizeof(long long) * h->n, cudaMemcpyHostToDevice));
+  }
+  launch_break_random(h->d, fraction, (unsigned long long)seed, gid, h->stream);
   launch_count_active(h->d, h->stream);
   PD_CUDA(cudaStreamSynchronize(h->stream));
+  dfree(h, gid);
   h->damage_valid = true;
   PD_TRY(check_symmetry(h));
   destroy_graph(h);

@@ -46,7 +46,7 @@ __global__ void k_cell_ranges(long long n, const unsigned long long* key, int* s
 // pass 0: count (cnt[i]); pass 1: write into nbr[off[i]...]
 template <int PASS>
 __global__ void k_search(long long n, const double* X, const double* delta, const unsigned short* cmask,
-                         Grid g, const int* start, const int* end, const int* sorted, long long* cnt,
+                         const unsigned char* owned, Grid g, const int* start, const int* end, const int* sorted, long long* cnt,
                          const long long* off, int* nbr, int* flags) {
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
@@ -54,6 +54,7 @@ __global__ void k_search(long long n, const double* X, const double* delta, cons
   const double di = delta[i];
   const double r2 = di * di;
   const unsigned short mi = cmask ? cmask[i] : 0;
+  const bool own_i = owned ? owned[i] != 0 : true;
   const long long cx = cell_coord(xi, g.lo[0], g.h, g.nc[0]);
   const long long cy = cell_coord(yi, g.lo[1], g.h, g.nc[1]);
   const long long cz = cell_coord(zi, g.lo[2], g.h, g.nc[2]);
@@ -75,6 +76,7 @@ __global__ void k_search(long long n, const double* X, const double* delta, cons
                        dz = zi - X[3 * (long long)j + 2];
           const double d2 = (dx * dx + dy * dy) + dz * dz;
           if (!(d2 <= r2)) continue;
+          if (!own_i && !owned[j]) continue;
           if (cmask) {
             // crack k: point in set a -> bit 2k, in set b -> bit 2k+1
             const unsigned short mj = cmask[j];
@@ -118,7 +120,8 @@ static inline int nblk(long long n, int t) { return (int)((n + t - 1) / t < 1 ? 
   } while (0)
 
 cudaError_t device_find_bonds_grid(long long n, const double* dX, const double* ddelta,
-                                   const unsigned short* dmask, const double lo[3], double h,
+                                   const unsigned short* dmask, const unsigned char* downed,
+                                   const double lo[3], double h,
                                    const long long nc[3], long long* d_off, int** d_nbr_out,
                                    long long* nb_out, int* dup_out, cudaStream_t s) {
   cudaError_t err = cudaSuccess;
@@ -163,7 +166,7 @@ cudaError_t device_find_bonds_grid(long long n, const double* dX, const double* 
   }
   k_cell_ranges<<<nblk(n, 256), 256, 0, s>>>(n, key2, start, end);
   CK(cudaGetLastError());
-  k_search<0><<<nblk(n, 128), 128, 0, s>>>(n, dX, ddelta, dmask, g, start, end, val2, cnt, nullptr,
+  k_search<0><<<nblk(n, 128), 128, 0, s>>>(n, dX, ddelta, dmask, downed, g, start, end, val2, cnt, nullptr,
                                            nullptr, flags);
   CK(cudaGetLastError());
   CK(cub::DeviceScan::ExclusiveSum(nullptr, need, cnt, d_off, (int)n, s));
@@ -177,7 +180,7 @@ cudaError_t device_find_bonds_grid(long long n, const double* dX, const double* 
   if (nb > 0x7fffffffLL) { err = cudaErrorInvalidValue; goto done; }
   CK(cudaMalloc(&nbr, sizeof(int) * (nb > 0 ? nb : 1)));
   CK(cudaMalloc(&nbr2, sizeof(int) * (nb > 0 ? nb : 1)));
-  k_search<1><<<nblk(n, 128), 128, 0, s>>>(n, dX, ddelta, dmask, g, start, end, val2, nullptr, d_off,
+  k_search<1><<<nblk(n, 128), 128, 0, s>>>(n, dX, ddelta, dmask, downed, g, start, end, val2, nullptr, d_off,
                                            nbr, flags);
   CK(cudaGetLastError());
   if (nb > 0) {

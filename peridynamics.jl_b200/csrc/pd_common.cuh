@@ -49,6 +49,9 @@ constexpr uint32_t META_PID_MASK = 0xFFFFu;
 constexpr uint32_t META_KILLED = 1u << 16;  // CMaterial: all bonds killed (too_much_damage!)
 constexpr uint32_t META_HAS_BC = 1u << 17;  // point carries boundary conditions
 constexpr uint32_t META_HAS_BEXT = 1u << 18; // point has a nonzero or prescribed b_ext
+// halo row of a partitioned body: a copy of a point another partition owns, bonded only to
+// owned points; its state is overwritten by halo exchanges, and the owner decides its kills
+constexpr uint32_t META_HALO = 1u << 19;
 
 enum Material : int { MAT_BB = 0, MAT_OSB = 1, MAT_CMAT = 2 };
 enum CModel : int { CM_SVK = 0, CM_NEOHOOKE = 1, CM_NHPENALTY = 2 };
@@ -67,7 +70,8 @@ struct Ctrl {
   long long base;        // step number of the first step of the current launch block
   long long table_first; // first step held in the boundary-condition value table
   long long table_n;     // steps held in the table
-  int err;               // 1: NaN in b_int; 2: boundary values missing for a step
+  int err;               // 1: NaN in b_int; 2: boundary values missing for a step;
+                         // 3: a bounded wait gave up; 4: halo row index outside the body
   int pad;
   long long err_step;
 };

@@ -546,7 +546,9 @@ __global__ void __launch_bounds__(256, PD_MINB_CA) k_c_a32(DevBody d, int kstep)
       bool hasnan = false;
       for (int q = 0; q < 9; q++) { d.H32[9 * i + q] = H[q]; hasnan |= isnan(H[q]); }
       const double damage = 1.0 - (double)na / (double)cnt;
-      killed = (meta & META_KILLED) || damage > d.maxdmg || hasnan;
+      // a halo row sees only part of its bonds: its owner decides (the kill arrives with the
+      // halo exchange of the phase-A state)
+      killed = (meta & META_KILLED) || (!(meta & META_HALO) && (damage > d.maxdmg || hasnan));
       float4* cs = d.cst32 + 3 * i;
       if (killed) {
         if (!(meta & META_KILLED)) d.meta[i] = meta | META_KILLED;

@@ -442,7 +442,9 @@ __global__ void PD_LB64 k_c_a64(DevBody d, int kstep) {
       matmul3(Ft, Kinv, F);
       bool hasnan = false;
       for (int q = 0; q < 9; q++) { d.F64[9 * i + q] = F[q]; hasnan |= isnan(F[q]); }
-      killed = (meta & META_KILLED) || damage > d.maxdmg || hasnan;
+      // a halo row sees only part of its bonds: its owner decides (the kill arrives with the
+      // halo exchange of the phase-A state)
+      killed = (meta & META_KILLED) || (!(meta & META_HALO) && (damage > d.maxdmg || hasnan));
       if (killed) {
         if (!(meta & META_KILLED)) d.meta[i] = meta | META_KILLED;
         na = 0;

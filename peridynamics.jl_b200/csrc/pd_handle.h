@@ -52,7 +52,8 @@ struct GraphKey {
 
 struct pd_handle {
   int device = 0;
-  cudaStream_t stream = nullptr;
+  cudaStream_t stream = nullptr;      // the stream all work is issued on
+  cudaStream_t own_stream = nullptr;  // the stream the handle created (destroyed with it)
   long long n = 0, nb = 0;
   int material = 0, kernel = 1, cmodel = 0, precision = 0, multi = 0;
   double cs = 0.5, maxdmg = 0.85;
@@ -87,6 +88,9 @@ struct pd_handle {
   long long nslots = 0;
   pd::NKState* nk = nullptr;  // created by the first pd_nk_* call
   pd::DRState* dr = nullptr;  // created by pd_dr_init
+  // staged Velocity Verlet run (pd_vv_begin .. pd_vv_end)
+  long long stage_n = 0;
+  double stage_dto = -1.0;
 };
 
 template <class T>

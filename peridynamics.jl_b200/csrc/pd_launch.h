@@ -61,6 +61,7 @@ void launch_bc(const DevBody& d, const IntDev& g, const BCDev& bc, double dt_ove
                cudaStream_t s);
 void launch_finish(const DevBody& d, const IntDev& g, double dt_override, cudaStream_t s);
 void launch_split_u(const DevBody& d, cudaStream_t s);
+void launch_split_u_rows(const DevBody& d, long long row0, long long n, cudaStream_t s);
 
 // sliced bond layout and bond-array helpers (pd_layout.cu)
 cudaError_t build_slices(long long n, const long long* off, int G, long long** soff_out,
@@ -82,6 +83,7 @@ void launch_export_damage(const DevBody& d, int valid, double* out, cudaStream_t
 void launch_export_position(const DevBody& d, const IntDev& g, double* out, int what, cudaStream_t s);
 void launch_timestep(const DevBody& d, double* dt_point, cudaStream_t s);
 void launch_break_sets(const DevBody& d, const unsigned char* A, const unsigned char* B, cudaStream_t s);
-void launch_break_random(const DevBody& d, double fraction, unsigned long long seed, cudaStream_t s);
+void launch_break_random(const DevBody& d, double fraction, unsigned long long seed,
+                         const long long* gid, cudaStream_t s);
 
 }  // namespace pd

@@ -304,6 +304,10 @@ __global__ void k_timestep(DevBody d, double* dtp) {
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= d.n) return;
   const DevParam& P = d.params[d.meta[i] & META_PID_MASK];
+  if (d.meta[i] & META_HALO) {  // its owner's partition gives the step of a halo row
+    dtp[i] = INFINITY;
+    return;
+  }
   const int cnt = (int)(d.off[i + 1] - d.off[i]);
   double dtsum = 0.0;
   for (int k = 0; k < cnt; k++) {
@@ -352,24 +356,29 @@ __device__ __forceinline__ unsigned long long mix64(unsigned long long x) {
   return x;
 }
 
-__global__ void k_break_random(DevBody d, unsigned long long threshold, unsigned long long seed) {
+// gid (may be null): the point numbers the pair hash uses (a partition passes the body's)
+__global__ void k_break_random(DevBody d, unsigned long long threshold, unsigned long long seed,
+                               const long long* gid) {
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= d.n) return;
   const int cnt = (int)(d.off[i + 1] - d.off[i]);
+  const unsigned long long gi = gid ? (unsigned long long)gid[i] : (unsigned long long)i;
   for (int k = 0; k < cnt; k++) {
     const long long b = bond_slot(d, i, k);
-    const unsigned long long j = (unsigned long long)d.nbr[b];
-    const unsigned long long lo = j < (unsigned long long)i ? j : (unsigned long long)i;
-    const unsigned long long hi = j < (unsigned long long)i ? (unsigned long long)i : j;
+    const int jl = d.nbr[b];
+    const unsigned long long j = gid ? (unsigned long long)gid[jl] : (unsigned long long)jl;
+    const unsigned long long lo = j < gi ? j : gi;
+    const unsigned long long hi = j < gi ? gi : j;
     const unsigned long long r = mix64(mix64(lo * 0x9e3779b97f4a7c15ull + seed) ^ hi);
     if (r < threshold) atomicAnd(d.bits + (b >> 5), ~(1u << (b & 31)));
   }
 }
 
-void launch_break_random(const DevBody& d, double fraction, unsigned long long seed, cudaStream_t s) {
+void launch_break_random(const DevBody& d, double fraction, unsigned long long seed,
+                         const long long* gid, cudaStream_t s) {
   const long double t = (long double)fraction * 18446744073709551616.0L;
   const unsigned long long thr = fraction >= 1.0 ? ~0ull : (unsigned long long)t;
-  k_break_random<<<blocks_for(d.n, 256), 256, 0, s>>>(d, thr, seed);
+  k_break_random<<<blocks_for(d.n, 256), 256, 0, s>>>(d, thr, seed, gid);
 }
 
 }  // namespace pd

@@ -41,6 +41,9 @@ EXPORTS = (
     "pd_force", "pd_run_vv", "pd_nan_step", "pd_run_vv_timed", "pd_autotune", "pd_set_mapping",
     "pd_set_graph", "pd_set_pipeline", "pd_get_mapping", "pd_info", "pd_launch_count", "pd_stream",
     "pd_dr_init", "pd_run_dr", "pd_run_dr_timed", "pd_dr_density_matrix",
+    "pd_break_random_pairs_ids", "pd_create_partition", "pd_set_stream", "pd_vv_begin",
+    "pd_force_phase", "pd_vv_stage", "pd_vv_end", "pd_halo_row_bytes", "pd_halo_pack",
+    "pd_halo_unpack",
     "pd_nk_set_conditions", "pd_nk_step", "pd_nk_set_corrections", "pd_nk_apply",
     "pd_nk_record", "pd_nk_recorded", "pd_nk_recorded_vector",
     "pd_mpnn_create", "pd_mpnn_destroy", "pd_mpnn_set_params", "pd_mpnn_get_params",
@@ -150,6 +153,16 @@ def lib():
         "pd_stream": [vp, vp],
         "pd_osb_force_static": [i64] + [vp] * 8 + [vp, i32, vp, vp, vp],
         "pd_dr_init": [vp, dbl, dbl],
+        "pd_break_random_pairs_ids": [vp, dbl, C.c_uint64, vp],
+        "pd_create_partition": [vp, vp, vp, i32, vp, vp, vp, vp],
+        "pd_set_stream": [vp, vp],
+        "pd_vv_begin": [vp, i64, i64, dbl],
+        "pd_force_phase": [vp, i32, dbl, dbl],
+        "pd_vv_stage": [vp, i32, i64],
+        "pd_vv_end": [vp],
+        "pd_halo_row_bytes": [vp, i32, vp],
+        "pd_halo_pack": [vp, i32, vp, i64, vp],
+        "pd_halo_unpack": [vp, i32, i64, i64, vp],
         "pd_run_dr": [vp, i64, i64],
         "pd_run_dr_timed": [vp, i64, i64, vp, vp, vp, vp],
         "pd_dr_density_matrix": [vp, vp],

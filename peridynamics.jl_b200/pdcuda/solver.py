@@ -82,7 +82,7 @@ class DeviceBody:
     """One body (all points in one chunk) resident on a CUDA device."""
 
     def __init__(self, body: Body, precision="fp64", device=0, param_dt=None,
-                 independent_params=False):
+                 independent_params=False, owned=None):
         if precision not in _PREC:
             raise ValueError("precision must be 'fp64' or 'fp32'")
         if np.any(body.params_map == 0):
@@ -123,8 +123,14 @@ class DeviceBody:
             fb[k, body.point_sets[b]] = 1
         fp = body.fail_permit.astype(np.uint8)
         spos = getattr(body, "_search_pos", None)
-        L.check(lib.pd_create_search(C.byref(desc), L.ptr(spos), L.ptr(fp), nf, L.ptr(fa),
-                                     L.ptr(fb), C.byref(self.h)), "pd_create_search")
+        if owned is None:
+            L.check(lib.pd_create_search(C.byref(desc), L.ptr(spos), L.ptr(fp), nf, L.ptr(fa),
+                                         L.ptr(fb), C.byref(self.h)), "pd_create_search")
+        else:  # a partition: owned rows and halo rows (pdcuda.halo)
+            own = np.ascontiguousarray(owned, np.uint8)
+            L.check(lib.pd_create_partition(C.byref(desc), L.ptr(spos), L.ptr(fp), nf, L.ptr(fa),
+                                            L.ptr(fb), L.ptr(own), C.byref(self.h)),
+                    "pd_create_partition")
         self.n_bonds = self.info()[1]
         # apply_precracks! (predefined_cracks.jl:31-60): damage-mode cracks break bonds
         for a, b, filt_mode in body.point_sets_precracks:

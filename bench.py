@@ -478,6 +478,65 @@ def run_dr(args, rank, world, local, dist):
         print(json.dumps(line), flush=True)
 
 
+def run_halo(args, rank, world, local, dist):
+    """--halo: one body cut into partitions with halo exchange (pdcuda.halo): one partition per
+    rank over NCCL (strong scaling), or --halo-parts P partitions held by one process on one GPU
+    (the exchange is then device copies: the cost of partitioning without the link)."""
+    import pdcuda as pd
+    from pdcuda.halo import Partition, PartitionedBody
+    from pdcuda.replicas import reduce_max
+    nx, ny, nz, dx, mat, frac, vbc = CONFIGS[args.config]
+    body, frac = make_body(args.config)
+    n_parts = world if world > 1 else max(args.halo_parts, 1)
+    mine = [rank] if world > 1 else list(range(n_parts))
+    t0 = time.perf_counter()
+    from pdcuda.halo import decompose
+    owner = decompose(body, n_parts, args.halo_decomposition)
+    parts = [Partition(body, n_parts, p, args.precision, device=local, owner=owner) for p in mine]
+    for p in parts:
+        if frac > 0:
+            p.break_random_pairs(frac, 0x5EED)
+        p.dev.autotune()
+    pb = PartitionedBody(parts, dist if world > 1 else None, device=local)
+    setup_s = time.perf_counter() - t0
+    dt = pb.stable_timestep(0.7)
+    pb.force(0.0, dt)
+    pb.run(1, args.warmup, dt)
+    launches0 = sum(p.dev.launch_count() for p in parts)
+    if dist:
+        dist.barrier()
+    with ClockSampler(local) as clk:
+        ms = pb.run(args.warmup + 1, args.steps, dt, timed=True)
+    launches = sum(p.dev.launch_count() for p in parts) - launches0
+    ms_max = reduce_max(ms["total"], dist, f"cuda:{local}")
+    owned_bonds = sum(len(p.owned_field("bond_active")) for p in parts)
+    halo_rows = sum(int(np.count_nonzero(p.owned == 0)) for p in parts)
+    rows = sum(len(p.rows) for p in parts)
+    all_bonds = sum(p.dev.info()[1] for p in parts)
+    from pdcuda.replicas import reduce_sum
+    body_bonds = reduce_sum(owned_bonds, dist, f"cuda:{local}")
+    value = body_bonds * args.steps / (ms_max / 1e3)
+    mapping = [dict(zip(("group", "block", "pipe"), p.dev.mapping())) for p in parts]
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+            "scaling": "strong", "vs_baseline": None,
+            "dtype": "f32" if args.precision == "fp32" else "f64", "data": "synthetic",
+            "config": {"workload": f"{args.config}: {mat} {nx}x{ny}x{nz} points, dx={dx}, "
+                                   f"{frac:.0%} pairs broken, VV step, {n_parts} partitions",
+                       "partitions": n_parts, "decomposition": args.halo_decomposition, "parallelism": f"halo x{world}" if world > 1 else
+                       f"{n_parts} partitions in one process", "mapping": mapping,
+                       "setup_s": setup_s},
+            "halo": {"ms_per_step": {k: v / args.steps for k, v in ms.items()},
+                     "rows_here": rows, "halo_rows_here": halo_rows,
+                     "bonds_here": all_bonds, "owned_bonds_here": owned_bonds},
+            "gpu_launches": launches, "clocks": clk.summary(),
+        }
+        print(json.dumps(line), flush=True)
+    pb.close()
+
+
 def run_reference(args, rank, world):
     """The reference arm: the CPU restatement of the reference (Julia is not installed) on all
     host threads; every step is one Velocity Verlet step of the bounded sample."""
@@ -656,6 +715,12 @@ def main():
     ap.add_argument("--fp64-steps", type=int, default=-1, help="steps of the FP64 comparison (0 = skip)")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--graph", type=int, default=0)
+    ap.add_argument("--halo", action="store_true",
+                    help="one body in partitions with halo exchange (one per rank) instead of replicas")
+    ap.add_argument("--halo-parts", type=int, default=1,
+                    help="with --halo on one GPU: partitions held by the one process")
+    ap.add_argument("--halo-decomposition", default="index", choices=["index", "slabs"],
+                    help="index: the reference's contiguous point ranges; slabs: along the longest side")
     ap.add_argument("--jfnk-increments", type=int, default=-1,
                     help="load increments of the JFNK comparison (default: 20 with --config "
                          "jfnk500k, 2 in the default run, 0 = skip)")
@@ -697,6 +762,12 @@ def main():
     if args.config == "pulse1m":
         if rank == 0 and args.impl == "ours":
             run_precision_study(args, local)
+        if dist:
+            dist.barrier()
+            dist.destroy_process_group()
+        return
+    if args.halo and args.impl == "ours":
+        run_halo(args, rank, world, local, dist)
         if dist:
             dist.barrier()
             dist.destroy_process_group()

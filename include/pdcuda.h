@@ -310,14 +310,14 @@ pd_status pd_vv_end(pd_handle *h);
  * neighbours, exchanged after stage 0; kind 1 = the per-point state of the first force kernel
  * that the second one gathers (OSB, CMat; nothing for BB), exchanged after stage 1. Every row
  * is pd_halo_row_bytes bytes. pd_halo_pack gathers rows d_rows[0 .. n_rows) (int32, device)
- * into d_buf (device); pd_halo_unpack writes d_buf into rows row0 .. row0 + n_rows - 1 and
- * finishes them (FP32: the split displacement; CMat with directed bond states: the bonds of
- * killed rows). Both are asynchronous on the handle's stream; a row index outside the body
- * is reported by the next pd_vv_end. */
+ * into d_buf (device); pd_halo_unpack writes d_buf into rows d_rows[0 .. n_rows) and finishes
+ * them (FP32: the split displacement; CMat with directed bond states: the bonds of killed
+ * rows). Both are asynchronous on the handle's stream; a row index outside the body is
+ * reported by the next pd_vv_end. */
 pd_status pd_halo_row_bytes(pd_handle *h, int32_t kind, int64_t *bytes);
 pd_status pd_halo_pack(pd_handle *h, int32_t kind, const int32_t *d_rows, int64_t n_rows,
                        void *d_buf);
-pd_status pd_halo_unpack(pd_handle *h, int32_t kind, int64_t row0, int64_t n_rows,
+pd_status pd_halo_unpack(pd_handle *h, int32_t kind, const int32_t *d_rows, int64_t n_rows,
                          const void *d_buf);
 
 /* ---------------------------------------------------------------------------------------

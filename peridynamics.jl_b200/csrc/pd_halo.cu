@@ -89,22 +89,30 @@ __global__ void k_halo_pack(HaloKind k, long long n_body, const int* rows, long 
   buf[t] = k.seg[s].base[row * k.seg[s].words + w];
 }
 
-__global__ void k_halo_unpack(HaloKind k, long long row0, long long n, const unsigned* buf) {
+// row rows[t / row_words] = buf word t; an index outside the body records error 4 and is skipped
+__global__ void k_halo_unpack(HaloKind k, long long n_body, const int* rows, long long n,
+                              const unsigned* buf, Ctrl* ctrl) {
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= n * k.row_words) return;
   const long long r = t / k.row_words;
   int w = (int)(t - r * k.row_words);
+  const long long row = rows[r];
+  if (row < 0 || row >= n_body) {
+    ctrl->err = 4;
+    return;
+  }
   const int s = halo_seg_of(k, w);
-  unsigned* dst = k.seg[s].base + (row0 + r) * k.seg[s].words + w;
+  unsigned* dst = k.seg[s].base + row * k.seg[s].words + w;
   const unsigned v = buf[t];
   *dst = k.seg[s].kill_only ? ((*dst & ~META_KILLED) | (v & META_KILLED)) : v;
 }
 
 // directed bond states: a halo row its owner killed loses all its bonds (correspondence.jl:293)
-__global__ void k_halo_kill_bonds(DevBody d, long long row0, long long n) {
-  const long long i = row0 + (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= row0 + n) return;
-  if (!(d.meta[i] & META_KILLED)) return;
+__global__ void k_halo_kill_bonds(DevBody d, const int* rows, long long n) {
+  const long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= n) return;
+  const long long i = rows[r];
+  if (i < 0 || i >= d.n || !(d.meta[i] & META_KILLED)) return;
   const int cnt = (int)(d.off[i + 1] - d.off[i]);
   for (int k = 0; k < cnt; k++) clear_bit(d.bits, bond_slot(d, i, k));
 }
@@ -146,24 +154,24 @@ extern "C" pd_status pd_halo_pack(pd_handle* h, int32_t kind, const int32_t* d_r
   return PD_OK;
 }
 
-extern "C" pd_status pd_halo_unpack(pd_handle* h, int32_t kind, int64_t row0, int64_t n_rows,
+extern "C" pd_status pd_halo_unpack(pd_handle* h, int32_t kind, const int32_t* d_rows, int64_t n_rows,
                                     const void* d_buf) {
   if (!h) return pd_fail(PD_ERR_ARG, "handle is NULL");
   if (kind != 0 && kind != 1) return pd_fail(PD_ERR_ARG, "kind must be 0 or 1");
-  if (row0 < 0 || n_rows < 0 || row0 + n_rows > h->n) return pd_fail(PD_ERR_ARG, "rows out of range");
+  if (n_rows < 0 || n_rows > h->n) return pd_fail(PD_ERR_ARG, "n_rows out of range");
   const HaloKind k = halo_kind(h, kind);
   if (n_rows == 0 || k.row_words == 0) return PD_OK;
-  if (!d_buf) return pd_fail(PD_ERR_ARG, "NULL device array");
+  if (!d_rows || !d_buf) return pd_fail(PD_ERR_ARG, "NULL device array");
   PD_CUDA(cudaSetDevice(h->device));
   k_halo_unpack<<<halo_blocks(n_rows * k.row_words), 256, 0, h->stream>>>(
-      k, row0, n_rows, static_cast<const unsigned*>(d_buf));
+      k, h->n, d_rows, n_rows, static_cast<const unsigned*>(d_buf), h->d.ctrl);
   h->launches++;
   if (kind == 0 && h->precision != PD_PREC_FP64) {
-    launch_split_u_rows(h->d, row0, n_rows, h->stream);
+    launch_split_u_rows(h->d, d_rows, n_rows, h->stream);
     h->launches++;
   }
   if (kind == 1 && h->material == PD_MAT_CMAT && !h->d.sym) {
-    k_halo_kill_bonds<<<halo_blocks(n_rows), 256, 0, h->stream>>>(h->d, row0, n_rows);
+    k_halo_kill_bonds<<<halo_blocks(n_rows), 256, 0, h->stream>>>(h->d, d_rows, n_rows);
     h->launches++;
   }
   PD_CUDA(cudaGetLastError());

@@ -147,15 +147,17 @@ void launch_split_u(const DevBody& d, cudaStream_t s) {
   k_split_u<<<blocks_for(d.n, 256), 256, 0, s>>>(d);
 }
 
-__global__ void k_split_u_rows(DevBody d, long long row0, long long n) {
-  const long long i = row0 + (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= row0 + n || i >= d.n) return;
+__global__ void k_split_u_rows(DevBody d, const int* rows, long long n) {
+  const long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= n) return;
+  const long long i = rows[r];
+  if (i < 0 || i >= d.n) return;
   split_u(d, i, d.cur[i]);
 }
 
-void launch_split_u_rows(const DevBody& d, long long row0, long long n, cudaStream_t s) {
+void launch_split_u_rows(const DevBody& d, const int* rows, long long n, cudaStream_t s) {
   if (n <= 0 || d.uhi == nullptr) return;
-  k_split_u_rows<<<blocks_for(n, 256), 256, 0, s>>>(d, row0, n);
+  k_split_u_rows<<<blocks_for(n, 256), 256, 0, s>>>(d, rows, n);
 }
 
 void launch_finish(const DevBody& d, const IntDev& g, double dt_override, cudaStream_t s) {

@@ -61,7 +61,8 @@ void launch_bc(const DevBody& d, const IntDev& g, const BCDev& bc, double dt_ove
                cudaStream_t s);
 void launch_finish(const DevBody& d, const IntDev& g, double dt_override, cudaStream_t s);
 void launch_split_u(const DevBody& d, cudaStream_t s);
-void launch_split_u_rows(const DevBody& d, long long row0, long long n, cudaStream_t s);
+// the split of rows[0 .. n) (halo rows that received a displacement)
+void launch_split_u_rows(const DevBody& d, const int* rows, long long n, cudaStream_t s);
 
 // sliced bond layout and bond-array helpers (pd_layout.cu)
 cudaError_t build_slices(long long n, const long long* off, int G, long long** soff_out,

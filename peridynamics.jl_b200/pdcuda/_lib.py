@@ -162,7 +162,7 @@ def lib():
         "pd_vv_end": [vp],
         "pd_halo_row_bytes": [vp, i32, vp],
         "pd_halo_pack": [vp, i32, vp, i64, vp],
-        "pd_halo_unpack": [vp, i32, i64, i64, vp],
+        "pd_halo_unpack": [vp, i32, vp, i64, vp],
         "pd_run_dr": [vp, i64, i64],
         "pd_run_dr_timed": [vp, i64, i64, vp, vp, vp, vp],
         "pd_dr_density_matrix": [vp, vp],

@@ -3,7 +3,10 @@
 The reference's MPI data handler (src/core/mpi_body_data_handler.jl) re-expressed for GPUs:
 
 - the body's points are cut into contiguous index ranges, one per rank (PointDecomposition /
-  distribute_equally, src/discretization/decomposition.jl:32-63; mpi_data_handler :81-100);
+  distribute_equally, src/discretization/decomposition.jl:32-63; mpi_data_handler :81-100),
+  or, as an option, into slabs of equal point counts along the body's longest extent, which
+  cross the body where it is thinnest (fewer halo points when the point order runs along a
+  short side);
 - a partition holds its owned points and the halo points bonded to them, in the body's point
   order (chop_body_mpi :102-109, get_halo_infos :111-125). Halo rows carry only their bonds to
   owned points (pd_create_partition), so every owned point keeps the bond list and the
@@ -48,44 +51,75 @@ def owner_of(ranges, points):
     return np.searchsorted(stops, np.asarray(points), side="right")
 
 
-def candidate_rows(body, o0, o1):
-    """The owned points [o0, o1) and every point inside their bounding box grown by the largest
+def decompose(body, n_parts, how="index"):
+    """The partition that owns every point. "index": the reference's PointDecomposition,
+    contiguous ranges of point numbers (distribute_equally); "slabs": the same counts taken
+    along the body's longest extent (points ordered by that coordinate, then by number), so
+    that the cuts cross the body where it is thinnest."""
+    n = body.n_points
+    ranges = distribute_equally(n, n_parts)
+    owner = np.empty(n, np.int32)
+    if how == "index":
+        order = np.arange(n)
+    elif how == "slabs":
+        X = body._pos
+        axis = int(np.argmax(X.max(axis=0) - X.min(axis=0)))
+        order = np.lexsort((np.arange(n), X[:, axis]))
+    else:
+        raise ValueError('decomposition must be "index" or "slabs"')
+    for p, (a, b) in enumerate(ranges):
+        owner[order[a:b]] = p
+    return owner
+
+
+def candidate_rows(body, owned_points):
+    """The owned points and every point inside their bounding box grown by the largest
     horizon: a superset of the halo (a bond is never longer than its owner's horizon)."""
     X = body._pos
     dmax = max(p.delta for p in body.point_params)
-    own = X[o0:o1]
+    own = X[owned_points]
     lo = own.min(axis=0) - dmax * (1 + 1e-12)
     hi = own.max(axis=0) + dmax * (1 + 1e-12)
     inside = np.all((X >= lo) & (X <= hi), axis=1)
-    inside[o0:o1] = True
+    inside[owned_points] = True
     return np.nonzero(inside)[0]
 
 
-def recv_blocks(rows, owned, ranges):
-    """{source partition: (first row, point numbers)} of the halo rows; rows are in the body's
-    point order and ranges are contiguous, so each source's halo rows are one block."""
-    halo_rows = np.nonzero(~owned.astype(bool))[0]
+def recv_lists(rows, owned, owner):
+    """{source partition: (rows (int32), point numbers)} of the halo rows, by owner."""
+    halo_rows = np.nonzero(~np.asarray(owned, bool))[0]
     halo = rows[halo_rows]
-    owner = owner_of(ranges, halo)
+    src_of = owner[halo]
     out = {}
-    for src in np.unique(owner):
-        idx = np.nonzero(owner == src)[0]
-        r = halo_rows[idx]
-        if r[-1] - r[0] + 1 != len(r):
-            raise AssertionError("halo rows of one source are not contiguous")
-        out[int(src)] = (int(r[0]), halo[idx])
+    for src in np.unique(src_of):
+        idx = np.nonzero(src_of == src)[0]
+        out[int(src)] = (np.ascontiguousarray(halo_rows[idx], np.int32), halo[idx])
     return out
 
 
-def send_rows(part, ranges, own_row0, requests):
+def send_rows(part, rows, requests):
     """{destination partition: rows (int32)} this partition sends: requests[r] is partition
-    r's {source: point numbers} of its halo rows."""
-    o0 = ranges[part][0]
+    r's {source: point numbers} of its halo rows; rows are this partition's point numbers."""
     out = {}
     for r, req in enumerate(requests):
         if r != part and part in req:
-            out[r] = np.ascontiguousarray(own_row0 + (np.asarray(req[part]) - o0), np.int32)
+            gids = np.asarray(req[part])
+            idx = np.searchsorted(rows, gids)
+            if not np.array_equal(rows[np.minimum(idx, len(rows) - 1)], gids):
+                raise AssertionError(f"partition {r} asks partition {part} for points it does not hold")
+            out[r] = np.ascontiguousarray(idx, np.int32)
     return out
+
+
+def bond_segments(nn, rows):
+    """Flat indices of the bonds of the given rows in a CSR with bond counts nn."""
+    rows = np.asarray(rows)
+    if len(rows) == 0:
+        return np.zeros(0, np.int64)
+    off = np.concatenate(([0], np.cumsum(nn)))
+    cnt = nn[rows]
+    starts = np.repeat(off[rows] - np.concatenate(([0], np.cumsum(cnt)[:-1])), cnt)
+    return starts + np.arange(int(cnt.sum()))
 
 
 def part_body(body, rows, owned):
@@ -124,18 +158,20 @@ def part_body(body, rows, owned):
 
 class Partition:
     """Partition `part` of `n_parts` of a body on one device (chop_body_mpi): a DeviceBody over
-    its owned and halo rows, and the rows it receives and sends."""
+    its owned and halo rows (in the body's point order), and the rows it receives and sends.
+    owner: the partition of every point (decompose; computed from `decomposition` if None)."""
 
-    def __init__(self, body, n_parts, part, precision="fp64", device=0):
+    def __init__(self, body, n_parts, part, precision="fp64", device=0, decomposition="index",
+                 owner=None):
         from .solver import DeviceBody
         self.body, self.n_parts, self.part = body, n_parts, part
         self.precision, self.device = precision, device
-        self.ranges = distribute_equally(body.n_points, n_parts)
-        o0, o1 = self.ranges[part]
-        if o1 <= o0:
+        self.owner = decompose(body, n_parts, decomposition) if owner is None else owner
+        owned_points = np.nonzero(self.owner == part)[0]
+        if len(owned_points) == 0:
             raise ValueError(f"partition {part} of {n_parts} has no points")
-        rows = candidate_rows(body, o0, o1)
-        owned = ((rows >= o0) & (rows < o1)).astype(np.uint8)
+        rows = candidate_rows(body, owned_points)
+        owned = (self.owner[rows] == part).astype(np.uint8)
         dev = DeviceBody(part_body(body, rows, owned), precision, device, owned=owned)
         keep = owned.astype(bool) | (dev.field("n_neighbors") > 0)
         if not keep.all():  # candidates without a bond to an owned point
@@ -144,16 +180,16 @@ class Partition:
             owned = owned[keep]
             dev = DeviceBody(part_body(body, rows, owned), precision, device, owned=owned)
         self.dev, self.rows, self.owned = dev, rows, owned
-        self.own_row0 = int(np.searchsorted(rows, o0))
-        self.n_owned = o1 - o0
-        self.recv = recv_blocks(rows, owned, self.ranges)
+        self.owned_rows = np.nonzero(owned)[0]
+        self.n_owned = len(self.owned_rows)
+        self.recv = recv_lists(rows, owned, self.owner)
         self.send = {}
 
     def requests(self):
         return {src: gids for src, (_, gids) in self.recv.items()}
 
     def link(self, requests):
-        self.send = send_rows(self.part, self.ranges, self.own_row0, requests)
+        self.send = send_rows(self.part, self.rows, requests)
 
     def break_random_pairs(self, fraction, seed):
         """pd_break_random_pairs on the body's point numbers: the same pairs as the body."""
@@ -162,16 +198,13 @@ class Partition:
                 "pd_break_random_pairs_ids")
 
     def owned_field(self, name):
-        """A point field of the owned rows (3 x n_owned or n_owned); bond_active: the owned
-        rows' bonds, which are the body's bonds of these points in the body's order."""
+        """A point field of the owned rows (3 x n_owned or n_owned, in the body's point order);
+        bond_active: the bonds of the owned rows, which are the body's bonds of these points."""
         if name == "bond_active":
             nn = self.dev.field("n_neighbors")
-            off = np.concatenate(([0], np.cumsum(nn)))
-            b = self.dev.field("bond_active")
-            return b[off[self.own_row0]:off[self.own_row0 + self.n_owned]]
+            return self.dev.field("bond_active")[bond_segments(nn, self.owned_rows)]
         f = self.dev.field(name)
-        sl = slice(self.own_row0, self.own_row0 + self.n_owned)
-        return f[..., sl] if f.ndim == 2 else f[sl]
+        return f[..., self.owned_rows] if f.ndim == 2 else f[self.owned_rows]
 
     # -- halo data on the device -----------------------------------------------------------
     def alloc_buffers(self, kinds, torch_device):
@@ -188,6 +221,8 @@ class Partition:
             self.recv_bufs[kind] = {
                 src: torch.empty(len(gids) * rb, dtype=torch.uint8, device=torch_device)
                 for src, (_, gids) in self.recv.items()}
+        self.recv_rows = {src: torch.from_numpy(rows).to(torch_device)
+                          for src, (rows, _) in self.recv.items()}
 
     def pack(self, kind):
         for dst, (rows, buf) in self.send_bufs[kind].items():
@@ -196,8 +231,8 @@ class Partition:
 
     def unpack(self, kind):
         for src, buf in self.recv_bufs[kind].items():
-            row0, gids = self.recv[src]
-            L.check(L.lib().pd_halo_unpack(self.dev.h, kind, row0, len(gids),
+            rows = self.recv_rows[src]
+            L.check(L.lib().pd_halo_unpack(self.dev.h, kind, C.c_void_p(rows.data_ptr()), len(rows),
                                            C.c_void_p(buf.data_ptr())), "pd_halo_unpack")
 
     def close(self):
@@ -310,33 +345,80 @@ class PartitionedBody:
             statuses = [lib.pd_force_phase(p.dev.h, 2, t, dt) for p in self.parts]
         self._finish(statuses, t, dt)
 
-    def run(self, first_step, n_steps, dt):
+    def run(self, first_step, n_steps, dt, timed=False):
         """n_steps Velocity Verlet steps from first_step (verlet_timestep!, velocity_verlet.jl:
-        226-237, on every partition)."""
+        226-237, on every partition). timed: CUDA events on the partitions' stream at every
+        stage boundary; returns milliseconds {total, integrate, halo_0, force_a, halo_1,
+        force_b} summed over the steps."""
         import torch
         lib = L.lib()
         for p in self.parts:
             p.dev.tabulate_bcs(first_step, n_steps, dt)
             L.check(lib.pd_vv_begin(p.dev.h, first_step, n_steps, dt), "pd_vv_begin")
+        ev = []
+
+        def mark():
+            if timed:
+                e = torch.cuda.Event(enable_timing=True)
+                e.record(self.stream)
+                ev.append(e)
+
         with torch.cuda.stream(self.stream):
             for k in range(n_steps):
+                mark()
                 for p in self.parts:
                     L.check(lib.pd_vv_stage(p.dev.h, 0, k), "pd_vv_stage")
+                mark()
                 self.exchange(0)
+                mark()
                 for p in self.parts:
                     L.check(lib.pd_vv_stage(p.dev.h, 1, k), "pd_vv_stage")
+                mark()
                 if self.state_based:
                     self.exchange(1)
+                    mark()
                     for p in self.parts:
                         L.check(lib.pd_vv_stage(p.dev.h, 2, k), "pd_vv_stage")
+                    mark()
+            mark()
             statuses = [lib.pd_vv_end(p.dev.h) for p in self.parts]
+            mark()
         self._finish(statuses, (first_step + n_steps - 1) * dt, dt)
+        if not timed:
+            return None
+        self.stream.synchronize()
+        per = 6 if self.state_based else 4
+        names = ("integrate", "halo_0", "force_a", "halo_1", "force_b")[:per - 1]
+        out = dict.fromkeys(names, 0.0)
+        for k in range(n_steps):
+            base = k * per
+            for j, nm in enumerate(names):
+                out[nm] += ev[base + j].elapsed_time(ev[base + j + 1])
+        out["integrate"] += ev[-2].elapsed_time(ev[-1])
+        out["total"] = ev[0].elapsed_time(ev[-1])
+        return out
 
     def field(self, name):
-        """The owned rows of every partition held here, in the body's point order."""
-        parts = sorted(self.parts, key=lambda p: p.part)
-        vals = [p.owned_field(name) for p in parts]
-        return np.concatenate(vals, axis=-1 if vals[0].ndim == 2 else 0)
+        """A field of the whole body assembled from the owned rows (all partitions held by
+        this process); bond_active in the body's bond order."""
+        if len(self.parts) != self.parts[0].n_parts:
+            raise ValueError("field() needs every partition in this process (dist is None)")
+        n = self.parts[0].body.n_points
+        if name == "bond_active":
+            nn = np.zeros(n, np.int64)
+            for p in self.parts:
+                nn[p.rows[p.owned_rows]] = p.dev.field("n_neighbors")[p.owned_rows]
+            out = np.empty(int(nn.sum()), np.uint8)
+            for p in self.parts:
+                out[bond_segments(nn, p.rows[p.owned_rows])] = p.owned_field(name)
+            return out
+        out = None
+        for p in self.parts:
+            v = p.owned_field(name)
+            if out is None:
+                out = np.empty(v.shape[:-1] + (n,), v.dtype)
+            out[..., p.rows[p.owned_rows]] = v
+        return out
 
     def close(self):
         for p in self.parts:

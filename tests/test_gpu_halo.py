@@ -43,8 +43,8 @@ def run_body(body, prec, mapping, n):
     return dev, dt
 
 
-def run_parts(body, n_parts, prec, mapping, n):
-    parts = [Partition(body, n_parts, p, prec) for p in range(n_parts)]
+def run_parts(body, n_parts, prec, mapping, n, how="index"):
+    parts = [Partition(body, n_parts, p, prec, decomposition=how) for p in range(n_parts)]
     for p in parts:
         p.dev.set_mapping(*mapping)
     pb = PartitionedBody(parts)
@@ -62,11 +62,12 @@ def assert_same(dev, pb):
 
 
 @pytest.mark.parametrize("name", ["BB", "OSB", "C"])
-@pytest.mark.parametrize("prec,mapping", [("fp64", (0,)), ("fp32", (8,)), ("fp64", (4,))])
-def test_partitions_step_like_the_body(name, prec, mapping):
+@pytest.mark.parametrize("prec,mapping,how", [("fp64", (0,), "index"), ("fp32", (8,), "index"),
+                                              ("fp64", (4,), "slabs"), ("fp32", (1,), "slabs")])
+def test_partitions_step_like_the_body(name, prec, mapping, how):
     body = make_plate(name)
     dev, dt = run_body(body, prec, mapping, 100)
-    pb, dt2 = run_parts(body, 3, prec, mapping, 100)
+    pb, dt2 = run_parts(body, 3, prec, mapping, 100, how)
     assert dt2 == dt
     assert_same(dev, pb)
     assert np.count_nonzero(dev.field("bond_active") == 0) > 0
@@ -97,7 +98,7 @@ def test_random_pairs_and_single_partition():
     body = make_plate("OSB")
     dev = pd.DeviceBody(body, precision="fp32")
     dev.break_random_pairs(0.05, 1234)
-    parts = [Partition(body, 4, p, "fp32") for p in range(4)]
+    parts = [Partition(body, 4, p, "fp32", decomposition="slabs") for p in range(4)]
     for p in parts:
         p.break_random_pairs(0.05, 1234)
     pb = PartitionedBody(parts)

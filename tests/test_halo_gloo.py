@@ -11,8 +11,9 @@ import pytest
 import torch.multiprocessing as mp
 
 import pdcuda as pd
-from pdcuda.halo import (HaloExchange, candidate_rows, distribute_equally, link_partitions,
-                         owner_of, part_body, recv_blocks, send_rows)
+from pdcuda.halo import (HaloExchange, bond_segments, candidate_rows, decompose,
+                         distribute_equally, link_partitions, owner_of, part_body, recv_lists,
+                         send_rows)
 from helpers import oracle_body, plate_body
 
 
@@ -32,45 +33,67 @@ def small_plate():
     return body
 
 
-def exact_rows(ob, o0, o1):
+def exact_rows(ob, owned_points):
     """Owned points and every point bonded to one of them (from the oracle's bond lists)."""
-    nb = set(range(o0, o1))
-    for i in range(o0, o1):
+    nb = set(int(i) for i in owned_points)
+    for i in owned_points:
         nb.update(ob.nbr[ob.off[i]:ob.off[i + 1]].tolist())
     return np.array(sorted(nb))
 
 
-@pytest.mark.parametrize("n_parts", [2, 3, 5])
-def test_plan_rows_and_exchange_lists(n_parts):
+def test_decompositions():
+    body = small_plate()
+    owner = decompose(body, 3, "index")
+    assert [np.nonzero(owner == p)[0].tolist() for p in range(3)] == \
+        [list(range(a, b)) for a, b in distribute_equally(body.n_points, 3)]
+    owner = decompose(body, 4, "slabs")          # the plate is longest along x
+    x = body._pos[:, 0]
+    counts = np.bincount(owner, minlength=4)
+    assert counts.max() - counts.min() <= 1
+    for p in range(3):
+        assert x[owner == p].max() <= x[owner == p + 1].min()
+
+
+@pytest.mark.parametrize("how,n_parts", [("index", 2), ("index", 3), ("index", 5), ("slabs", 3)])
+def test_plan_rows_and_exchange_lists(how, n_parts):
     body = small_plate()
     ob = oracle_body(body)
-    ranges = distribute_equally(body.n_points, n_parts)
+    owner = decompose(body, n_parts, how)
     plans = []
-    for p, (o0, o1) in enumerate(ranges):
-        rows = exact_rows(ob, o0, o1)
-        assert set(rows) <= set(candidate_rows(body, o0, o1))
-        owned = ((rows >= o0) & (rows < o1)).astype(np.uint8)
-        recv = recv_blocks(rows, owned, ranges)
-        # every halo row is received once, from its owner, in a contiguous block
+    for p in range(n_parts):
+        own_pts = np.nonzero(owner == p)[0]
+        rows = exact_rows(ob, own_pts)
+        assert set(rows) <= set(candidate_rows(body, own_pts))
+        owned = (owner[rows] == p).astype(np.uint8)
+        recv = recv_lists(rows, owned, owner)
+        # every halo row is received once, from its owner
         got = np.sort(np.concatenate([g for _, g in recv.values()])) if recv else np.array([])
         assert np.array_equal(got, rows[owned == 0])
-        for src, (row0, gids) in recv.items():
-            assert np.array_equal(rows[row0:row0 + len(gids)], gids)
-            assert all(ranges[src][0] <= g < ranges[src][1] for g in gids)
-        plans.append((rows, owned, recv, int(np.searchsorted(rows, o0))))
-    requests = [{s: g for s, (_, g) in recv.items()} for _, _, recv, _ in plans]
-    for p, (rows, owned, recv, own0) in enumerate(plans):
-        for dst, srows in send_rows(p, ranges, own0, requests).items():
+        for src, (r, gids) in recv.items():
+            assert np.array_equal(rows[r], gids) and (owner[gids] == src).all()
+            if how == "index":     # contiguous point ranges: one block of rows per source
+                assert r[-1] - r[0] + 1 == len(r)
+        plans.append((rows, owned, recv))
+    requests = [{s: g for s, (_, g) in recv.items()} for _, _, recv in plans]
+    for p, (rows, owned, recv) in enumerate(plans):
+        for dst, srows in send_rows(p, rows, requests).items():
             # the rows p sends to dst are the points dst holds as halo rows from p, in order
             assert np.array_equal(rows[srows], plans[dst][2][p][1])
             assert owned[srows].all()
+
+
+def test_bond_segments():
+    nn = np.array([2, 0, 3, 1])
+    assert bond_segments(nn, [0, 2]).tolist() == [0, 1, 2, 3, 4]
+    assert bond_segments(nn, [3, 1, 0]).tolist() == [5, 0, 1]
+    assert bond_segments(nn, []).tolist() == []
 
 
 def test_part_body_restricts_conditions_to_owned_rows():
     body = small_plate()
     ob = oracle_body(body)
     o0, o1 = distribute_equally(body.n_points, 2)[1]
-    rows = exact_rows(ob, o0, o1)
+    rows = exact_rows(ob, np.arange(o0, o1))
     owned = ((rows >= o0) & (rows < o1)).astype(np.uint8)
     sub = part_body(body, rows, owned)
     top = body.point_sets["top"]
@@ -87,24 +110,22 @@ class OraclePart:
     """A partition whose force is the FP64 oracle on its rows (halo rows bonded to all rows
     in reach: only the owned rows' forces are used)."""
 
-    def __init__(self, body, ranges, part, ob_body):
+    def __init__(self, body, owner, part, ob_body):
         import torch
-        o0, o1 = ranges[part]
-        self.part, self.n_parts, self.ranges = part, len(ranges), ranges
-        self.rows = exact_rows(ob_body, o0, o1)
-        self.owned = ((self.rows >= o0) & (self.rows < o1)).astype(np.uint8)
+        self.part, self.n_parts = part, int(owner.max()) + 1
+        self.rows = exact_rows(ob_body, np.nonzero(owner == part)[0])
+        self.owned = (owner[self.rows] == part).astype(np.uint8)
+        self.owned_rows = np.nonzero(self.owned)[0]
         self.sub = part_body(body, self.rows, self.owned)
         self.ob = oracle_body(self.sub)
-        self.own_row0 = int(np.searchsorted(self.rows, o0))
-        self.n_owned = o1 - o0
-        self.recv = recv_blocks(self.rows, self.owned, ranges)
+        self.recv = recv_lists(self.rows, self.owned, owner)
         self.torch = torch
 
     def requests(self):
         return {s: g for s, (_, g) in self.recv.items()}
 
     def link(self, requests):
-        self.send = send_rows(self.part, self.ranges, self.own_row0, requests)
+        self.send = send_rows(self.part, self.rows, requests)
         t = self.torch
         self.send_bufs = {0: {d: (t.from_numpy(r), t.empty(len(r) * 24, dtype=t.uint8))
                               for d, r in self.send.items()}}
@@ -116,8 +137,8 @@ class OraclePart:
 
     def unpack(self, kind):
         for s, buf in self.recv_bufs[kind].items():
-            row0, g = self.recv[s]
-            self.ob.pos[row0:row0 + len(g)] = buf.numpy().view(np.float64).reshape(-1, 3)
+            rows, _ = self.recv[s]
+            self.ob.pos[rows] = buf.numpy().view(np.float64).reshape(-1, 3)
 
 
 def vv_steps(ob, sets, n, dt, v, exchange=None):
@@ -138,7 +159,7 @@ def vv_steps(ob, sets, n, dt, v, exchange=None):
         ob.v[:] = ob.vh + 0.5 * dt * ob.a
 
 
-def _rank(rank, world, port, q):
+def _rank(rank, world, port, how, q):
     import datetime
     import torch.distributed as dist
     os.environ["MASTER_ADDR"] = "127.0.0.1"
@@ -148,8 +169,8 @@ def _rank(rank, world, port, q):
     try:
         body = small_plate()
         gob = oracle_body(body)
-        ranges = distribute_equally(body.n_points, world)
-        part = OraclePart(body, ranges, rank, gob)
+        owner = decompose(body, world, how)
+        part = OraclePart(body, owner, rank, gob)
         link_partitions([part], dist)
         # calc_stable_timestep: the minimum over the ranks is the body's step
         import torch
@@ -160,11 +181,11 @@ def _rank(rank, world, port, q):
         ex(0)
         part.ob.force_density(0.0, dt)
         vv_steps(part.ob, part.sub.point_sets, 40, dt, 0.5, exchange=ex)
-        sl = slice(part.own_row0, part.own_row0 + part.n_owned)
+        own = part.owned_rows
         nn = np.diff(part.ob.off)
-        off = np.concatenate(([0], np.cumsum(nn)))
-        bonds = part.ob.bond_active[off[part.own_row0]:off[part.own_row0 + part.n_owned]]
-        out = (rank, dt, part.ob.u[sl].copy(), part.ob.v[sl].copy(), bonds.copy())
+        bonds = part.ob.bond_active[bond_segments(nn, own)]
+        out = (rank, dt, part.rows[own], part.ob.u[own].copy(), part.ob.v[own].copy(),
+               bonds.copy(), nn[own])
         gathered = [None] * world
         dist.all_gather_object(gathered, out)
         if rank == 0:
@@ -181,11 +202,12 @@ def _free_port():
 
 
 @pytest.mark.timeout(180)
-def test_two_gloo_ranks_step_like_the_undivided_body():
+@pytest.mark.parametrize("how", ["index", "slabs"])
+def test_two_gloo_ranks_step_like_the_undivided_body(how):
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
     port = _free_port()
-    procs = [ctx.Process(target=_rank, args=(r, 2, port, q)) for r in range(2)]
+    procs = [ctx.Process(target=_rank, args=(r, 2, port, how, q)) for r in range(2)]
     for p in procs:
         p.start()
     res = sorted(q.get(timeout=150), key=lambda r: r[0])
@@ -198,9 +220,15 @@ def test_two_gloo_ranks_step_like_the_undivided_body():
     assert all(r[1] == dt for r in res)
     ob.force_density(0.0, dt)
     vv_steps(ob, body.point_sets, 40, dt, 0.5)
-    u = np.concatenate([r[2] for r in res])
-    v = np.concatenate([r[3] for r in res])
-    bonds = np.concatenate([r[4] for r in res])
+    u = np.empty_like(ob.u)
+    v = np.empty_like(ob.v)
+    nn = np.zeros(body.n_points, np.int64)
+    for _, _, gids, uu, vv, _, n_nb in res:
+        u[gids], v[gids], nn[gids] = uu, vv, n_nb
+    bonds = np.empty(int(nn.sum()), np.uint8)
+    for _, _, gids, _, _, b, _ in res:
+        bonds[bond_segments(nn, gids)] = b
     assert np.array_equal(u, ob.u) and np.array_equal(v, ob.v)
+    assert np.array_equal(nn, np.diff(ob.off))
     assert np.array_equal(bonds, ob.bond_active[:ob.n_bonds])
     assert np.count_nonzero(bonds == 0) > 0      # bonds failed during the run

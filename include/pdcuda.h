@@ -308,7 +308,9 @@ pd_status pd_vv_end(pd_handle *h);
 
 /* Halo data (exchange_loc_to_halo!): kind 0 = the point state the force kernels gather from
  * neighbours, exchanged after stage 0; kind 1 = the per-point state of the first force kernel
- * that the second one gathers (OSB, CMat; nothing for BB), exchanged after stage 1. Every row
+ * that the second one gathers (OSB, CMat; nothing for BB), exchanged after stage 1; kind 2 =
+ * the surface-correction multiplication factors, exchanged once between pd_esc_init(h, 1)
+ * and pd_esc_init(h, 2) (exchange_loc_to_halo!(get_mfactor, ...), :82, :92). Every row
  * is pd_halo_row_bytes bytes. pd_halo_pack gathers rows d_rows[0 .. n_rows) (int32, device)
  * into d_buf (device); pd_halo_unpack writes d_buf into rows d_rows[0 .. n_rows) and finishes
  * them (FP32: the split displacement; CMat with directed bond states: the bonds of killed
@@ -319,6 +321,25 @@ pd_status pd_halo_pack(pd_handle *h, int32_t kind, const int32_t *d_rows, int64_
                        void *d_buf);
 pd_status pd_halo_unpack(pd_handle *h, int32_t kind, const int32_t *d_rows, int64_t n_rows,
                          const void *d_buf);
+
+/* ---------------------------------------------------------------------------------------
+ * EnergySurfaceCorrection (src/discretization/bond_system_corrections.jl) of BBMaterial and
+ * OSBMaterial: BBMaterial{EnergySurfaceCorrection}() / OSBMaterial{EnergySurfaceCorrection}().
+ * --------------------------------------------------------------------------------------- */
+
+/* initialize! of the correction (:78-94), after the pre-cracks: what = 0 computes the
+ * multiplication factors of every point from the current bond states (calc_mfactor!, :96-124)
+ * and the factor of every bond from them (calc_scfactor!, :156-204); from then on every force
+ * evaluation multiplies each bond by its factor (BB: bond_based.jl:156, 175; OSB: weighted
+ * volume, dilatation and force, ordinary_state_based.jl:143-198). what = 1 computes only the
+ * multiplication factors and what = 2 only the bond factors (a partition exchanges the halo
+ * rows' multiplication factors between the two). FP32 OSB uses the one-row bond stream (pipe
+ * 0) with the correction. PD_ERR_UNSUPPORTED for CMaterial. */
+pd_status pd_esc_init(pd_handle *h, int32_t what);
+
+/* The multiplication factors (3n doubles, {x, y, z} per point, may be NULL) and the bond
+ * factors (n_bonds doubles in CSR order, may be NULL), host arrays. */
+pd_status pd_esc_get(pd_handle *h, double *mfactor, double *scfactor);
 
 /* ---------------------------------------------------------------------------------------
  * Dynamic relaxation (src/time_solvers/dynamic_relaxation.jl): adaptive-damping explicit

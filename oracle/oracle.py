@@ -34,7 +34,8 @@ class Sys(C.Structure):
                 ("nbr", C.c_void_p), ("L", C.c_void_p), ("fail_permit", C.c_void_p),
                 ("omega", C.c_void_p), ("pid", C.c_void_p), ("params", C.c_void_p),
                 ("n_params", C.c_int32), ("material", C.c_int32), ("cmodel", C.c_int32),
-                ("multi", C.c_int32), ("zem_cs", C.c_double), ("maxdmg", C.c_double)]
+                ("multi", C.c_int32), ("zem_cs", C.c_double), ("maxdmg", C.c_double),
+                ("scfactor", C.c_void_p)]
 
 
 class State(C.Structure):
@@ -82,6 +83,9 @@ def lib():
         L.or_point_params.restype = C.c_int
         L.or_point_params.argtypes = [i32] + [dbl] * 10 + [vp, C.c_char_p, i32]
         L.or_set_threads.argtypes = [i32]
+        L.or_esc_mfactor.argtypes = [vp, vp, vp]
+        L.or_esc_scfactor.argtypes = [vp, vp, vp]
+        L.or_esc_lame.argtypes = [vp, vp, i64, vp]
         _LIB = L
     return _LIB
 
@@ -160,7 +164,7 @@ class OracleBody:
         self.sys = Sys(n, B, _p(self.X), _p(self.vol), _p(self.off), _p(self.nbr), _p(self.L),
                        _p(self.fail_permit), _p(self.omega), _p(self.pid),
                        C.cast(self.params, C.c_void_p), len(params), material, cmodel, multi,
-                       zem_cs, maxdmg)
+                       zem_cs, maxdmg, None)
         lib().or_kernels(C.byref(self.sys), kernel, _p(self.omega))
         z3 = lambda: np.zeros((n, 3), np.float64)
         self.pos, self.u, self.v, self.vh, self.a, self.b_int, self.b_ext = (z3() for _ in range(7))
@@ -186,6 +190,21 @@ class OracleBody:
         a[np.asarray(set_a, np.int64)] = 1
         b[np.asarray(set_b, np.int64)] = 1
         lib().or_break_bonds(C.byref(self.sys), C.byref(self.st), _p(a), _p(b))
+
+    def init_surface_correction(self):
+        """EnergySurfaceCorrection (bond_system_corrections.jl:78-124, 156-204) from the
+        current bond states: mfactor (n, 3) and scfactor (n_bonds), then used by the force."""
+        self.mfactor = np.zeros((self.n, 3), np.float64)
+        self.scfactor = np.ones(max(self.n_bonds, 1), np.float64)
+        lib().or_esc_mfactor(C.byref(self.sys), C.byref(self.st), _p(self.mfactor))
+        lib().or_esc_scfactor(C.byref(self.sys), _p(self.mfactor), _p(self.scfactor))
+        self.sys.scfactor = _p(self.scfactor)
+
+    def esc_lame(self, i):
+        """get_averaged_lame_parameters of point i: (lambda, mu)."""
+        out = np.zeros(2)
+        lib().or_esc_lame(C.byref(self.sys), C.byref(self.st), int(i), _p(out))
+        return out
 
     def calc_damage(self):
         lib().or_calc_damage(C.byref(self.sys), C.byref(self.st))

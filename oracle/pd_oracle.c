@@ -388,6 +388,9 @@ void or_calc_damage(const or_sys *sys, or_state *st) {
 
 static inline const or_params *P_of(const or_sys *sys, int64_t i) { return &sys->params[sys->pid[i]]; }
 
+/* surface_correction_factor (bond_system_corrections.jl:37-39, 72-75) */
+#define SCF(sys, b) ((sys)->scfactor ? (sys)->scfactor[b] : 1.0)
+
 /* calc_failure!: bond_system.jl:309-327 (generic) and bond_based.jl:125-144 /
  * ordinary_state_based.jl:107-126 (store the current bond length) */
 static void failure_point(const or_sys *sys, or_state *st, int64_t i) {
@@ -418,7 +421,7 @@ static void bb_force_point(const or_sys *sys, or_state *st, int64_t i) {
         double d[3] = {x[3 * j] - x[3 * i], x[3 * j + 1] - x[3 * i + 1], x[3 * j + 2] - x[3 * i + 2]};
         double l = st->bond_length[b];
         double eps = (l - Lb) / Lb;
-        double om = bmul(st->bond_active[b], 1.0);
+        double om = bmul(st->bond_active[b], SCF(sys, b));
         double s;
         if (sys->multi) s = om * (pi->bc + P_of(sys, j)->bc) / 2 * eps * sys->vol[j];
         else s = om * pi->bc * eps * sys->vol[j];
@@ -435,7 +438,7 @@ static void osb_force_point(const or_sys *sys, or_state *st, double *bsink, int6
         int32_t j = sys->nbr[b];
         double D[3] = {X[3 * j] - X[3 * i], X[3 * j + 1] - X[3 * i + 1], X[3 * j + 2] - X[3 * i + 2]};
         double om = sys->omega[b] * (st->bond_active[b] ? 1.0 : 0.0);
-        wvol += om * 1.0 * dot3(D, D) * sys->vol[j];
+        wvol += om * SCF(sys, b) * dot3(D, D) * sys->vol[j];
     }
     if (wvol == 0.0) return;
     double dil = 0.0, c1d = 3.0 / wvol;
@@ -443,7 +446,7 @@ static void osb_force_point(const or_sys *sys, or_state *st, double *bsink, int6
         int32_t j = sys->nbr[b];
         double Lb = sys->L[b], l = st->bond_length[b];
         double om = sys->omega[b] * (st->bond_active[b] ? 1.0 : 0.0);
-        dil += om * 1.0 * c1d * Lb * (l - Lb) * sys->vol[j];
+        dil += om * SCF(sys, b) * c1d * Lb * (l - Lb) * sys->vol[j];
     }
     double c1 = 0, c2 = 0;
     if (!sys->multi) {
@@ -460,7 +463,7 @@ static void osb_force_point(const or_sys *sys, or_state *st, double *bsink, int6
             c2 = dil * (3.0 * (pi->K + pj->K) / (2 * wvol) - c1 / 3.0);
         }
         double om = sys->omega[b] * (st->bond_active[b] ? 1.0 : 0.0);
-        double s = om * 1.0 * (c2 * Lb + c1 * (l - Lb)) / l;
+        double s = om * SCF(sys, b) * (c2 * Lb + c1 * (l - Lb)) / l;
         for (int k = 0; k < 3; k++) {
             double p = s * d[k];
             bsink[3 * i + k] += p * sys->vol[j];
@@ -693,4 +696,138 @@ int64_t or_run_vv(const or_sys *sys, or_state *st, const or_bc *bcs, int32_t n_b
         }
     }
     return 0;
+}
+
+/* ---------------------------------------------------------------------------------------
+ * EnergySurfaceCorrection (src/discretization/bond_system_corrections.jl)
+ * --------------------------------------------------------------------------------------- */
+
+/* coordinate k of point j uniformly stretched by lam along dimension d (calc_mfactor! :101-104) */
+static inline double stretched(const or_sys *sys, int64_t j, int k, int d, double lam) {
+    return k == d ? lam * sys->X[3 * j + k] : sys->X[3 * j + k];
+}
+
+/* strain_energy_density_point! with scfactor = 1: BB (bond_based.jl:183-201) and OSB
+ * (ordinary_state_based.jl:206-234, update_bond_lengths! :236-247) at the stretched positions */
+static double esc_energy(const or_sys *sys, const or_state *st, int64_t i, int d, double lam) {
+    const or_params *pi = P_of(sys, i);
+    int64_t b0 = sys->off[i], b1 = sys->off[i + 1];
+    double xi[3] = {stretched(sys, i, 0, d, lam), stretched(sys, i, 1, d, lam), stretched(sys, i, 2, d, lam)};
+    if (sys->material == OR_BB) {
+        double psi = 0.0;
+        for (int64_t b = b0; b < b1; b++) {
+            int32_t j = sys->nbr[b];
+            double Lb = sys->L[b];
+            double dx[3] = {stretched(sys, j, 0, d, lam) - xi[0], stretched(sys, j, 1, d, lam) - xi[1],
+                            stretched(sys, j, 2, d, lam) - xi[2]};
+            double l = sqrt(dot3(dx, dx));
+            double eps = (l - Lb) / Lb;
+            double om = bmul(st->bond_active[b], 1.0);
+            double bc = (pi->bc + P_of(sys, j)->bc) / 2;
+            psi += 0.25 * om * bc * eps * eps * Lb * sys->vol[j];
+        }
+        return psi;
+    }
+    const double *X = sys->X;
+    double wvol = 0.0;
+    for (int64_t b = b0; b < b1; b++) {
+        int32_t j = sys->nbr[b];
+        double D[3] = {X[3 * j] - X[3 * i], X[3 * j + 1] - X[3 * i + 1], X[3 * j + 2] - X[3 * i + 2]};
+        double om = sys->omega[b] * (st->bond_active[b] ? 1.0 : 0.0);
+        wvol += om * 1.0 * dot3(D, D) * sys->vol[j];
+    }
+    if (wvol == 0.0) return 0.0;  /* the density keeps its cleared value */
+    double dil = 0.0, c1d = 3.0 / wvol;
+    for (int64_t b = b0; b < b1; b++) {
+        int32_t j = sys->nbr[b];
+        double Lb = sys->L[b];
+        double dx[3] = {stretched(sys, j, 0, d, lam) - xi[0], stretched(sys, j, 1, d, lam) - xi[1],
+                        stretched(sys, j, 2, d, lam) - xi[2]};
+        double l = sqrt(dot3(dx, dx));
+        double om = sys->omega[b] * (st->bond_active[b] ? 1.0 : 0.0);
+        dil += om * 1.0 * c1d * Lb * (l - Lb) * sys->vol[j];
+    }
+    double psivol = 0.5 * pi->K * (dil * dil);
+    double psidev = 0.0;
+    for (int64_t b = b0; b < b1; b++) {
+        int32_t j = sys->nbr[b];
+        double Lb = sys->L[b];
+        double dx[3] = {stretched(sys, j, 0, d, lam) - xi[0], stretched(sys, j, 1, d, lam) - xi[1],
+                        stretched(sys, j, 2, d, lam) - xi[2]};
+        double l = sqrt(dot3(dx, dx));
+        double e = l - Lb;
+        double edev = e - 1.0 / 3.0 * dil * Lb;
+        double om = sys->omega[b] * (st->bond_active[b] ? 1.0 : 0.0);
+        double G = (pi->G + P_of(sys, j)->G) / 2;
+        double cdev = 15.0 * G / (2 * wvol);
+        psidev += cdev * om * 1.0 * edev * edev * sys->vol[j];
+    }
+    return psivol + psidev;
+}
+
+/* get_averaged_lame_parameters (:126-148): the point's (lambda, mu), or with several
+ * parameter sets the mean over its active bonds of the bond-averaged pair */
+void or_esc_lame(const or_sys *sys, const or_state *st, int64_t i, double *lame) {
+    const or_params *pi = P_of(sys, i);
+    lame[0] = pi->lambda;
+    lame[1] = pi->mu;
+    if (!sys->multi) return;
+    double sl = 0.0, sm = 0.0;
+    int64_t na = 0;
+    for (int64_t b = sys->off[i]; b < sys->off[i + 1]; b++) {
+        if (!st->bond_active[b]) continue;
+        const or_params *pj = P_of(sys, sys->nbr[b]);
+        sl += (pi->lambda + pj->lambda) / 2;
+        sm += (pi->mu + pj->mu) / 2;
+        na++;
+    }
+    lame[0] = sl / (double)na;
+    lame[1] = sm / (double)na;
+}
+
+/* calc_mfactor! (:96-124) with stendens_uniext_small_strain (:150-152) */
+void or_esc_mfactor(const or_sys *sys, const or_state *st, double *mfactor) {
+    const double lam = 1.001;
+    for (int d = 0; d < 3; d++) {
+        for (int64_t i = 0; i < sys->n; i++) {
+            double lame[2];
+            or_esc_lame(sys, st, i, lame);
+            double psi_theory = (0.5 * lame[0] + lame[1]) * ((lam - 1) * (lam - 1));
+            mfactor[3 * i + d] = psi_theory / esc_energy(sys, st, i, d, lam);
+        }
+    }
+}
+
+/* calc_scfactor! (:156-204): the factor of bond i -> j from the mean mfactor of i and j in
+ * the directions of the reference bond */
+void or_esc_scfactor(const or_sys *sys, const double *mf, double *scfactor) {
+    const double *X = sys->X;
+    const double half_pi = 90 * M_PI / 180;
+    for (int64_t i = 0; i < sys->n; i++) {
+        for (int64_t b = sys->off[i]; b < sys->off[i + 1]; b++) {
+            int32_t j = sys->nbr[b];
+            double Lb = sys->L[b];
+            double ax = fabs(X[3 * j] - X[3 * i]), ay = fabs(X[3 * j + 1] - X[3 * i + 1]),
+                   az = fabs(X[3 * j + 2] - X[3 * i + 2]);
+            double scx = (mf[3 * i] + mf[3 * j]) / 2;
+            double scy = (mf[3 * i + 1] + mf[3 * j + 1]) / 2;
+            double scz = (mf[3 * i + 2] + mf[3 * j + 2]) / 2;
+            double scr, th, ph;
+            if (az <= 1e-10) {
+                if (ay <= 1e-10) th = 0.0;
+                else if (ax <= 1e-10) th = half_pi;
+                else th = atan(ay / ax);
+                ph = half_pi;
+            } else if (ax <= 1e-10 && ay <= 1e-10) {
+                scfactor[b] = scz;
+                continue;
+            } else {
+                th = atan(ay / ax);
+                ph = acos(az / Lb);
+            }
+            double a = cos(th) * sin(ph), c = sin(th) * sin(ph), e = cos(ph);
+            scr = sqrt(1 / ((a * a / (scx * scx) + c * c / (scy * scy)) + e * e / (scz * scz)));
+            scfactor[b] = scr;
+        }
+    }
 }

@@ -51,6 +51,7 @@ typedef struct {
     int32_t multi;            /* 1: ParameterHandler semantics (per-bond averaged parameters) */
     double zem_cs;            /* ZEMSilling Cs */
     double maxdmg;            /* CMaterial maxdmg */
+    const double *scfactor;   /* B surface correction factor per bond; NULL: NoCorrection */
 } or_sys;
 
 typedef struct {
@@ -93,6 +94,11 @@ int or_point_params(int32_t material, double delta, double rho, double E, double
                     double K, double lambda, double mu, double Gc, double epsc,
                     or_params *out, char *msg, int32_t msg_len);
 void or_set_threads(int32_t n);
+/* EnergySurfaceCorrection (bond_system_corrections.jl): mfactor[3 i + d] of every point from the
+ * current bond states (calc_mfactor!), and the per-bond factor from it (calc_scfactor!). */
+void or_esc_mfactor(const or_sys *sys, const or_state *st, double *mfactor);
+void or_esc_lame(const or_sys *sys, const or_state *st, int64_t i, double *lame);
+void or_esc_scfactor(const or_sys *sys, const double *mfactor, double *scfactor);
 
 #ifdef __cplusplus
 }

@@ -272,6 +272,20 @@ static pd_status relayout(pd_handle* h, int G) {
     launch_relayout_f4(a, b, a.geo, geo, h->stream);
     b.geo = geo;
   }
+  if (a.sc64) {  // surface correction factors follow the bond slots
+    double* sc = nullptr;
+    PD_TRY(dalloc(h, &sc, nslots));
+    PD_CUDA(cudaMemsetAsync(sc, 0, sizeof(double) * (nslots > 0 ? nslots : 1), h->stream));
+    launch_relayout_f64(a, b, a.sc64, sc, h->stream);
+    b.sc64 = sc;
+  }
+  if (a.sc32) {
+    float* sc = nullptr;
+    PD_TRY(dalloc(h, &sc, nslots));
+    PD_CUDA(cudaMemsetAsync(sc, 0, sizeof(float) * (nslots > 0 ? nslots : 1), h->stream));
+    launch_relayout_i32(a, b, reinterpret_cast<const int*>(a.sc32), reinterpret_cast<int*>(sc), h->stream);
+    b.sc32 = sc;
+  }
   unsigned* bits = nullptr;
   unsigned char* bytes = nullptr;
   PD_TRY(dalloc(h, &bits, nslots / 32 + 1));
@@ -285,6 +299,7 @@ static pd_status relayout(pd_handle* h, int G) {
   dfree(h, bytes);
   dfree(h, (void*)a.soff); dfree(h, (void*)a.nbr); dfree(h, (void*)a.rev);
   dfree(h, (void*)a.len64); dfree(h, (void*)a.geo); dfree(h, a.bits);
+  dfree(h, (void*)a.sc64); dfree(h, (void*)a.sc32);
   h->d = b;
   h->nslots = nslots;
   destroy_graph(h);
@@ -911,7 +926,8 @@ extern "C" pd_status pd_set_param_timesteps(pd_handle* h, const double* dtp) {
 static int launch_force(pd_handle* h, int kstep, int phase) {
   int k;
   if (h->precision == PD_PREC_FP64) k = launch_force64(h->d, h->cfg, kstep, phase, h->stream);
-  else if (h->cfg.pipe >= 1 && h->cfg.pipe <= 3 && tma_supported(h->d)) k = launch_force32_tma(h->d, h->cfg.pipe, kstep, phase, h->stream);
+  else if (h->cfg.pipe >= 1 && h->cfg.pipe <= 3 && !h->d.sc32 && tma_supported(h->d))
+    k = launch_force32_tma(h->d, h->cfg.pipe, kstep, phase, h->stream);
   else k = launch_force32(h->d, h->cfg, kstep, phase, h->stream);
   h->launches += k;
   return k;

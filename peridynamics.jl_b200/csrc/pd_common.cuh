@@ -103,6 +103,11 @@ struct DevBody {
   double* PK64;      // CMat FP64: P K^-1 (9 per point)
   float* H32;        // CMat FP32: displacement gradient H = F - I (9 per point)
   float4* cst32;     // CMat FP32: 3 float4 per point {A (9), beta~, 0, 0}
+  // EnergySurfaceCorrection (BB, OSB): the factor of every bond slot (FP64 / FP32 path) and
+  // the per-point multiplication factors {x, y, z} it is made from; null without correction
+  const double* sc64;
+  const float* sc32;
+  double* mf;
   Ctrl* ctrl;
   int material, kernel, cmodel, sym, multi;
   double maxdmg;

@@ -85,7 +85,8 @@ __device__ __forceinline__ void commit_row(unsigned int* bits, long long word_id
 // -------------------------------------------------------------------------------------------
 // BB (bond_based.jl:125-180): one sweep, failure then the pairwise force
 // -------------------------------------------------------------------------------------------
-template <int G, bool MULTI>
+// ESC: the bond's surface correction factor multiplies its force (bond_based.jl:156, 175)
+template <int G, bool MULTI, bool ESC>
 __global__ void PD_LB k_bb32(DevBody d, int kstep) {
   if (d.ctrl->err) return;
   PD_SLICE_LOOP(G) {
@@ -112,7 +113,8 @@ __global__ void PD_LB k_bb32(DevBody d, int kstep) {
         if (act) {
           float bc = bci;
           if (MULTI) bc = 0.5f * (bci + d.params[d.meta[j] & META_PID_MASK].bcf);
-          const float sc = bc * B.eps * hj.w * B.rl;
+          float sc = bc * B.eps * hj.w * B.rl;
+          if (ESC) sc *= __ldg(d.sc32 + b);
           bx.add(sc * B.ex); by.add(sc * B.ey); bz.add(sc * B.ez);
         }
       }
@@ -133,7 +135,8 @@ __global__ void PD_LB k_bb32(DevBody d, int kstep) {
 // OSB phase A (ordinary_state_based.jl:107-126, 176-204): failure, weighted volume m,
 // dilatation theta, and c1 = 15 G / m, c2 = theta (3 K / m - c1 / 3) (:135-136)
 // -------------------------------------------------------------------------------------------
-template <int G>
+// ESC: the bond factor beta in the weighted volume and the dilatation (:182, :198)
+template <int G, bool ESC>
 __global__ void PD_LB_A k_osb_a32(DevBody d, int kstep) {
   if (d.ctrl->err) return;
   PD_SLICE_LOOP(G) {
@@ -166,7 +169,8 @@ __global__ void PD_LB_A k_osb_a32(DevBody d, int kstep) {
         bond32(g, hi, lo, hj, lj, B);
         act = ((word >> lane) & 1u) && !fails32(B, epsc);
         if (act) {
-          const float om = omega_r(d.kernel, delta, B.L, B.rL) * hj.w;
+          float om = omega_r(d.kernel, delta, B.L, B.rL) * hj.w;
+          if (ESC) om *= __ldg(d.sc32 + b0 + (long long)r * 32);
           m.add(om * (B.gx * B.gx + B.gy * B.gy + B.gz * B.gz));
           th.add(om * B.L * B.e);
         }
@@ -207,7 +211,8 @@ __device__ __forceinline__ float osb_s32(const float2& c, const float2& m, const
 // -------------------------------------------------------------------------------------------
 // OSB phase B (ordinary_state_based.jl:128-174): b_i = sum_j (s_ij + s_ji) V_j eta / l
 // -------------------------------------------------------------------------------------------
-template <int G, bool MULTI>
+// ESC: beta of the bond, which is also the factor of its reverse bond (equal by construction)
+template <int G, bool MULTI, bool ESC>
 __global__ void PD_LB k_osb_b32(DevBody d, int kstep) {
   if (d.ctrl->err) return;
   PD_SLICE_LOOP(G) {
@@ -257,7 +262,8 @@ __global__ void PD_LB k_osb_b32(DevBody d, int kstep) {
       const float oj = aj ? omega_r(d.kernel, Pj->deltaf, B.L, B.rL) : 0.f;
       const float si = osb_s32<MULTI>(ci, mi, Pi, *Pj, oi, B.L, B.e);
       const float sj = osb_s32<MULTI>(cj, mj, *Pj, Pi, oj, B.L, B.e);
-      const float f = (si + sj) * hj.w * B.rl;
+      float f = (si + sj) * hj.w * B.rl;
+      if (ESC) f *= __ldg(d.sc32 + b);
       bx.add(f * B.ex); by.add(f * B.ey); bz.add(f * B.ez);
     }
     if (G > 1) { group_reduce<G>(bx); group_reduce<G>(by); group_reduce<G>(bz); }
@@ -668,9 +674,24 @@ int launch_force32(const DevBody& d, const LaunchCfg& c, int kstep, int phase, c
   int launches = 0;
   if (d.material == MAT_BB) {
     if (!A) return 0;
-    if (d.multi) { PD_DISPATCH_G(G, (k_bb32<GG, true><<<grid, c.block, 0, s>>>(d, kstep))); }
-    else { PD_DISPATCH_G(G, (k_bb32<GG, false><<<grid, c.block, 0, s>>>(d, kstep))); }
+    if (d.sc32) {
+      if (d.multi) { PD_DISPATCH_G(G, (k_bb32<GG, true, true><<<grid, c.block, 0, s>>>(d, kstep))); }
+      else { PD_DISPATCH_G(G, (k_bb32<GG, false, true><<<grid, c.block, 0, s>>>(d, kstep))); }
+    } else if (d.multi) {
+      PD_DISPATCH_G(G, (k_bb32<GG, true, false><<<grid, c.block, 0, s>>>(d, kstep)));
+    } else {
+      PD_DISPATCH_G(G, (k_bb32<GG, false, false><<<grid, c.block, 0, s>>>(d, kstep)));
+    }
     return 1;
+  }
+  if (d.material == MAT_OSB && d.sc32) {  // surface correction: the one-row kernels
+    if (A) { PD_DISPATCH_G(G, (k_osb_a32<GG, true><<<grid, c.block, 0, s>>>(d, kstep))); launches++; }
+    if (B) {
+      if (d.multi) { PD_DISPATCH_G(G, (k_osb_b32<GG, true, true><<<grid, c.block, 0, s>>>(d, kstep))); }
+      else { PD_DISPATCH_G(G, (k_osb_b32<GG, false, true><<<grid, c.block, 0, s>>>(d, kstep))); }
+      launches++;
+    }
+    return launches;
   }
   if (d.material == MAT_OSB && c.pipe == 4) {
     if (A) { PD_DISPATCH_G(G, (k_osb_a32u<GG><<<grid, c.block, 0, s>>>(d, kstep))); launches++; }
@@ -682,10 +703,10 @@ int launch_force32(const DevBody& d, const LaunchCfg& c, int kstep, int phase, c
     return launches;
   }
   if (d.material == MAT_OSB) {
-    if (A) { PD_DISPATCH_G(G, (k_osb_a32<GG><<<grid, c.block, 0, s>>>(d, kstep))); launches++; }
+    if (A) { PD_DISPATCH_G(G, (k_osb_a32<GG, false><<<grid, c.block, 0, s>>>(d, kstep))); launches++; }
     if (B) {
-      if (d.multi) { PD_DISPATCH_G(G, (k_osb_b32<GG, true><<<grid, c.block, 0, s>>>(d, kstep))); }
-      else { PD_DISPATCH_G(G, (k_osb_b32<GG, false><<<grid, c.block, 0, s>>>(d, kstep))); }
+      if (d.multi) { PD_DISPATCH_G(G, (k_osb_b32<GG, true, false><<<grid, c.block, 0, s>>>(d, kstep))); }
+      else { PD_DISPATCH_G(G, (k_osb_b32<GG, false, false><<<grid, c.block, 0, s>>>(d, kstep))); }
       launches++;
     }
     return launches;

@@ -123,7 +123,8 @@ __device__ __forceinline__ void commit_row64(unsigned int* bits, long long word_
 // (l - L) / (L l), in place of the reference's (l - L) / L and three divisions by l; the
 // forces differ from the serial order by a few units in the last place, as the lane-group sums
 // already do. The failure decision keeps the reference's expression.
-template <int G, bool MULTI, bool FAST>
+// ESC: the bond's surface correction factor multiplies its force (bond_based.jl:156, 175)
+template <int G, bool MULTI, bool FAST, bool ESC>
 __global__ void __launch_bounds__(256, FAST ? 3 : 2) k_bb64(DevBody d, int kstep) {
   if (d.ctrl->err) return;
   PD_SLICE_LOOP(G) {
@@ -161,7 +162,8 @@ __global__ void __launch_bounds__(256, FAST ? 3 : 2) k_bb64(DevBody d, int kstep
           const double q = (l - L) / (L * l);  // eps / l
           const double bcb =
               MULTI ? 0.5 * (P.bc + d.params[d.meta[u ? j1 : j0] & META_PID_MASK].bc) : P.bc;
-          const double sc = act ? bcb * q * xj.w : 0.0;
+          const double bet = ESC ? __ldg(d.sc64 + (u ? b1 : b0)) : 1.0;
+          const double sc = act ? bet * bcb * q * xj.w : 0.0;
           bx += sc * dx;
           by += sc * dy;
           bz += sc * dz;
@@ -188,7 +190,7 @@ __global__ void __launch_bounds__(256, FAST ? 3 : 2) k_bb64(DevBody d, int kstep
         {
           const double eps = (l - L) / L;
           act = ((word >> lane) & 1u) && !(eps > P.epsc && Ls > 0);
-          const double om = act ? 1.0 : 0.0;
+          const double om = act ? (ESC ? __ldg(d.sc64 + b) : 1.0) : 0.0;
           double sc;
           if (MULTI) {
             const double bcj = d.params[d.meta[j] & META_PID_MASK].bc;
@@ -219,7 +221,8 @@ __global__ void __launch_bounds__(256, FAST ? 3 : 2) k_bb64(DevBody d, int kstep
 // OSB phase A: calc_failure! (ordinary_state_based.jl:107-126), calc_damage!,
 // calc_weighted_volume (:176-189), calc_dilatation (:191-204), c1, c2 (:135-136)
 // -------------------------------------------------------------------------------------------
-template <int G, bool EXACT>
+// ESC: the bond factor beta in the weighted volume and the dilatation (:182, :198)
+template <int G, bool EXACT, bool ESC>
 __global__ void PD_LB64 k_osb_a64(DevBody d, int kstep) {
   if (d.ctrl->err) return;
   PD_SLICE_LOOP(G) {
@@ -246,8 +249,9 @@ __global__ void PD_LB64 k_osb_a64(DevBody d, int kstep) {
         act = ((word >> lane) & 1u) && !(eps > P.epsc && Ls > 0);
         const double DX = Xj.x - Xi.x, DY = Xj.y - Xi.y, DZ = Xj.z - Xi.z;
         const double om = act ? omega_of(d.kernel, P.delta, L) : 0.0;
-        wvol += om * 1.0 * ((DX * DX + DY * DY) + DZ * DZ) * xj.w;
-        if (!EXACT) sdil += om * 1.0 * L * (l - L) * xj.w;
+        const double bet = ESC ? __ldg(d.sc64 + b) : 1.0;
+        wvol += om * bet * ((DX * DX + DY * DY) + DZ * DZ) * xj.w;
+        if (!EXACT) sdil += om * bet * L * (l - L) * xj.w;
       }
       na += act;
       commit_row64(d.bits, wi, word, act, lane);
@@ -274,7 +278,7 @@ __global__ void PD_LB64 k_osb_a64(DevBody d, int kstep) {
         const double eps = (l - L) / L;
         const bool act = bond_bit_live(d.bits, b) && !(eps > P.epsc && Ls > 0);
         const double om = act ? omega_of(d.kernel, P.delta, L) : 0.0;
-        dil += om * 1.0 * c1d * L * (l - L) * xj.w;
+        dil += om * (ESC ? __ldg(d.sc64 + b) : 1.0) * c1d * L * (l - L) * xj.w;
       }
     } else if (wvol != 0.0) {
       dil = 3.0 / wvol * sdil;
@@ -295,7 +299,7 @@ __global__ void PD_LB64 k_osb_a64(DevBody d, int kstep) {
 // bond owner o with the partner q (ParameterHandler form :165-166 when MULTI)
 template <bool MULTI>
 __device__ __forceinline__ double osb_s64(const double4& co, const DevParam& Po, const DevParam& Pq,
-                                          double om, double L, double l) {
+                                          double om, double bet, double L, double l) {
   double c1, c2;
   if (MULTI) {
     c1 = 15.0 * (Po.G + Pq.G) / (2 * co.z);
@@ -304,13 +308,14 @@ __device__ __forceinline__ double osb_s64(const double4& co, const DevParam& Po,
     c1 = co.x;
     c2 = co.y;
   }
-  return om * 1.0 * (c2 * L + c1 * (l - L)) / l;
+  return om * bet * (c2 * L + c1 * (l - L)) / l;
 }
 
 // -------------------------------------------------------------------------------------------
 // OSB phase B: force_density_point! (ordinary_state_based.jl:128-174) in gather form
 // -------------------------------------------------------------------------------------------
-template <int G, bool EXACT, bool MULTI>
+// ESC: beta of the bond, which is also the factor of its reverse bond (equal by construction)
+template <int G, bool EXACT, bool MULTI, bool ESC>
 __global__ void PD_LB64 k_osb_b64(DevBody d, int kstep) {
   if (d.ctrl->err) return;
   PD_SLICE_LOOP(G) {
@@ -330,7 +335,7 @@ __global__ void PD_LB64 k_osb_b64(DevBody d, int kstep) {
       const bool act = bond_bit(d.bits, b);
       const double om = act ? omega_of(d.kernel, Pi.delta, L) : 0.0;
       const DevParam& Pj = MULTI ? d.params[d.meta[j] & META_PID_MASK] : Pi;
-      const double sc = osb_s64<MULTI>(ci, Pi, Pj, om, L, l);
+      const double sc = osb_s64<MULTI>(ci, Pi, Pj, om, ESC ? __ldg(d.sc64 + b) : 1.0, L, l);
       bx += sc * dx * xj.w;
       by += sc * dy * xj.w;
       bz += sc * dz * xj.w;
@@ -347,7 +352,7 @@ __global__ void PD_LB64 k_osb_b64(DevBody d, int kstep) {
       const bool act = d.sym ? bond_bit(d.bits, b) : bond_bit(d.bits, rev_slot(d, b, j));
       const DevParam& Pj = d.params[d.meta[j] & META_PID_MASK];
       const double om = act ? omega_of(d.kernel, Pj.delta, L) : 0.0;
-      const double sc = osb_s64<MULTI>(cj, Pj, Pi, om, L, l);
+      const double sc = osb_s64<MULTI>(cj, Pj, Pi, om, ESC ? __ldg(d.sc64 + b) : 1.0, L, l);
       bx += -(sc * dx) * xj.w;
       by += -(sc * dy) * xj.w;
       bz += -(sc * dz) * xj.w;
@@ -595,6 +600,41 @@ static int grid_for(long long nslices, int block) {
   return (int)blocks;
 }
 
+template <bool ESC>
+static void launch_bb64(const DevBody& d, const LaunchCfg& c, int G, int grid, int kstep, cudaStream_t s) {
+  if (c.exact) {
+    if (d.multi) k_bb64<1, true, false, ESC><<<grid, c.block, 0, s>>>(d, kstep);
+    else k_bb64<1, false, false, ESC><<<grid, c.block, 0, s>>>(d, kstep);
+  } else if (d.multi) {
+    PD_DISPATCH_G(G, (k_bb64<GG, true, true, ESC><<<grid, c.block, 0, s>>>(d, kstep)));
+  } else {
+    PD_DISPATCH_G(G, (k_bb64<GG, false, true, ESC><<<grid, c.block, 0, s>>>(d, kstep)));
+  }
+}
+
+template <bool ESC>
+static int launch_osb64(const DevBody& d, const LaunchCfg& c, int G, int grid, int kstep, bool A,
+                        bool B, cudaStream_t s) {
+  int launches = 0;
+  if (A) {
+    if (c.exact) k_osb_a64<1, true, ESC><<<grid, c.block, 0, s>>>(d, kstep);
+    else { PD_DISPATCH_G(G, (k_osb_a64<GG, false, ESC><<<grid, c.block, 0, s>>>(d, kstep))); }
+    launches++;
+  }
+  if (B) {
+    if (c.exact) {
+      if (d.multi) k_osb_b64<1, true, true, ESC><<<grid, c.block, 0, s>>>(d, kstep);
+      else k_osb_b64<1, true, false, ESC><<<grid, c.block, 0, s>>>(d, kstep);
+    } else if (d.multi) {
+      PD_DISPATCH_G(G, (k_osb_b64<GG, false, true, ESC><<<grid, c.block, 0, s>>>(d, kstep)));
+    } else {
+      PD_DISPATCH_G(G, (k_osb_b64<GG, false, false, ESC><<<grid, c.block, 0, s>>>(d, kstep)));
+    }
+    launches++;
+  }
+  return launches;
+}
+
 int launch_force64(const DevBody& d, const LaunchCfg& c, int kstep, int phase, cudaStream_t s) {
   const int G = d.lg;
   const int grid = grid_for(d.nslices, c.block);
@@ -602,34 +642,13 @@ int launch_force64(const DevBody& d, const LaunchCfg& c, int kstep, int phase, c
   int launches = 0;
   if (d.material == MAT_BB) {
     if (!A) return 0;
-    if (c.exact) {
-      if (d.multi) k_bb64<1, true, false><<<grid, c.block, 0, s>>>(d, kstep);
-      else k_bb64<1, false, false><<<grid, c.block, 0, s>>>(d, kstep);
-    } else if (d.multi) {
-      PD_DISPATCH_G(G, (k_bb64<GG, true, true><<<grid, c.block, 0, s>>>(d, kstep)));
-    } else {
-      PD_DISPATCH_G(G, (k_bb64<GG, false, true><<<grid, c.block, 0, s>>>(d, kstep)));
-    }
+    if (d.sc64) launch_bb64<true>(d, c, G, grid, kstep, s);
+    else launch_bb64<false>(d, c, G, grid, kstep, s);
     return 1;
   }
   if (d.material == MAT_OSB) {
-    if (A) {
-      if (c.exact) k_osb_a64<1, true><<<grid, c.block, 0, s>>>(d, kstep);
-      else { PD_DISPATCH_G(G, (k_osb_a64<GG, false><<<grid, c.block, 0, s>>>(d, kstep))); }
-      launches++;
-    }
-    if (B) {
-      if (c.exact) {
-        if (d.multi) k_osb_b64<1, true, true><<<grid, c.block, 0, s>>>(d, kstep);
-        else k_osb_b64<1, true, false><<<grid, c.block, 0, s>>>(d, kstep);
-      } else if (d.multi) {
-        PD_DISPATCH_G(G, (k_osb_b64<GG, false, true><<<grid, c.block, 0, s>>>(d, kstep)));
-      } else {
-        PD_DISPATCH_G(G, (k_osb_b64<GG, false, false><<<grid, c.block, 0, s>>>(d, kstep)));
-      }
-      launches++;
-    }
-    return launches;
+    if (d.sc64) return launch_osb64<true>(d, c, G, grid, kstep, A, B, s);
+    return launch_osb64<false>(d, c, G, grid, kstep, A, B, s);
   }
   if (A) {
     PD_DISPATCH_G(G, (k_c_a64<GG><<<grid, c.block, 0, s>>>(d, kstep)));

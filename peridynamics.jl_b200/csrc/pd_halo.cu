@@ -44,6 +44,8 @@ static HaloKind halo_kind(const pd_handle* h, int kind) {
   const DevBody& d = h->d;
   if (kind == 0) {
     add(d.cur, 8, 0);
+  } else if (kind == 2) {
+    add(d.mf, 6, 0);  // the row size holds before pd_esc_init allocates the array
   } else if (h->material == PD_MAT_OSB) {
     if (h->precision == PD_PREC_FP64) {
       add(d.coef64, 8, 0);
@@ -133,7 +135,7 @@ extern "C" pd_status pd_set_stream(pd_handle* h, void* stream) {
 
 extern "C" pd_status pd_halo_row_bytes(pd_handle* h, int32_t kind, int64_t* bytes) {
   if (!h || !bytes) return pd_fail(PD_ERR_ARG, "NULL argument");
-  if (kind != 0 && kind != 1) return pd_fail(PD_ERR_ARG, "kind must be 0 or 1");
+  if (kind < 0 || kind > 2) return pd_fail(PD_ERR_ARG, "kind must be 0, 1 or 2");
   *bytes = 4 * (int64_t)halo_kind(h, kind).row_words;
   return PD_OK;
 }
@@ -141,11 +143,12 @@ extern "C" pd_status pd_halo_row_bytes(pd_handle* h, int32_t kind, int64_t* byte
 extern "C" pd_status pd_halo_pack(pd_handle* h, int32_t kind, const int32_t* d_rows, int64_t n_rows,
                                   void* d_buf) {
   if (!h) return pd_fail(PD_ERR_ARG, "handle is NULL");
-  if (kind != 0 && kind != 1) return pd_fail(PD_ERR_ARG, "kind must be 0 or 1");
+  if (kind < 0 || kind > 2) return pd_fail(PD_ERR_ARG, "kind must be 0, 1 or 2");
   if (n_rows < 0 || n_rows > h->n) return pd_fail(PD_ERR_ARG, "n_rows out of range");
   const HaloKind k = halo_kind(h, kind);
   if (n_rows == 0 || k.row_words == 0) return PD_OK;
   if (!d_rows || !d_buf) return pd_fail(PD_ERR_ARG, "NULL device array");
+  if (kind == 2 && !h->d.mf) return pd_fail(PD_ERR_ARG, "no surface correction factors (pd_esc_init)");
   PD_CUDA(cudaSetDevice(h->device));
   k_halo_pack<<<halo_blocks(n_rows * k.row_words), 256, 0, h->stream>>>(
       k, h->n, d_rows, n_rows, static_cast<unsigned*>(d_buf), h->d.ctrl);
@@ -157,11 +160,12 @@ extern "C" pd_status pd_halo_pack(pd_handle* h, int32_t kind, const int32_t* d_r
 extern "C" pd_status pd_halo_unpack(pd_handle* h, int32_t kind, const int32_t* d_rows, int64_t n_rows,
                                     const void* d_buf) {
   if (!h) return pd_fail(PD_ERR_ARG, "handle is NULL");
-  if (kind != 0 && kind != 1) return pd_fail(PD_ERR_ARG, "kind must be 0 or 1");
+  if (kind < 0 || kind > 2) return pd_fail(PD_ERR_ARG, "kind must be 0, 1 or 2");
   if (n_rows < 0 || n_rows > h->n) return pd_fail(PD_ERR_ARG, "n_rows out of range");
   const HaloKind k = halo_kind(h, kind);
   if (n_rows == 0 || k.row_words == 0) return PD_OK;
   if (!d_rows || !d_buf) return pd_fail(PD_ERR_ARG, "NULL device array");
+  if (kind == 2 && !h->d.mf) return pd_fail(PD_ERR_ARG, "no surface correction factors (pd_esc_init)");
   PD_CUDA(cudaSetDevice(h->device));
   k_halo_unpack<<<halo_blocks(n_rows * k.row_words), 256, 0, h->stream>>>(
       k, h->n, d_rows, n_rows, static_cast<const unsigned*>(d_buf), h->d.ctrl);

@@ -8,6 +8,7 @@ Verlet update run as CUDA kernels; there is no CPU fallback.
 from ._lib import NaNError, PDCudaError, lib, LIB_PATH, EXPORTS
 from .materials import (BBMaterial, OSBMaterial, CMaterial, SaintVenantKirchhoff, NeoHooke,
                         NeoHookePenalty, ZEMSilling, CriticalStretch, NoCorrection,
+                        EnergySurfaceCorrection,
                         const_one_kernel, linear_kernel, cubic_b_spline_kernel,
                         point_parameters, PointParameters)
 from .body import (Body, point_set, material, failure_permit, no_failure, velocity_bc,

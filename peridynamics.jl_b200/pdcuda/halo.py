@@ -30,7 +30,12 @@ import numpy as np
 
 from . import _lib as L
 from .body import Body, Condition
-from .materials import BBMaterial
+from .materials import BBMaterial, EnergySurfaceCorrection
+
+
+def torch_int32():
+    import torch
+    return torch.int32
 
 
 def distribute_equally(n_elems, n_chunks):
@@ -209,11 +214,11 @@ class Partition:
     # -- halo data on the device -----------------------------------------------------------
     def alloc_buffers(self, kinds, torch_device):
         import torch
-        self.send_bufs, self.recv_bufs = {}, {}
+        self.send_bufs, self.recv_bufs, self.row_bytes = {}, {}, {}
         for kind in kinds:
             rb = C.c_int64()
             L.check(L.lib().pd_halo_row_bytes(self.dev.h, kind, C.byref(rb)), "pd_halo_row_bytes")
-            rb = rb.value
+            rb = self.row_bytes[kind] = rb.value
             self.send_bufs[kind] = {
                 dst: (torch.from_numpy(rows).to(torch_device),
                       torch.empty(len(rows) * rb, dtype=torch.uint8, device=torch_device))
@@ -224,14 +229,21 @@ class Partition:
         self.recv_rows = {src: torch.from_numpy(rows).to(torch_device)
                           for src, (rows, _) in self.recv.items()}
 
+    def _check_buffer(self, kind, rows, buf):
+        # the kernels write rows x row bytes: the buffer must hold exactly that
+        if buf.numel() != len(rows) * self.row_bytes[kind] or rows.dtype != torch_int32():
+            raise ValueError("halo buffer does not match its row list")
+
     def pack(self, kind):
         for dst, (rows, buf) in self.send_bufs[kind].items():
+            self._check_buffer(kind, rows, buf)
             L.check(L.lib().pd_halo_pack(self.dev.h, kind, C.c_void_p(rows.data_ptr()), len(rows),
                                          C.c_void_p(buf.data_ptr())), "pd_halo_pack")
 
     def unpack(self, kind):
         for src, buf in self.recv_bufs[kind].items():
             rows = self.recv_rows[src]
+            self._check_buffer(kind, rows, buf)
             L.check(L.lib().pd_halo_unpack(self.dev.h, kind, C.c_void_p(rows.data_ptr()), len(rows),
                                            C.c_void_p(buf.data_ptr())), "pd_halo_unpack")
 
@@ -305,9 +317,20 @@ class PartitionedBody:
             L.check(L.lib().pd_set_stream(p.dev.h, C.c_void_p(self.stream.cuda_stream)), "pd_set_stream")
         self.state_based = not isinstance(parts[0].body.mat, BBMaterial)
         self.kinds = (0, 1) if self.state_based else (0,)
+        esc = isinstance(getattr(parts[0].body.mat, "correction", None), EnergySurfaceCorrection)
         for p in parts:
-            p.alloc_buffers(self.kinds, self.torch_device)
+            p.alloc_buffers(self.kinds + ((2,) if esc else ()), self.torch_device)
         self.exchange = HaloExchange(parts, dist)
+        if esc:
+            # initialize! of the correction (bond_system_corrections.jl:86-94): the owners'
+            # multiplication factors reach the halo rows before the bond factors are formed
+            import torch
+            with torch.cuda.stream(self.stream):
+                for p in parts:
+                    L.check(L.lib().pd_esc_init(p.dev.h, 1), "pd_esc_init")
+                self.exchange(2)
+                for p in parts:
+                    L.check(L.lib().pd_esc_init(p.dev.h, 2), "pd_esc_init")
 
     # -- reductions over ranks (MPI.Allreduce of the reference) -----------------------------
     def _reduce(self, x, op):

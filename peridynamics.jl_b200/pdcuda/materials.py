@@ -69,10 +69,6 @@ class ZEMSilling:
     Cs: float = 0.5
 
 
-class NoCorrection:
-    """No surface correction (bond_system_corrections.jl:11-45): factor 1."""
-
-
 # ----------------------------------------------------------------------------------------
 # material types
 # ----------------------------------------------------------------------------------------
@@ -92,28 +88,56 @@ class AbstractMaterial:
                              "are available on the device") from e
 
 
-class BBMaterial(AbstractMaterial):
-    """Bond-based peridynamics (bond_based.jl:74-84); nu is fixed to 1/4."""
-    material_id = L.MAT_BB
-
-    def __init__(self, dmgmodel=None):
-        self.dmgmodel = dmgmodel or CriticalStretch()
-        self.kernel = const_one_kernel
+class NoCorrection:
+    """No surface correction (bond_system_corrections.jl:1-10): every bond factor is 1."""
 
     def __repr__(self):
-        return "BBMaterial{NoCorrection}()"
+        return "NoCorrection"
+
+
+class EnergySurfaceCorrection:
+    """The energy based surface correction of Le and Bobaru (2018)
+    (bond_system_corrections.jl:50-64): per-bond factors from the strain energy of every
+    point under uniform stretches, computed when the body is set up on the device."""
+
+    def __repr__(self):
+        return "EnergySurfaceCorrection"
+
+
+def _correction(c):
+    if c is None or c is NoCorrection or isinstance(c, NoCorrection):
+        return NoCorrection()
+    if c is EnergySurfaceCorrection or isinstance(c, EnergySurfaceCorrection):
+        return EnergySurfaceCorrection()
+    raise ValueError("correction must be NoCorrection or EnergySurfaceCorrection")
+
+
+class BBMaterial(AbstractMaterial):
+    """Bond-based peridynamics (bond_based.jl:74-84); nu is fixed to 1/4. correction: the
+    material's type parameter of the reference (BBMaterial{EnergySurfaceCorrection}())."""
+    material_id = L.MAT_BB
+
+    def __init__(self, dmgmodel=None, correction=None):
+        self.dmgmodel = dmgmodel or CriticalStretch()
+        self.kernel = const_one_kernel
+        self.correction = _correction(correction)
+
+    def __repr__(self):
+        return f"BBMaterial{{{self.correction!r}}}()"
 
 
 class OSBMaterial(AbstractMaterial):
-    """Ordinary state-based peridynamics (ordinary_state_based.jl:82-94)."""
+    """Ordinary state-based peridynamics (ordinary_state_based.jl:82-94); correction as for
+    BBMaterial."""
     material_id = L.MAT_OSB
 
-    def __init__(self, kernel=linear_kernel, dmgmodel=None):
+    def __init__(self, kernel=linear_kernel, dmgmodel=None, correction=None):
         self.kernel = kernel
         self.dmgmodel = dmgmodel or CriticalStretch()
+        self.correction = _correction(correction)
 
     def __repr__(self):
-        return "OSBMaterial{NoCorrection}(dmgmodel=CriticalStretch())"
+        return f"OSBMaterial{{{self.correction!r}}}(dmgmodel=CriticalStretch())"
 
 
 class CMaterial(AbstractMaterial):

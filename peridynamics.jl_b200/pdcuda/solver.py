@@ -15,7 +15,7 @@ import numpy as np
 
 from . import _lib as L
 from .body import Body
-from .materials import CMaterial
+from .materials import CMaterial, EnergySurfaceCorrection
 
 _FIELDS = {
     "position": (L.F_POSITION, 3, np.float64), "displacement": (L.F_DISPLACEMENT, 3, np.float64),
@@ -152,6 +152,11 @@ class DeviceBody:
                     if not math.isnan(val):
                         v[i, ic.dim] = val
             self.set_state(velocity=v)
+        # initialize! of EnergySurfaceCorrection (bond_system_corrections.jl:78-94) after the
+        # pre-cracks; a partition computes it with its neighbours (pdcuda.halo)
+        self.esc = isinstance(getattr(mat, "correction", None), EnergySurfaceCorrection)
+        if self.esc and owned is None:
+            L.check(lib.pd_esc_init(self.h, 0), "pd_esc_init")
         self._setup_bcs()
         self.param_dt = param_dt
 
@@ -309,6 +314,13 @@ class DeviceBody:
         c = C.c_int64()
         L.check(L.lib().pd_launch_count(self.h, C.byref(c)))
         return c.value
+
+    def surface_correction(self):
+        """(mfactor (n, 3), scfactor (n_bonds, CSR order)) of EnergySurfaceCorrection."""
+        mf = np.empty((self.n, 3))
+        sc = np.empty(self.info()[1])
+        L.check(L.lib().pd_esc_get(self.h, L.ptr(mf), L.ptr(sc)), "pd_esc_get")
+        return mf, sc
 
     def break_random_pairs(self, fraction, seed):
         L.check(L.lib().pd_break_random_pairs(self.h, float(fraction), int(seed)), "pd_break_random_pairs")

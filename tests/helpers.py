@@ -32,6 +32,8 @@ def oracle_body(body, cmodel=None):
         if not filt:
             ob.break_bonds(body.point_sets[a], body.point_sets[b])
             ob.calc_damage()
+    if isinstance(getattr(mat, "correction", None), pd.EnergySurfaceCorrection):
+        ob.init_surface_correction()   # initialize! after the pre-cracks
     for ic in body.single_dim_ics:
         ob.v[body.point_sets[ic.point_set], ic.dim] = ic.fun
     for ic in body.posdep_single_dim_ics:

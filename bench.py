@@ -74,12 +74,16 @@ def load_peaks():
         return 6650.0, "fallback"
 
 
-def make_body(cfg, jitter_seed=None):
+def make_body(cfg, jitter_seed=None, correction=None):
     import pdcuda as pd
     nx, ny, nz, dx, mat, frac, vbc = CONFIGS[cfg]
     lx, ly, lz = nx * dx, ny * dx, nz * dx
     pos, vol = pd.uniform_box(lx, ly, lz, dx)
-    material = {"OSB": pd.OSBMaterial, "BB": pd.BBMaterial,
+    corr = pd.EnergySurfaceCorrection if correction == "energy" else None
+    if corr is not None and mat == "C":
+        raise ValueError("the surface correction is available for BB and OSB")
+    material = {"OSB": lambda: pd.OSBMaterial(correction=corr),
+                "BB": lambda: pd.BBMaterial(correction=corr),
                 "C": lambda: pd.CMaterial(model=pd.NeoHooke())}[mat]()
     body = pd.Body(material, pos, vol)
     kw = dict(horizon=3.015 * dx, rho=2700.0, E=70e9, Gc=100.0)
@@ -328,10 +332,12 @@ def oracle_sample(cfg, threads):
     return b, dt, (sx, sy, sz)
 
 
-def cpu_baseline(cfg, threads, budget_s=15.0):
+def cpu_baseline(cfg, threads, budget_s=15.0, correction="none"):
     """bond-updates/s of the oracle sample over whole Velocity Verlet steps (a run of about
     budget_s seconds)."""
     b, dt, (sx, sy, sz) = oracle_sample(cfg, threads)
+    if correction == "energy":
+        b.init_surface_correction()
     steps, t0 = 0, time.perf_counter()
     while True:
         b.run_vv(steps + 1, 1, dt)
@@ -715,6 +721,8 @@ def main():
     ap.add_argument("--fp64-steps", type=int, default=-1, help="steps of the FP64 comparison (0 = skip)")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--graph", type=int, default=0)
+    ap.add_argument("--correction", default="none", choices=["none", "energy"],
+                    help="BB / OSB with EnergySurfaceCorrection")
     ap.add_argument("--halo", action="store_true",
                     help="one body in partitions with halo exchange (one per rank) instead of replicas")
     ap.add_argument("--halo-parts", type=int, default=1,
@@ -807,10 +815,12 @@ def main():
         return reduce_max(x, dist, device=f"cuda:{local}")
 
     def build(prec):
-        body, frac_ = make_body(args.config)
+        body, frac_ = make_body(args.config, correction=args.correction)
         dev = pd.DeviceBody(body, precision=prec, device=local)
         if frac_ > 0:
             dev.break_random_pairs(frac_, 0x5EED + rank)
+            if args.correction == "energy":  # the correction sees the initial damage
+                pd.lib().pd_esc_init(dev.h, 0)
         dt = dev.stable_timestep(0.7)
         dev.force(0.0, dt)
         return body, dev, dt
@@ -848,7 +858,8 @@ def main():
         pt_bytes = {"phase_a": 32 + 8 + 16 + 4 + 4, "phase_b": 32 + 8 + 16 + 12 + 4}[dom]
     else:
         pt_bytes = {"phase_a": 64 + 8 + 32 + 4 + 4, "phase_b": 64 + 8 + 32 + 24 + 4}[dom]
-    alg_bytes = n_bonds * B_BOND[prec] + n_pts * pt_bytes
+    b_bond = B_BOND[prec] + (({"fp32": 4.0, "fp64": 8.0}[prec]) if args.correction == "energy" else 0.0)
+    alg_bytes = n_bonds * b_bond + n_pts * pt_bytes
     achieved = alg_bytes / (dom_ms / 1e3) / 1e9
     # DRAM traffic per launch from the committed ncu capture, scaled by the bond count
     traffic = None
@@ -860,7 +871,7 @@ def main():
             traffic = tb[key] * n_bonds
     except Exception:
         traffic = None
-    step_bytes = n_bonds * B_BOND[prec] + n_pts * (B_POINT[prec] + B_POINT_EXTRA[mat])
+    step_bytes = n_bonds * b_bond + n_pts * (B_POINT[prec] + B_POINT_EXTRA[mat])
     step_ms = ms_max / args.steps
     step_achieved = step_bytes / (step_ms / 1e3) / 1e9
 
@@ -899,7 +910,7 @@ def main():
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        cpu = cpu_baseline(args.config, os.cpu_count() or 1)
+        cpu = cpu_baseline(args.config, os.cpu_count() or 1, correction=args.correction)
     dev.close()
     jfnk = None
     if rank == 0 and world == 1 and args.jfnk_increments > 0:
@@ -912,7 +923,8 @@ def main():
             "scaling": "weak", "vs_baseline": None, "dtype": "f32" if prec == "fp32" else "f64",
             "data": "synthetic",
             "config": {"workload": f"{args.config}: {mat} {nx}x{ny}x{nz} points, dx={dx}, "
-                                   f"horizon 3.015dx, {frac:.0%} pairs broken, VV step",
+                                   f"horizon 3.015dx, {frac:.0%} pairs broken, VV step"
+                                   + (", EnergySurfaceCorrection" if args.correction == "energy" else ""),
                        "points": n_pts, "bonds": n_bonds, "precision": prec,
                        "mapping": dict(zip(("group", "block", "pipe"), dev_mapping)),
                        "symmetric_pairs": bool(sym),

@@ -106,6 +106,7 @@ __global__ void PD_LB k_bb32(DevBody d, int kstep) {
         const long long b = sbase + (long long)r * 32 + lane;
         const int j = __ldg(d.nbr + b);
         const float4 g = __ldg(d.geo + b);
+        const float bet = ESC ? __ldg(d.sc32 + b) : 1.f;  // loaded with the bond record
         const float4 hj = __ldg(d.uhi + j), lj = __ldg(d.ulo + j);
         BondF B;
         bond32(g, hi, lo, hj, lj, B);
@@ -114,7 +115,7 @@ __global__ void PD_LB k_bb32(DevBody d, int kstep) {
           float bc = bci;
           if (MULTI) bc = 0.5f * (bci + d.params[d.meta[j] & META_PID_MASK].bcf);
           float sc = bc * B.eps * hj.w * B.rl;
-          if (ESC) sc *= __ldg(d.sc32 + b);
+          if (ESC) sc *= bet;
           bx.add(sc * B.ex); by.add(sc * B.ey); bz.add(sc * B.ez);
         }
       }
@@ -150,17 +151,23 @@ __global__ void PD_LB_A k_osb_a32(DevBody d, int kstep) {
     const long long b0 = sbase + lane;
     int jn = 0;
     float4 gn = make_float4(0.f, 0.f, 0.f, 0.f);
-    if (rows > 0 && gl < cnt) { jn = __ldg(d.nbr + b0); gn = __ldg(d.geo + b0); }
+    float sn = 1.f;
+    if (rows > 0 && gl < cnt) {
+      jn = __ldg(d.nbr + b0); gn = __ldg(d.geo + b0);
+      if (ESC) sn = __ldg(d.sc32 + b0);
+    }
     for (int r = 0; r < rows; r++) {
       const long long wi = (sbase >> 5) + r;
       const unsigned word = d.bits[wi];
       const int k = r * G + gl;
       const int j = jn;
       const float4 g = gn;
+      const float bet = sn;
       if (r + 1 < rows && k + G < cnt) {
         const long long b1 = b0 + (long long)(r + 1) * 32;
         jn = __ldg(d.nbr + b1);
         gn = __ldg(d.geo + b1);
+        if (ESC) sn = __ldg(d.sc32 + b1);
       }
       bool act = false;
       if (k < cnt) {
@@ -170,7 +177,7 @@ __global__ void PD_LB_A k_osb_a32(DevBody d, int kstep) {
         act = ((word >> lane) & 1u) && !fails32(B, epsc);
         if (act) {
           float om = omega_r(d.kernel, delta, B.L, B.rL) * hj.w;
-          if (ESC) om *= __ldg(d.sc32 + b0 + (long long)r * 32);
+          if (ESC) om *= bet;
           m.add(om * (B.gx * B.gx + B.gy * B.gy + B.gz * B.gz));
           th.add(om * B.L * B.e);
         }
@@ -228,14 +235,19 @@ __global__ void PD_LB k_osb_b32(DevBody d, int kstep) {
     const long long b0 = sbase + lane;
     int jn = 0;
     float4 gn = make_float4(0.f, 0.f, 0.f, 0.f);
+    float sn = 1.f;
     unsigned wn = 0;
     if (rows > 0) {
       wn = __ldg(wrow);
-      if (gl < cnt) { jn = __ldg(d.nbr + b0); gn = __ldg(d.geo + b0); }
+      if (gl < cnt) {
+        jn = __ldg(d.nbr + b0); gn = __ldg(d.geo + b0);
+        if (ESC) sn = __ldg(d.sc32 + b0);
+      }
     }
     for (int r = 0; r < rows; r++) {
       const int j = jn;
       const float4 g = gn;
+      const float bet = sn;
       const unsigned word = wn;
       const int k = r * G + gl;
       if (r + 1 < rows) {
@@ -244,6 +256,7 @@ __global__ void PD_LB k_osb_b32(DevBody d, int kstep) {
           const long long b1 = b0 + (long long)(r + 1) * 32;
           jn = __ldg(d.nbr + b1);
           gn = __ldg(d.geo + b1);
+          if (ESC) sn = __ldg(d.sc32 + b1);
         }
       }
       if (k >= cnt) continue;
@@ -263,7 +276,7 @@ __global__ void PD_LB k_osb_b32(DevBody d, int kstep) {
       const float si = osb_s32<MULTI>(ci, mi, Pi, *Pj, oi, B.L, B.e);
       const float sj = osb_s32<MULTI>(cj, mj, *Pj, Pi, oj, B.L, B.e);
       float f = (si + sj) * hj.w * B.rl;
-      if (ESC) f *= __ldg(d.sc32 + b);
+      if (ESC) f *= bet;
       bx.add(f * B.ex); by.add(f * B.ey); bz.add(f * B.ez);
     }
     if (G > 1) { group_reduce<G>(bx); group_reduce<G>(by); group_reduce<G>(bz); }
@@ -290,7 +303,7 @@ __global__ void PD_LB k_osb_b32(DevBody d, int kstep) {
 #ifndef PD_MINB_UB
 #define PD_MINB_UB 4
 #endif
-template <int G>
+template <int G, bool ESC>
 __global__ void __launch_bounds__(256, PD_MINB_UA) k_osb_a32u(DevBody d, int kstep) {
   if (d.ctrl->err) return;
   PD_SLICE_LOOP(G) {
@@ -311,8 +324,9 @@ __global__ void __launch_bounds__(256, PD_MINB_UA) k_osb_a32u(DevBody d, int kst
       const long long b0 = sbase + (long long)r * 32 + lane;
       int j0 = self, j1 = self;
       float4 g0 = make_float4(0.f, 0.f, 0.f, 1.f), g1 = g0;
-      if (h0) { j0 = __ldg(d.nbr + b0); g0 = __ldg(d.geo + b0); }
-      if (h1) { j1 = __ldg(d.nbr + b0 + 32); g1 = __ldg(d.geo + b0 + 32); }
+      float s0 = 1.f, s1 = 1.f;
+      if (h0) { j0 = __ldg(d.nbr + b0); g0 = __ldg(d.geo + b0); if (ESC) s0 = __ldg(d.sc32 + b0); }
+      if (h1) { j1 = __ldg(d.nbr + b0 + 32); g1 = __ldg(d.geo + b0 + 32); if (ESC) s1 = __ldg(d.sc32 + b0 + 32); }
       const float4 hj0 = __ldg(d.uhi + j0), lj0 = __ldg(d.ulo + j0);
       const float4 hj1 = __ldg(d.uhi + j1), lj1 = __ldg(d.ulo + j1);
       bool act0 = false, act1 = false;
@@ -324,7 +338,8 @@ __global__ void __launch_bounds__(256, PD_MINB_UA) k_osb_a32u(DevBody d, int kst
         bond32(u ? g1 : g0, hi, lo, hj, u ? lj1 : lj0, B);
         const bool act = (((u ? w1 : w0) >> lane) & 1u) && !fails32(B, epsc);
         if (act) {
-          const float om = omega_r(d.kernel, delta, B.L, B.rL) * hj.w;
+          float om = omega_r(d.kernel, delta, B.L, B.rL) * hj.w;
+          if (ESC) om *= u ? s1 : s0;
           m.add(om * (B.gx * B.gx + B.gy * B.gy + B.gz * B.gz));
           th.add(om * B.L * B.e);
         }
@@ -350,7 +365,7 @@ __global__ void __launch_bounds__(256, PD_MINB_UA) k_osb_a32u(DevBody d, int kst
   }
 }
 
-template <int G, bool MULTI>
+template <int G, bool MULTI, bool ESC>
 __global__ void __launch_bounds__(256, PD_MINB_UB) k_osb_b32u(DevBody d, int kstep) {
   if (d.ctrl->err) return;
   PD_SLICE_LOOP(G) {
@@ -371,8 +386,9 @@ __global__ void __launch_bounds__(256, PD_MINB_UB) k_osb_b32u(DevBody d, int kst
       bool h0 = k0 < cnt, h1 = two && k0 + G < cnt;
       int j0 = self, j1 = self;
       float4 g0 = make_float4(0.f, 0.f, 0.f, 1.f), g1 = g0;
-      if (h0) { j0 = __ldg(d.nbr + b0); g0 = __ldg(d.geo + b0); }
-      if (h1) { j1 = __ldg(d.nbr + b0 + 32); g1 = __ldg(d.geo + b0 + 32); }
+      float s0 = 1.f, s1 = 1.f;
+      if (h0) { j0 = __ldg(d.nbr + b0); g0 = __ldg(d.geo + b0); if (ESC) s0 = __ldg(d.sc32 + b0); }
+      if (h1) { j1 = __ldg(d.nbr + b0 + 32); g1 = __ldg(d.geo + b0 + 32); if (ESC) s1 = __ldg(d.sc32 + b0 + 32); }
       const bool ai0 = (w0 >> lane) & 1u, ai1 = (w1 >> lane) & 1u;
       const bool aj0 = h0 && (d.sym ? ai0 : bond_bit(d.bits, rev_slot(d, b0, j0)));
       const bool aj1 = h1 && (d.sym ? ai1 : bond_bit(d.bits, rev_slot(d, b0 + 32, j1)));
@@ -399,7 +415,8 @@ __global__ void __launch_bounds__(256, PD_MINB_UB) k_osb_b32u(DevBody d, int kst
         const float oj = aj ? omega_r(d.kernel, Pj->deltaf, B.L, B.rL) : 0.f;
         const float si = osb_s32<MULTI>(ci, mi, Pi, *Pj, oi, B.L, B.e);
         const float sj = osb_s32<MULTI>(cj, mj, *Pj, Pi, oj, B.L, B.e);
-        const float f = (si + sj) * hj.w * B.rl;
+        float f = (si + sj) * hj.w * B.rl;
+        if (ESC) f *= u ? s1 : s0;
         bx.add(f * B.ex); by.add(f * B.ey); bz.add(f * B.ez);
       }
     }
@@ -667,6 +684,30 @@ static int grid_for32(long long nslices, int block) {
   return (int)blocks;
 }
 
+// OSB: the two-row kernels for pipe 4, else the one-row kernels (also for pipes 1-3 when the
+// surface correction is on: the TMA-staged stream carries no bond factors)
+template <bool ESC>
+static int launch_osb32(const DevBody& d, const LaunchCfg& c, int G, int grid, int kstep, bool A,
+                        bool B, cudaStream_t s) {
+  int launches = 0;
+  if (c.pipe == 4) {
+    if (A) { PD_DISPATCH_G(G, (k_osb_a32u<GG, ESC><<<grid, c.block, 0, s>>>(d, kstep))); launches++; }
+    if (B) {
+      if (d.multi) { PD_DISPATCH_G(G, (k_osb_b32u<GG, true, ESC><<<grid, c.block, 0, s>>>(d, kstep))); }
+      else { PD_DISPATCH_G(G, (k_osb_b32u<GG, false, ESC><<<grid, c.block, 0, s>>>(d, kstep))); }
+      launches++;
+    }
+    return launches;
+  }
+  if (A) { PD_DISPATCH_G(G, (k_osb_a32<GG, ESC><<<grid, c.block, 0, s>>>(d, kstep))); launches++; }
+  if (B) {
+    if (d.multi) { PD_DISPATCH_G(G, (k_osb_b32<GG, true, ESC><<<grid, c.block, 0, s>>>(d, kstep))); }
+    else { PD_DISPATCH_G(G, (k_osb_b32<GG, false, ESC><<<grid, c.block, 0, s>>>(d, kstep))); }
+    launches++;
+  }
+  return launches;
+}
+
 int launch_force32(const DevBody& d, const LaunchCfg& c, int kstep, int phase, cudaStream_t s) {
   const int G = d.lg;
   const int grid = grid_for32(d.nslices, c.block);
@@ -684,32 +725,9 @@ int launch_force32(const DevBody& d, const LaunchCfg& c, int kstep, int phase, c
     }
     return 1;
   }
-  if (d.material == MAT_OSB && d.sc32) {  // surface correction: the one-row kernels
-    if (A) { PD_DISPATCH_G(G, (k_osb_a32<GG, true><<<grid, c.block, 0, s>>>(d, kstep))); launches++; }
-    if (B) {
-      if (d.multi) { PD_DISPATCH_G(G, (k_osb_b32<GG, true, true><<<grid, c.block, 0, s>>>(d, kstep))); }
-      else { PD_DISPATCH_G(G, (k_osb_b32<GG, false, true><<<grid, c.block, 0, s>>>(d, kstep))); }
-      launches++;
-    }
-    return launches;
-  }
-  if (d.material == MAT_OSB && c.pipe == 4) {
-    if (A) { PD_DISPATCH_G(G, (k_osb_a32u<GG><<<grid, c.block, 0, s>>>(d, kstep))); launches++; }
-    if (B) {
-      if (d.multi) { PD_DISPATCH_G(G, (k_osb_b32u<GG, true><<<grid, c.block, 0, s>>>(d, kstep))); }
-      else { PD_DISPATCH_G(G, (k_osb_b32u<GG, false><<<grid, c.block, 0, s>>>(d, kstep))); }
-      launches++;
-    }
-    return launches;
-  }
   if (d.material == MAT_OSB) {
-    if (A) { PD_DISPATCH_G(G, (k_osb_a32<GG, false><<<grid, c.block, 0, s>>>(d, kstep))); launches++; }
-    if (B) {
-      if (d.multi) { PD_DISPATCH_G(G, (k_osb_b32<GG, true, false><<<grid, c.block, 0, s>>>(d, kstep))); }
-      else { PD_DISPATCH_G(G, (k_osb_b32<GG, false, false><<<grid, c.block, 0, s>>>(d, kstep))); }
-      launches++;
-    }
-    return launches;
+    if (d.sc32) return launch_osb32<true>(d, c, G, grid, kstep, A, B, s);
+    return launch_osb32<false>(d, c, G, grid, kstep, A, B, s);
   }
   if (A) { PD_DISPATCH_G(G, (k_c_a32<GG><<<grid, c.block, 0, s>>>(d, kstep))); launches++; }
   if (B) { PD_DISPATCH_G(G, (k_c_b32<GG><<<grid, c.block, 0, s>>>(d, kstep))); launches++; }

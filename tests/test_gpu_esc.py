@@ -131,3 +131,19 @@ def test_partitions_with_correction(prec, mapping):
     assert np.array_equal(pb.field("bond_active"), dev.field("bond_active"))
     pb.close()
     dev.close()
+
+
+def test_two_row_kernels_equal_one_row_with_correction():
+    """pipe 4 (two rows of gathers in flight) and pipe 0 add the same terms in the same order."""
+    body = plate_body(pd.OSBMaterial(correction=ESC), nx=24, ny=12, nz=3, nu=0.25)
+    res = []
+    for pipe in (0, 4):
+        dev = pd.DeviceBody(body, precision="fp32")
+        dev.set_mapping(1)
+        dev.set_pipeline(pipe)
+        dt = dev.stable_timestep(0.7)
+        dev.force(0.0, dt)
+        dev.run(1, 60, dt)
+        res.append((dev.field("displacement"), dev.field("bond_active")))
+        dev.close()
+    assert np.array_equal(res[0][0], res[1][0]) and np.array_equal(res[0][1], res[1][1])

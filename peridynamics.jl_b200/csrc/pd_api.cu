@@ -1115,8 +1115,19 @@ extern "C" pd_status pd_autotune(pd_handle* h, int32_t* group_out, int32_t* bloc
   cudaEvent_t e0, e1;
   PD_CUDA(cudaEventCreate(&e0));
   PD_CUDA(cudaEventCreate(&e1));
-  float best = INFINITY;
-  LaunchCfg bestc = keep;
+  struct Cand { float ms; LaunchCfg c; };
+  std::vector<Cand> cands;
+  // five evaluations of the current configuration after one warm-up
+  auto time_cfg = [&](float* out) -> pd_status {
+    launch_force(h, 0, 0);
+    cudaEventRecord(e0, h->stream);
+    for (int r = 0; r < 5; r++) launch_force(h, 0, 0);
+    cudaEventRecord(e1, h->stream);
+    cudaError_t e = cudaEventSynchronize(e1);
+    if (e != cudaSuccess) return fail(PD_ERR_CUDA, cudaGetErrorString(e));
+    cudaEventElapsedTime(out, e0, e1);
+    return PD_OK;
+  };
   const int groups[] = {1, 4, 32};
   const int blocks[] = {128, 256};
   // force evaluations are idempotent at fixed positions: bonds that broke stay broken and
@@ -1135,19 +1146,31 @@ extern "C" pd_status pd_autotune(pd_handle* h, int32_t* group_out, int32_t* bloc
       const int B = v < 4 ? blocks[v % 2] : 128;
       h->cfg.group = G; h->cfg.block = B; h->cfg.exact = false;
       h->cfg.pipe = v < 2 ? 0 : v < 4 ? 4 : v - 3;
-      launch_force(h, 0, 0);
-      cudaEventRecord(e0, h->stream);
-      for (int r = 0; r < 5; r++) launch_force(h, 0, 0);
-      cudaEventRecord(e1, h->stream);
-      cudaError_t e = cudaEventSynchronize(e1);
-      if (e != cudaSuccess) { cudaEventDestroy(e0); cudaEventDestroy(e1); return fail(PD_ERR_CUDA, cudaGetErrorString(e)); }
       float ms;
-      cudaEventElapsedTime(&ms, e0, e1);
-      if (ms < best) { best = ms; bestc = h->cfg; }
+      pd_status ts = time_cfg(&ms);
+      if (ts != PD_OK) { cudaEventDestroy(e0); cudaEventDestroy(e1); return ts; }
+      cands.push_back({ms, h->cfg});
     }
   }
+  // the three fastest are timed twice more, interleaved, and keep their best time: one window
+  // of five evaluations moves with the clocks of a power-capped GPU
+  std::sort(cands.begin(), cands.end(), [](const Cand& a, const Cand& b) { return a.ms < b.ms; });
+  if (cands.size() > 3) cands.resize(3);
+  for (int round = 0; round < 2 && cands.size() > 1; round++)
+    for (auto& c : cands) {
+      if (relayout(h, c.c.group) != PD_OK) { cudaGetLastError(); continue; }
+      h->cfg = c.c;
+      float ms;
+      pd_status ts = time_cfg(&ms);
+      if (ts != PD_OK) { cudaEventDestroy(e0); cudaEventDestroy(e1); return ts; }
+      c.ms = std::min(c.ms, ms);
+    }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
+  LaunchCfg bestc = keep;
+  float best = INFINITY;
+  for (const auto& c : cands)
+    if (c.ms < best) { best = c.ms; bestc = c.c; }
   PD_TRY(relayout(h, bestc.group));
   h->cfg = bestc;
   destroy_graph(h);

@@ -250,7 +250,7 @@ pd_status pd_set_mapping(pd_handle *h, int32_t group, int32_t block);
 /* How the FP32 force kernels read the bond stream: 0 = direct loads; 1, 2, 3 = chunks of
  * the sliced bond arrays staged in shared memory by TMA bulk copies (4 rows x 3 stages,
  * 4 rows x 4 stages, 8 rows x 3 stages per warp; one lane per point, BB or OSB); 4 = direct
- * loads two rows at a time, all their neighbour gathers in flight together (OSB; results
+ * loads two rows at a time, all their neighbour gathers in flight together (BB, OSB; results
  * identical to 0). pd_autotune times all that apply. */
 pd_status pd_set_pipeline(pd_handle *h, int32_t pipe);
 

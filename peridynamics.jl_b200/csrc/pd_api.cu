@@ -1137,7 +1137,7 @@ extern "C" pd_status pd_autotune(pd_handle* h, int32_t* group_out, int32_t* bloc
     if (st == PD_ERR_OOM) { cudaGetLastError(); continue; }  // no room for a second layout
     if (st != PD_OK) { cudaEventDestroy(e0); cudaEventDestroy(e1); return st; }
     const bool tma = h->precision == PD_PREC_FP32_KAHAN && G == 1 && tma_supported(h->d);
-    const bool two = h->precision == PD_PREC_FP32_KAHAN && h->material == PD_MAT_OSB;
+    const bool two = h->precision == PD_PREC_FP32_KAHAN && h->material != PD_MAT_CMAT;
     // candidates: blocks of 128 / 256 with plain loads, then (FP32 OSB) the two-row kernels,
     // then (one lane per point) the TMA-staged bond stream
     for (int v = 0; v < 7; v++) {
@@ -1266,8 +1266,8 @@ extern "C" pd_status pd_get_mapping(pd_handle* h, int32_t* group, int32_t* block
 extern "C" pd_status pd_set_pipeline(pd_handle* h, int32_t pipe) {
   if (!h) return fail(PD_ERR_ARG, "handle is NULL");
   if (pipe < 0 || pipe > 4) return fail(PD_ERR_ARG, "pipe must be 0 to 4");
-  if (pipe == 4 && (h->precision != PD_PREC_FP32_KAHAN || h->material != PD_MAT_OSB))
-    return fail(PD_ERR_ARG, "the two-row kernels are the FP32 OSB ones");
+  if (pipe == 4 && (h->precision != PD_PREC_FP32_KAHAN || h->material == PD_MAT_CMAT))
+    return fail(PD_ERR_ARG, "the two-row kernels are the FP32 BB and OSB ones");
   if (pipe >= 1 && pipe <= 3 && (h->precision != PD_PREC_FP32_KAHAN || !tma_supported(h->d)))
     return fail(PD_ERR_ARG, "the staged bond stream needs the FP32 path, one lane per point and BB or OSB");
   h->cfg.pipe = pipe;

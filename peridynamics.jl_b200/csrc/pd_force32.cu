@@ -132,6 +132,69 @@ __global__ void PD_LB k_bb32(DevBody d, int kstep) {
   }
 }
 
+// Two-row BB (pipe 4): the bond records and neighbour gathers of rows r and r + 1 are issued
+// before either row is processed (two dependent gathers in flight per lane, as the OSB
+// two-row kernels); each lane adds its bonds in row order, so the sums equal k_bb32's.
+#ifndef PD_MINB_UBB
+#define PD_MINB_UBB 4
+#endif
+template <int G, bool MULTI, bool ESC>
+__global__ void __launch_bounds__(256, PD_MINB_UBB) k_bb32u(DevBody d, int kstep) {
+  if (d.ctrl->err) return;
+  PD_SLICE_LOOP(G) {
+    PD_SLICE_SETUP
+    KSum bx, by, bz;
+    int na = 0;
+    const float4 hi = valid ? d.uhi[i] : make_float4(0.f, 0.f, 0.f, 0.f);
+    const float4 lo = valid ? d.ulo[i] : make_float4(0.f, 0.f, 0.f, 0.f);
+    const DevParam& P = d.params[valid ? (d.meta[i] & META_PID_MASK) : 0];
+    const float epsc = P.epscf, bci = P.bcf;
+    const int self = valid ? (int)i : 0;
+    for (int r = 0; r < rows; r += 2) {
+      const bool two = r + 1 < rows;
+      const long long wi = (sbase >> 5) + r;
+      const unsigned w0 = d.bits[wi], w1 = two ? d.bits[wi + 1] : 0u;
+      const int k0 = r * G + gl;
+      const bool h0 = k0 < cnt, h1 = two && k0 + G < cnt;
+      const long long b0 = sbase + (long long)r * 32 + lane;
+      int j0 = self, j1 = self;
+      float4 g0 = make_float4(0.f, 0.f, 0.f, 1.f), g1 = g0;
+      float s0 = 1.f, s1 = 1.f;
+      if (h0) { j0 = __ldg(d.nbr + b0); g0 = __ldg(d.geo + b0); if (ESC) s0 = __ldg(d.sc32 + b0); }
+      if (h1) { j1 = __ldg(d.nbr + b0 + 32); g1 = __ldg(d.geo + b0 + 32); if (ESC) s1 = __ldg(d.sc32 + b0 + 32); }
+      const float4 hj0 = __ldg(d.uhi + j0), lj0 = __ldg(d.ulo + j0);
+      const float4 hj1 = __ldg(d.uhi + j1), lj1 = __ldg(d.ulo + j1);
+      bool act0 = false, act1 = false;
+#pragma unroll
+      for (int u = 0; u < 2; u++) {
+        if (!(u ? h1 : h0)) continue;
+        const float4 hj = u ? hj1 : hj0;
+        BondF B;
+        bond32(u ? g1 : g0, hi, lo, hj, u ? lj1 : lj0, B);
+        const bool act = (((u ? w1 : w0) >> lane) & 1u) && !fails32(B, epsc);
+        if (act) {
+          float bc = bci;
+          if (MULTI) bc = 0.5f * (bci + d.params[d.meta[u ? j1 : j0] & META_PID_MASK].bcf);
+          float sc = bc * B.eps * hj.w * B.rl;
+          if (ESC) sc *= u ? s1 : s0;
+          bx.add(sc * B.ex); by.add(sc * B.ey); bz.add(sc * B.ez);
+        }
+        if (u) act1 = act; else act0 = act;
+      }
+      na += act0 + act1;
+      commit_row(d.bits, wi, w0, act0, lane);
+      if (two) commit_row(d.bits, wi + 1, w1, act1, lane);
+    }
+    if (G > 1) { group_reduce<G>(bx); group_reduce<G>(by); group_reduce<G>(bz); na = group_sum<G>(na); }
+    if (valid && gl == 0) {
+      const float x = bx.value(), y = by.value(), z = bz.value();
+      d.b32[3 * i] = x; d.b32[3 * i + 1] = y; d.b32[3 * i + 2] = z;
+      d.n_active[i] = na;
+      flag_nan32(d, kstep, x, y, z);
+    }
+  }
+}
+
 // -------------------------------------------------------------------------------------------
 // OSB phase A (ordinary_state_based.jl:107-126, 176-204): failure, weighted volume m,
 // dilatation theta, and c1 = 15 G / m, c2 = theta (3 K / m - c1 / 3) (:135-136)
@@ -684,6 +747,19 @@ static int grid_for32(long long nslices, int block) {
   return (int)blocks;
 }
 
+// BB: the two-row kernel for pipe 4, else the one-row kernel
+template <bool ESC>
+static void launch_bb32(const DevBody& d, const LaunchCfg& c, int G, int grid, int kstep, cudaStream_t s) {
+  if (c.pipe == 4) {
+    if (d.multi) { PD_DISPATCH_G(G, (k_bb32u<GG, true, ESC><<<grid, c.block, 0, s>>>(d, kstep))); }
+    else { PD_DISPATCH_G(G, (k_bb32u<GG, false, ESC><<<grid, c.block, 0, s>>>(d, kstep))); }
+  } else if (d.multi) {
+    PD_DISPATCH_G(G, (k_bb32<GG, true, ESC><<<grid, c.block, 0, s>>>(d, kstep)));
+  } else {
+    PD_DISPATCH_G(G, (k_bb32<GG, false, ESC><<<grid, c.block, 0, s>>>(d, kstep)));
+  }
+}
+
 // OSB: the two-row kernels for pipe 4, else the one-row kernels (also for pipes 1-3 when the
 // surface correction is on: the TMA-staged stream carries no bond factors)
 template <bool ESC>
@@ -715,14 +791,8 @@ int launch_force32(const DevBody& d, const LaunchCfg& c, int kstep, int phase, c
   int launches = 0;
   if (d.material == MAT_BB) {
     if (!A) return 0;
-    if (d.sc32) {
-      if (d.multi) { PD_DISPATCH_G(G, (k_bb32<GG, true, true><<<grid, c.block, 0, s>>>(d, kstep))); }
-      else { PD_DISPATCH_G(G, (k_bb32<GG, false, true><<<grid, c.block, 0, s>>>(d, kstep))); }
-    } else if (d.multi) {
-      PD_DISPATCH_G(G, (k_bb32<GG, true, false><<<grid, c.block, 0, s>>>(d, kstep)));
-    } else {
-      PD_DISPATCH_G(G, (k_bb32<GG, false, false><<<grid, c.block, 0, s>>>(d, kstep)));
-    }
+    if (d.sc32) launch_bb32<true>(d, c, G, grid, kstep, s);
+    else launch_bb32<false>(d, c, G, grid, kstep, s);
     return 1;
   }
   if (d.material == MAT_OSB) {

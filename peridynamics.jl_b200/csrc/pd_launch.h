@@ -10,7 +10,7 @@ struct LaunchCfg {
   int block;  // threads per block
   bool exact; // FP64: one lane per point in the reference's serial summation order
   int pipe;   // FP32: 0 = plain loads, 1-3 = TMA-staged bond stream (pd_force32_tma.cu),
-              // 4 = two rows of neighbour gathers in flight (OSB)
+              // 4 = two rows of neighbour gathers in flight (BB, OSB)
 };
 
 // boundary conditions as the integration kernels see them

@@ -133,9 +133,11 @@ def test_partitions_with_correction(prec, mapping):
     dev.close()
 
 
-def test_two_row_kernels_equal_one_row_with_correction():
+@pytest.mark.parametrize("name", ["BB", "OSB"])
+def test_two_row_kernels_equal_one_row_with_correction(name):
     """pipe 4 (two rows of gathers in flight) and pipe 0 add the same terms in the same order."""
-    body = plate_body(pd.OSBMaterial(correction=ESC), nx=24, ny=12, nz=3, nu=0.25)
+    mat = pd.BBMaterial(correction=ESC) if name == "BB" else pd.OSBMaterial(correction=ESC)
+    body = plate_body(mat, nx=24, ny=12, nz=3, nu=None if name == "BB" else 0.25)
     res = []
     for pipe in (0, 4):
         dev = pd.DeviceBody(body, precision="fp32")

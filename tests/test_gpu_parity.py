@@ -345,3 +345,22 @@ def test_set_state_round_trip(prec):
     with pytest.raises(ValueError):
         dev.field(key, out=np.empty((dev.n, 2)))
     dev.close()
+
+
+@pytest.mark.parametrize("group", [1, 4, 8])
+def test_bb_two_row_kernel_equals_one_row(group):
+    """The two-row BB kernel (pipe 4) adds each lane's bonds in row order: the same bits."""
+    body = plate_body(pd.BBMaterial(), nx=24, ny=12, nz=3)
+    res = []
+    for pipe in (0, 4):
+        dev = pd.DeviceBody(body, precision="fp32")
+        dev.set_mapping(group)
+        dev.set_pipeline(pipe)
+        dt = dev.stable_timestep(0.7)
+        dev.force(0.0, dt)
+        dev.run(1, 80, dt)
+        res.append((dev.field("displacement"), dev.field("bond_active"), dev.field("damage")))
+        dev.close()
+    for a, b in zip(*res):
+        assert np.array_equal(a, b)
+

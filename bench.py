@@ -890,6 +890,9 @@ def main():
         fp64 = n_bonds * f64_steps * world / (t64 / 1e3)
         d64.close()
         _, dev, dt = build(prec)
+        # the tuned mapping of the timed run, so that e2e runs the same kernels
+        dev.set_mapping(dev_mapping[0], dev_mapping[1])
+        dev.set_pipeline(dev_mapping[2])
         dev.set_graph(args.graph)
 
     # end to end through the public API with host buffers: upload the state, run, read back

@@ -48,7 +48,8 @@ DR_STRAIN = 5e-5
 # algorithmic bytes per point of the damping and velocity-update kernels of one relaxation step
 # (damping: u, v_half, b_int, b_int_old, v_half_old, Lambda; update: Lambda, b_int, b_ext,
 # v_half_old read, v_half, v, v_half_old, b_int_old written)
-B_DR_POINT = {"fp64": 328.0, "fp32": 304.0}
+# (FP64: 128 + 176 B; FP32: b_int is 12 B, 116 + 164 B)
+B_DR_POINT = {"fp64": 304.0, "fp32": 280.0}
 # algorithmic bytes (FP32-compensated form): per directed bond nbr 4 + xi 12 + L 4 + 1/8 bit;
 # per point 140 (u, v FP64 read+write, own u, b_ext/BC, parameter id, damage) + 8 for OSB
 # (m, theta) + 72 for CMat (F, P K^-1)

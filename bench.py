@@ -193,7 +193,7 @@ def run_precision_study(args, local):
         dev.force(0.0, dt)
         t0 = time.perf_counter()
         dev.run(1, steps, dt)
-        out[prec] = {"s": time.perf_counter() - t0, "dt": dt,
+        out[prec] = {"s": time.perf_counter() - t0, "dt": dt, "near": dev.near_critical(1e-12),
                      "u": dev.field("displacement"), "v": dev.field("velocity"),
                      "damage": dev.field("damage"), "bonds": dev.field("bond_active"),
                      "mapping": dev.mapping()}
@@ -213,7 +213,8 @@ def run_precision_study(args, local):
                        "points_differing": int((a["damage"] != b["damage"]).sum()),
                        "points_damaged_fp64": int((a["damage"] > 0).sum())},
             "broken_bonds": {"fp64": int((a["bonds"] == 0).sum()), "fp32": int((b["bonds"] == 0).sum()),
-                             "state_differs": int((a["bonds"] != b["bonds"]).sum())},
+                             "state_differs": int((a["bonds"] != b["bonds"]).sum()),
+                             "near_critical_1e-12": {"fp64": a["near"], "fp32": b["near"]}},
             "seconds": {"fp64": a["s"], "fp32": b["s"], "ratio": a["s"] / b["s"]},
             "mapping": {"fp64": a["mapping"], "fp32": b["mapping"]}}
     print(json.dumps(line), flush=True)

@@ -182,6 +182,11 @@ pd_status pd_break_bonds(pd_handle *h, const uint8_t *set_a, const uint8_t *set_
  * `fraction`, decided by a hash of (min(i,j), max(i,j), seed), so both directions agree. */
 pd_status pd_break_random_pairs(pd_handle *h, double fraction, uint64_t seed);
 
+/* Bonds that may fail and whose current stretch (l - L) / L, evaluated in FP64, lies within
+ * tol of the owner's critical stretch: the decisions of calc_failure! (bond_system.jl:309-327)
+ * that a different summation order can flip. Reported beside broken-bond comparisons. */
+pd_status pd_count_near_critical(pd_handle *h, double tol, int64_t *count);
+
 /* pd_break_random_pairs hashing point_ids[i] (n int64, host) instead of the row numbers: a
  * partition passes the body's point numbers of its rows and breaks the same pairs as the
  * undivided body. */

@@ -1230,6 +1230,28 @@ extern "C" pd_status pd_break_bonds(pd_handle* h, const uint8_t* set_a, const ui
   return PD_OK;
 }
 
+extern "C" pd_status pd_count_near_critical(pd_handle* h, double tol, int64_t* count) {
+  if (!h || !count) return fail(PD_ERR_ARG, "NULL argument");
+  if (!(tol >= 0)) return fail(PD_ERR_ARG, "tol must be >= 0");
+  PD_CUDA(cudaSetDevice(h->device));
+  *count = 0;
+  if (h->n == 0) return PD_OK;
+  unsigned long long* dc = nullptr;
+  PD_CUDA(cudaMalloc(&dc, sizeof(unsigned long long)));
+  cudaError_t e = cudaMemsetAsync(dc, 0, sizeof(unsigned long long), h->stream);
+  if (e == cudaSuccess) {
+    launch_near_critical(h->d, h->g, tol, dc, h->stream);
+    e = cudaGetLastError();
+  }
+  unsigned long long c = 0;
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&c, dc, sizeof(c), cudaMemcpyDeviceToHost, h->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  cudaFree(dc);
+  if (e != cudaSuccess) return fail(PD_ERR_CUDA, cudaGetErrorString(e));
+  *count = (int64_t)c;
+  return PD_OK;
+}
+
 extern "C" pd_status pd_break_random_pairs(pd_handle* h, double fraction, uint64_t seed) {
   return pd_break_random_pairs_ids(h, fraction, seed, nullptr);
 }

@@ -84,6 +84,8 @@ void launch_export_damage(const DevBody& d, int valid, double* out, cudaStream_t
 void launch_export_position(const DevBody& d, const IntDev& g, double* out, int what, cudaStream_t s);
 void launch_timestep(const DevBody& d, double* dt_point, cudaStream_t s);
 void launch_break_sets(const DevBody& d, const unsigned char* A, const unsigned char* B, cudaStream_t s);
+void launch_near_critical(const DevBody& d, const IntDev& g, double tol, unsigned long long* count,
+                          cudaStream_t s);
 void launch_break_random(const DevBody& d, double fraction, unsigned long long seed,
                          const long long* gid, cudaStream_t s);
 

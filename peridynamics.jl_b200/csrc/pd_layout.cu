@@ -330,6 +330,46 @@ void launch_timestep(const DevBody& d, double* dt_point, cudaStream_t s) {
   k_timestep<<<blocks_for(d.n, 256), 256, 0, s>>>(d, dt_point);
 }
 
+// bonds that may fail and whose current stretch lies within tol of the owner's critical
+// stretch (FP64 from the current state in both precisions): the failure decisions that the
+// rounding of a summation order can flip
+__global__ void k_near_critical(DevBody d, IntDev g, double tol, unsigned long long* count) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= d.n) return;
+  const DevParam& P = d.params[d.meta[i] & META_PID_MASK];
+  const int cnt = (int)(d.off[i + 1] - d.off[i]);
+  const double4 Xi = d.X0[i], ci = d.cur[i];
+  unsigned long long c = 0;
+  for (int k = 0; k < cnt; k++) {
+    const long long b = bond_slot(d, i, k);
+    const int j = d.nbr[b];
+    const double4 Xj = d.X0[j], cj = d.cur[j];
+    double L, dx, dy, dz;
+    bool permitted;
+    if (d.len64) {
+      L = fabs(d.len64[b]);
+      permitted = d.len64[b] > 0;
+      dx = cj.x - ci.x; dy = cj.y - ci.y; dz = cj.z - ci.z;
+    } else {  // FP32 path: cur holds the displacement
+      const double ex = Xi.x - Xj.x, ey = Xi.y - Xj.y, ez = Xi.z - Xj.z;
+      L = sqrt((ex * ex + ey * ey) + ez * ez);
+      permitted = d.geo[b].w > 0;
+      dx = (Xj.x + cj.x) - (Xi.x + ci.x);
+      dy = (Xj.y + cj.y) - (Xi.y + ci.y);
+      dz = (Xj.z + cj.z) - (Xi.z + ci.z);
+    }
+    const double l = sqrt((dx * dx + dy * dy) + dz * dz);
+    if (permitted && fabs((l - L) / L - P.epsc) <= tol) c++;
+  }
+  (void)g;
+  if (c) atomicAdd(count, c);
+}
+
+void launch_near_critical(const DevBody& d, const IntDev& g, double tol, unsigned long long* count,
+                          cudaStream_t s) {
+  k_near_critical<<<blocks_for(d.n, 256), 256, 0, s>>>(d, g, tol, count);
+}
+
 // break_bonds! (bond_system.jl:249-267): bonds between a point of set a and a point of set b
 // become inactive
 __global__ void k_break_sets(DevBody d, const unsigned char* A, const unsigned char* B) {

@@ -43,7 +43,7 @@ EXPORTS = (
     "pd_dr_init", "pd_run_dr", "pd_run_dr_timed", "pd_dr_density_matrix",
     "pd_break_random_pairs_ids", "pd_create_partition", "pd_set_stream", "pd_vv_begin",
     "pd_force_phase", "pd_vv_stage", "pd_vv_end", "pd_halo_row_bytes", "pd_halo_pack",
-    "pd_halo_unpack", "pd_esc_init", "pd_esc_get",
+    "pd_halo_unpack", "pd_esc_init", "pd_esc_get", "pd_count_near_critical",
     "pd_nk_set_conditions", "pd_nk_step", "pd_nk_set_corrections", "pd_nk_apply",
     "pd_nk_record", "pd_nk_recorded", "pd_nk_recorded_vector",
     "pd_mpnn_create", "pd_mpnn_destroy", "pd_mpnn_set_params", "pd_mpnn_get_params",
@@ -165,6 +165,7 @@ def lib():
         "pd_halo_unpack": [vp, i32, vp, i64, vp],
         "pd_esc_init": [vp, i32],
         "pd_esc_get": [vp, vp, vp],
+        "pd_count_near_critical": [vp, dbl, vp],
         "pd_run_dr": [vp, i64, i64],
         "pd_run_dr_timed": [vp, i64, i64, vp, vp, vp, vp],
         "pd_dr_density_matrix": [vp, vp],

@@ -315,6 +315,12 @@ class DeviceBody:
         L.check(L.lib().pd_launch_count(self.h, C.byref(c)))
         return c.value
 
+    def near_critical(self, tol=1e-12):
+        """Bonds that may fail with |eps - eps_c| <= tol at the current state."""
+        c = C.c_int64()
+        L.check(L.lib().pd_count_near_critical(self.h, float(tol), C.byref(c)), "pd_count_near_critical")
+        return c.value
+
     def surface_correction(self):
         """(mfactor (n, 3), scfactor (n_bonds, CSR order)) of EnergySurfaceCorrection."""
         mf = np.empty((self.n, 3))

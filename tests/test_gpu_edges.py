@@ -65,3 +65,21 @@ def test_point_without_bonds(name):
     assert np.max(np.abs(u32 - ob.u)) <= 1e-5 * np.max(np.abs(ob.u))
     assert not dev.field("b_int")[:, -1].any()
     dev.close()
+
+
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+def test_near_critical_bonds_are_counted(prec):
+    body = pd.Body(pd.BBMaterial(), np.array([[0.0, 1.0], [0.0, 0.0], [0.0, 0.0]]), np.ones(2))
+    pd.material(body, horizon=1.5, rho=1.0, E=1.0, Gc=1.0)
+    epsc = body.point_params[0].epsilon_c
+    dev = pd.DeviceBody(body, precision=prec)
+    for x, expected in ((1.0 + epsc, 2), (1.0 + 2 * epsc, 0), (1.0, 0)):
+        pos = body._pos.copy()
+        pos[1, 0] = x
+        if prec == "fp64":
+            dev.set_state(position=pos)
+        else:
+            dev.set_state(displacement=pos - body._pos)
+        assert dev.near_critical(1e-12) == expected, x
+    assert dev.near_critical(2 * epsc) == 2
+    dev.close()

@@ -224,8 +224,10 @@ static pd_status finish_create(pd_handle* h, int* dnbr_csr, const double* dL, co
     } else {
       PD_TRY(dalloc(h, &h->d.H32, 9 * n));
       PD_TRY(dalloc(h, &h->d.cst32, 3 * n));
+      PD_TRY(dalloc(h, &h->d.K32, 6 * n));
       PD_CUDA(cudaMemsetAsync(h->d.H32, 0, sizeof(float) * 9 * n, h->stream));
       PD_CUDA(cudaMemsetAsync(h->d.cst32, 0, sizeof(float4) * 3 * n, h->stream));
+      PD_CUDA(cudaMemsetAsync(h->d.K32, 0, sizeof(float) * 6 * n, h->stream));
     }
   }
   launch_count_active(h->d, h->stream);
@@ -673,6 +675,7 @@ extern "C" pd_status pd_set_state(pd_handle* h, const double* position, const do
     cudaError_t e = cudaMemcpy(tmp, bond_active, nb, cudaMemcpyHostToDevice);
     if (e == cudaSuccess) {
       launch_pack_bits(h->d, tmp, h->stream);
+      h->kfull = true;
       e = cudaStreamSynchronize(h->stream);
     }
     cudaFree(tmp);
@@ -925,6 +928,11 @@ extern "C" pd_status pd_set_param_timesteps(pd_handle* h, const double* dtp) {
 
 static int launch_force(pd_handle* h, int kstep, int phase) {
   int k;
+  // FP32 CMat: the first phase-A launch after bond states changed outside the kernels sums the
+  // shape tensors in full; graphs captured with that launch are captured again
+  const bool fullk = h->kfull && h->material == PD_MAT_CMAT && h->precision != PD_PREC_FP64 && phase != 2;
+  h->cfg.fullk = fullk ? 1 : 0;
+  if (fullk) { h->kfull = false; h->version++; }
   if (h->precision == PD_PREC_FP64) k = launch_force64(h->d, h->cfg, kstep, phase, h->stream);
   else if (h->cfg.pipe >= 1 && h->cfg.pipe <= 3 && !h->d.sc32 && tma_supported(h->d))
     k = launch_force32_tma(h->d, h->cfg.pipe, kstep, phase, h->stream);
@@ -1220,6 +1228,7 @@ extern "C" pd_status pd_break_bonds(pd_handle* h, const uint8_t* set_a, const ui
   if (e == cudaSuccess) e = cudaMemcpy(tmp + n, set_b, n, cudaMemcpyHostToDevice);
   if (e == cudaSuccess) {
     launch_break_sets(h->d, tmp, tmp + n, h->stream);
+    h->kfull = true;
     launch_count_active(h->d, h->stream);
     e = cudaStreamSynchronize(h->stream);
   }
@@ -1268,6 +1277,7 @@ extern "C" pd_status pd_break_random_pairs_ids(pd_handle* h, double fraction, ui
     PD_CUDA(cudaMemcpy(gid, point_ids, sizeof(long long) * h->n, cudaMemcpyHostToDevice));
   }
   launch_break_random(h->d, fraction, (unsigned long long)seed, gid, h->stream);
+  h->kfull = true;
   launch_count_active(h->d, h->stream);
   PD_CUDA(cudaStreamSynchronize(h->stream));
   dfree(h, gid);

@@ -103,6 +103,7 @@ struct DevBody {
   double* PK64;      // CMat FP64: P K^-1 (9 per point)
   float* H32;        // CMat FP32: displacement gradient H = F - I (9 per point)
   float4* cst32;     // CMat FP32: 3 float4 per point {A (9), beta~, 0, 0}
+  float* K32;        // CMat FP32: the scaled shape tensor of every point {xx, yy, zz, xy, xz, yz}
   // EnergySurfaceCorrection (BB, OSB): the factor of every bond slot (FP64 / FP32 path) and
   // the per-point multiplication factors {x, y, z} it is made from; null without correction
   const double* sc64;

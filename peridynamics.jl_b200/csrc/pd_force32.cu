@@ -573,12 +573,23 @@ __device__ void pk1_32(int cmodel, const DevParam& p, const float* H, float* P) 
 #ifndef PD_MINB_CA
 #define PD_MINB_CA 3
 #endif
-template <int G>
-__global__ void __launch_bounds__(256, PD_MINB_CA) k_c_a32(DevBody d, int kstep) {
+// The shape tensor K depends on the reference bonds and their states only. FULLK sums it over
+// the active bonds (the first evaluation, or after bond states changed outside the kernels);
+// otherwise the stored K of the point loses the terms of the bonds that break in this
+// evaluation, and only the nine sums of the deformation gradient run over all bonds.
+// the variant that updates the stored shape tensors keeps 9 compensated sums: 4 resident blocks
+// (64 registers). Measured on the 1M-point CMat block: phase A 1.09 ms at 4 blocks, 1.22 ms at
+// 3; the full-sum variant took 1.43 ms every step.
+#ifndef PD_MINB_CAI
+#define PD_MINB_CAI 4
+#endif
+template <int G, bool FULLK>
+__global__ void __launch_bounds__(256, FULLK ? PD_MINB_CA : PD_MINB_CAI) k_c_a32(DevBody d, int kstep) {
   if (d.ctrl->err) return;
   PD_SLICE_LOOP(G) {
     PD_SLICE_SETUP
-    KSum K[6], Hs[9];
+    KSum K[FULLK ? 6 : 1], Hs[9];
+    float dK[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
     int na = 0;
     const unsigned meta = valid ? d.meta[i] : 0u;
     const DevParam& P = d.params[meta & META_PID_MASK];
@@ -602,29 +613,57 @@ __global__ void __launch_bounds__(256, PD_MINB_CA) k_c_a32(DevBody d, int kstep)
           const float t = omega_r(d.kernel, P.deltaf, B.L, B.rL) * hj.w * vs;
           const float X[3] = {B.gx * id, B.gy * id, B.gz * id};
           const float U[3] = {B.dux * id, B.duy * id, B.duz * id};
-          K[0].add(t * X[0] * X[0]); K[1].add(t * X[1] * X[1]); K[2].add(t * X[2] * X[2]);
-          K[3].add(t * X[0] * X[1]); K[4].add(t * X[0] * X[2]); K[5].add(t * X[1] * X[2]);
+          if constexpr (FULLK) {
+            K[0].add(t * X[0] * X[0]); K[1].add(t * X[1] * X[1]); K[2].add(t * X[2] * X[2]);
+            K[3].add(t * X[0] * X[1]); K[4].add(t * X[0] * X[2]); K[5].add(t * X[1] * X[2]);
+          }
 #pragma unroll
           for (int c = 0; c < 3; c++)
 #pragma unroll
             for (int q = 0; q < 3; q++) Hs[q + 3 * c].add(t * U[q] * X[c]);
+        } else if (!FULLK && ((word >> lane) & 1u)) {
+          // the bond breaks now: its term leaves the stored shape tensor
+          const float t = omega_r(d.kernel, P.deltaf, B.L, B.rL) * hj.w * vs;
+          const float X[3] = {B.gx * id, B.gy * id, B.gz * id};
+          dK[0] += t * X[0] * X[0]; dK[1] += t * X[1] * X[1]; dK[2] += t * X[2] * X[2];
+          dK[3] += t * X[0] * X[1]; dK[4] += t * X[0] * X[2]; dK[5] += t * X[1] * X[2];
         }
       }
       na += act;
       commit_row(d.bits, wi, word, act, lane);
     }
     if (G > 1) {
+      if constexpr (FULLK) {
 #pragma unroll
-      for (int q = 0; q < 6; q++) group_reduce<G>(K[q]);
+        for (int q = 0; q < 6; q++) group_reduce<G>(K[q]);
+      } else {
+#pragma unroll
+        for (int q = 0; q < 6; q++) dK[q] = group_sum<G>(dK[q]);
+      }
 #pragma unroll
       for (int q = 0; q < 9; q++) group_reduce<G>(Hs[q]);
       na = group_sum<G>(na);
     }
     bool killed = false;
     if (valid && gl == 0) {
-      const float Km[9] = {K[0].value(), K[3].value(), K[4].value(),
-                           K[3].value(), K[1].value(), K[5].value(),
-                           K[4].value(), K[5].value(), K[2].value()};
+      float k6[6];
+      float2* ks = reinterpret_cast<float2*>(d.K32 + 6 * i);
+      if constexpr (FULLK) {
+#pragma unroll
+        for (int q = 0; q < 6; q++) k6[q] = K[q].value();
+        ks[0] = make_float2(k6[0], k6[1]); ks[1] = make_float2(k6[2], k6[3]); ks[2] = make_float2(k6[4], k6[5]);
+      } else {
+        const float2 a0 = ks[0], a1 = ks[1], a2 = ks[2];
+        k6[0] = a0.x; k6[1] = a0.y; k6[2] = a1.x; k6[3] = a1.y; k6[4] = a2.x; k6[5] = a2.y;
+        if (dK[0] != 0.f || dK[1] != 0.f || dK[2] != 0.f) {  // a bond broke
+#pragma unroll
+          for (int q = 0; q < 6; q++) k6[q] -= dK[q];
+          ks[0] = make_float2(k6[0], k6[1]); ks[1] = make_float2(k6[2], k6[3]); ks[2] = make_float2(k6[4], k6[5]);
+        }
+      }
+      const float Km[9] = {k6[0], k6[3], k6[4],
+                           k6[3], k6[1], k6[5],
+                           k6[4], k6[5], k6[2]};
       float Kinv[9], Hm[9], H[9];
       finv3(Km, Kinv);
       for (int q = 0; q < 9; q++) Hm[q] = Hs[q].value();
@@ -799,7 +838,11 @@ int launch_force32(const DevBody& d, const LaunchCfg& c, int kstep, int phase, c
     if (d.sc32) return launch_osb32<true>(d, c, G, grid, kstep, A, B, s);
     return launch_osb32<false>(d, c, G, grid, kstep, A, B, s);
   }
-  if (A) { PD_DISPATCH_G(G, (k_c_a32<GG><<<grid, c.block, 0, s>>>(d, kstep))); launches++; }
+  if (A) {
+    if (c.fullk) { PD_DISPATCH_G(G, (k_c_a32<GG, true><<<grid, c.block, 0, s>>>(d, kstep))); }
+    else { PD_DISPATCH_G(G, (k_c_a32<GG, false><<<grid, c.block, 0, s>>>(d, kstep))); }
+    launches++;
+  }
   if (B) { PD_DISPATCH_G(G, (k_c_b32<GG><<<grid, c.block, 0, s>>>(d, kstep))); launches++; }
   return launches;
 }

@@ -66,7 +66,9 @@ struct pd_handle {
   DevParam* dparams = nullptr;
   int* rev = nullptr;
   int* flags = nullptr;
-  LaunchCfg cfg{1, 256, false, 0};
+  LaunchCfg cfg{1, 256, false, 0, 0};
+  // FP32 CMat: the stored shape tensors are stale (bond states changed outside the kernels)
+  bool kfull = true;
   bool damage_valid = false;
   bool has_bext_state = false;
   // boundary conditions (host side)

@@ -928,9 +928,10 @@ extern "C" pd_status pd_set_param_timesteps(pd_handle* h, const double* dtp) {
 
 static int launch_force(pd_handle* h, int kstep, int phase) {
   int k;
-  // FP32 CMat: the first phase-A launch after bond states changed outside the kernels sums the
-  // shape tensors in full; graphs captured with that launch are captured again
-  const bool fullk = h->kfull && h->material == PD_MAT_CMAT && h->precision != PD_PREC_FP64 && phase != 2;
+  // FP32 OSB / CMat: the first phase-A launch after bond states changed outside the kernels sums
+  // the weighted volumes / shape tensors in full; graphs captured with that launch are
+  // captured again
+  const bool fullk = h->kfull && h->material != PD_MAT_BB && h->precision != PD_PREC_FP64 && phase != 2;
   h->cfg.fullk = fullk ? 1 : 0;
   if (fullk) { h->kfull = false; h->version++; }
   if (h->precision == PD_PREC_FP64) k = launch_force64(h->d, h->cfg, kstep, phase, h->stream);

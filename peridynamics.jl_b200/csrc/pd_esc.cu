@@ -202,7 +202,8 @@ extern "C" pd_status pd_esc_init(pd_handle* h, int32_t what) {
     h->launches++;
     h->d.sc64 = sc64;
     h->d.sc32 = sc32;
-    h->version++;  // cached step graphs hold the previous kernels
+    h->version++;     // cached step graphs hold the previous kernels
+    h->kfull = true;  // stored weighted volumes hold the previous factors
   }
   PD_CUDA(cudaGetLastError());
   PD_CUDA(cudaStreamSynchronize(h->stream));

@@ -199,13 +199,18 @@ __global__ void __launch_bounds__(256, PD_MINB_UBB) k_bb32u(DevBody d, int kstep
 // OSB phase A (ordinary_state_based.jl:107-126, 176-204): failure, weighted volume m,
 // dilatation theta, and c1 = 15 G / m, c2 = theta (3 K / m - c1 / 3) (:135-136)
 // -------------------------------------------------------------------------------------------
-// ESC: the bond factor beta in the weighted volume and the dilatation (:182, :198)
-template <int G, bool ESC>
+// ESC: the bond factor beta in the weighted volume and the dilatation (:182, :198).
+// FULLM: the weighted volume m depends on the reference bonds and their states only; it is
+// summed over the active bonds when FULLM (the first evaluation, or after bond states changed
+// outside the kernels), otherwise the stored m of the point loses the terms of the bonds that
+// break in this evaluation.
+template <int G, bool ESC, bool FULLM>
 __global__ void PD_LB_A k_osb_a32(DevBody d, int kstep) {
   if (d.ctrl->err) return;
   PD_SLICE_LOOP(G) {
     PD_SLICE_SETUP
     KSum m, th;
+    float dm = 0.f;
     int na = 0;
     const DevParam& P = d.params[valid ? (d.meta[i] & META_PID_MASK) : 0];
     const float4 hi = valid ? d.uhi[i] : make_float4(0.f, 0.f, 0.f, 0.f);
@@ -241,16 +246,23 @@ __global__ void PD_LB_A k_osb_a32(DevBody d, int kstep) {
         if (act) {
           float om = omega_r(d.kernel, delta, B.L, B.rL) * hj.w;
           if (ESC) om *= bet;
-          m.add(om * (B.gx * B.gx + B.gy * B.gy + B.gz * B.gz));
+          if (FULLM) m.add(om * (B.gx * B.gx + B.gy * B.gy + B.gz * B.gz));
           th.add(om * B.L * B.e);
+        } else if (!FULLM && ((word >> lane) & 1u)) {  // breaks now: leaves the stored m
+          float om = omega_r(d.kernel, delta, B.L, B.rL) * hj.w;
+          if (ESC) om *= bet;
+          dm += om * (B.gx * B.gx + B.gy * B.gy + B.gz * B.gz);
         }
       }
       na += act;
       commit_row(d.bits, wi, word, act, lane);
     }
-    if (G > 1) { group_reduce<G>(m); group_reduce<G>(th); na = group_sum<G>(na); }
+    if (G > 1) {
+      if (FULLM) group_reduce<G>(m); else dm = group_sum<G>(dm);
+      group_reduce<G>(th); na = group_sum<G>(na);
+    }
     if (valid && gl == 0) {
-      const float wv = m.value();
+      const float wv = FULLM ? m.value() : (dm != 0.f ? d.cm32[i].x - dm : d.cm32[i].x);
       float c1 = 0.f, c2 = 0.f, dil = 0.f;
       if (wv != 0.f) {
         dil = 3.f / wv * th.value();
@@ -366,12 +378,13 @@ __global__ void PD_LB k_osb_b32(DevBody d, int kstep) {
 #ifndef PD_MINB_UB
 #define PD_MINB_UB 4
 #endif
-template <int G, bool ESC>
+template <int G, bool ESC, bool FULLM>
 __global__ void __launch_bounds__(256, PD_MINB_UA) k_osb_a32u(DevBody d, int kstep) {
   if (d.ctrl->err) return;
   PD_SLICE_LOOP(G) {
     PD_SLICE_SETUP
     KSum m, th;
+    float dm = 0.f;
     int na = 0;
     const DevParam& P = d.params[valid ? (d.meta[i] & META_PID_MASK) : 0];
     const float4 hi = valid ? d.uhi[i] : make_float4(0.f, 0.f, 0.f, 0.f);
@@ -403,8 +416,12 @@ __global__ void __launch_bounds__(256, PD_MINB_UA) k_osb_a32u(DevBody d, int kst
         if (act) {
           float om = omega_r(d.kernel, delta, B.L, B.rL) * hj.w;
           if (ESC) om *= u ? s1 : s0;
-          m.add(om * (B.gx * B.gx + B.gy * B.gy + B.gz * B.gz));
+          if (FULLM) m.add(om * (B.gx * B.gx + B.gy * B.gy + B.gz * B.gz));
           th.add(om * B.L * B.e);
+        } else if (!FULLM && (((u ? w1 : w0) >> lane) & 1u)) {  // breaks now (see k_osb_a32)
+          float om = omega_r(d.kernel, delta, B.L, B.rL) * hj.w;
+          if (ESC) om *= u ? s1 : s0;
+          dm += om * (B.gx * B.gx + B.gy * B.gy + B.gz * B.gz);
         }
         if (u) act1 = act; else act0 = act;
       }
@@ -412,9 +429,12 @@ __global__ void __launch_bounds__(256, PD_MINB_UA) k_osb_a32u(DevBody d, int kst
       commit_row(d.bits, wi, w0, act0, lane);
       if (two) commit_row(d.bits, wi + 1, w1, act1, lane);
     }
-    if (G > 1) { group_reduce<G>(m); group_reduce<G>(th); na = group_sum<G>(na); }
+    if (G > 1) {
+      if (FULLM) group_reduce<G>(m); else dm = group_sum<G>(dm);
+      group_reduce<G>(th); na = group_sum<G>(na);
+    }
     if (valid && gl == 0) {
-      const float wv = m.value();
+      const float wv = FULLM ? m.value() : (dm != 0.f ? d.cm32[i].x - dm : d.cm32[i].x);
       float c1 = 0.f, c2 = 0.f, dil = 0.f;
       if (wv != 0.f) {
         dil = 3.f / wv * th.value();
@@ -806,7 +826,11 @@ static int launch_osb32(const DevBody& d, const LaunchCfg& c, int G, int grid, i
                         bool B, cudaStream_t s) {
   int launches = 0;
   if (c.pipe == 4) {
-    if (A) { PD_DISPATCH_G(G, (k_osb_a32u<GG, ESC><<<grid, c.block, 0, s>>>(d, kstep))); launches++; }
+    if (A) {
+      if (c.fullk) { PD_DISPATCH_G(G, (k_osb_a32u<GG, ESC, true><<<grid, c.block, 0, s>>>(d, kstep))); }
+      else { PD_DISPATCH_G(G, (k_osb_a32u<GG, ESC, false><<<grid, c.block, 0, s>>>(d, kstep))); }
+      launches++;
+    }
     if (B) {
       if (d.multi) { PD_DISPATCH_G(G, (k_osb_b32u<GG, true, ESC><<<grid, c.block, 0, s>>>(d, kstep))); }
       else { PD_DISPATCH_G(G, (k_osb_b32u<GG, false, ESC><<<grid, c.block, 0, s>>>(d, kstep))); }
@@ -814,7 +838,11 @@ static int launch_osb32(const DevBody& d, const LaunchCfg& c, int G, int grid, i
     }
     return launches;
   }
-  if (A) { PD_DISPATCH_G(G, (k_osb_a32<GG, ESC><<<grid, c.block, 0, s>>>(d, kstep))); launches++; }
+  if (A) {
+    if (c.fullk) { PD_DISPATCH_G(G, (k_osb_a32<GG, ESC, true><<<grid, c.block, 0, s>>>(d, kstep))); }
+    else { PD_DISPATCH_G(G, (k_osb_a32<GG, ESC, false><<<grid, c.block, 0, s>>>(d, kstep))); }
+    launches++;
+  }
   if (B) {
     if (d.multi) { PD_DISPATCH_G(G, (k_osb_b32<GG, true, ESC><<<grid, c.block, 0, s>>>(d, kstep))); }
     else { PD_DISPATCH_G(G, (k_osb_b32<GG, false, ESC><<<grid, c.block, 0, s>>>(d, kstep))); }

@@ -67,7 +67,8 @@ struct pd_handle {
   int* rev = nullptr;
   int* flags = nullptr;
   LaunchCfg cfg{1, 256, false, 0, 0};
-  // FP32 CMat: the stored shape tensors are stale (bond states changed outside the kernels)
+  // FP32 OSB / CMat: the stored weighted volumes / shape tensors are stale (bond states
+  // changed outside the kernels)
   bool kfull = true;
   bool damage_valid = false;
   bool has_bext_state = false;

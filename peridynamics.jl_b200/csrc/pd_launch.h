@@ -11,7 +11,8 @@ struct LaunchCfg {
   bool exact; // FP64: one lane per point in the reference's serial summation order
   int pipe;   // FP32: 0 = plain loads, 1-3 = TMA-staged bond stream (pd_force32_tma.cu),
               // 4 = two rows of neighbour gathers in flight (BB, OSB)
-  int fullk;  // FP32 CMat: sum the shape tensors in full (else update the stored ones)
+  int fullk;  // FP32 OSB / CMat: sum the weighted volumes / shape tensors in full (else
+              // update the stored ones)
 };
 
 // boundary conditions as the integration kernels see them

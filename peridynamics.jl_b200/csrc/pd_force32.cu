@@ -597,11 +597,12 @@ __device__ void pk1_32(int cmodel, const DevParam& p, const float* H, float* P) 
 // the active bonds (the first evaluation, or after bond states changed outside the kernels);
 // otherwise the stored K of the point loses the terms of the bonds that break in this
 // evaluation, and only the nine sums of the deformation gradient run over all bonds.
-// the variant that updates the stored shape tensors keeps 9 compensated sums: 4 resident blocks
-// (64 registers). Measured on the 1M-point CMat block: phase A 1.09 ms at 4 blocks, 1.22 ms at
-// 3; the full-sum variant took 1.43 ms every step.
+// the variant that updates the stored shape tensors keeps 9 compensated sums and the next row's
+// bond record in flight. Measured on the 1M-point CMat block: phase A 0.97 ms at 3 resident
+// blocks (80 registers), 1.01 ms at 4 (64, with spills); without the row prefetch 1.09 ms at 4
+// and 1.22 ms at 3; the full-sum variant took 1.43 ms every step.
 #ifndef PD_MINB_CAI
-#define PD_MINB_CAI 4
+#define PD_MINB_CAI 3
 #endif
 template <int G, bool FULLK>
 __global__ void __launch_bounds__(256, FULLK ? PD_MINB_CA : PD_MINB_CAI) k_c_a32(DevBody d, int kstep) {
@@ -616,15 +617,24 @@ __global__ void __launch_bounds__(256, FULLK ? PD_MINB_CA : PD_MINB_CAI) k_c_a32
     const float4 hi = valid ? d.uhi[i] : make_float4(0.f, 0.f, 0.f, 0.f);
     const float4 lo = valid ? d.ulo[i] : make_float4(0.f, 0.f, 0.f, 0.f);
     const float epsc = P.epscf, id = P.inv_delta, vs = P.vscale;
+    // the bond record of row r + 1 is loaded while row r is processed
+    const long long b0 = sbase + lane;
+    int jn = 0;
+    float4 gn = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (rows > 0 && gl < cnt) { jn = __ldg(d.nbr + b0); gn = __ldg(d.geo + b0); }
     for (int r = 0; r < rows; r++) {
       const long long wi = (sbase >> 5) + r;
       const unsigned word = d.bits[wi];
       const int k = r * G + gl;
+      const int j = jn;
+      const float4 g = gn;
+      if (r + 1 < rows && k + G < cnt) {
+        const long long b1 = b0 + (long long)(r + 1) * 32;
+        jn = __ldg(d.nbr + b1);
+        gn = __ldg(d.geo + b1);
+      }
       bool act = false;
       if (k < cnt) {
-        const long long b = sbase + (long long)r * 32 + lane;
-        const int j = __ldg(d.nbr + b);
-        const float4 g = __ldg(d.geo + b);
         const float4 hj = __ldg(d.uhi + j), lj = __ldg(d.ulo + j);
         BondF B;
         bond32(g, hi, lo, hj, lj, B);

@@ -135,6 +135,8 @@ __global__ void PD_LB k_bb32(DevBody d, int kstep) {
 // Two-row BB (pipe 4): the bond records and neighbour gathers of rows r and r + 1 are issued
 // before either row is processed (two dependent gathers in flight per lane, as the OSB
 // two-row kernels); each lane adds its bonds in row order, so the sums equal k_bb32's.
+// Measured on the 1M-point BB block: 0.581 ms per step at 4 resident blocks (64 registers),
+// 0.602 ms at 3, 0.725 ms at 5.
 #ifndef PD_MINB_UBB
 #define PD_MINB_UBB 4
 #endif

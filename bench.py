@@ -446,6 +446,11 @@ def run_dr(args, rank, world, local, dist):
     # (page-locked host buffers)
     bufs = [pinned(n_pts, 3), pinned(n_pts, 3), pinned(n_pts, 3), pinned(n_pts)]
     h_u, h_v, out_u, out_d = (b[1] for b in bufs)
+    # untimed warm-up through the same calls
+    dev.set_state(displacement=h_u, velocity=h_v)
+    drm.init(dev, dr)
+    drm.run(dev, dr, 1, max(args.warmup, 3))
+    dev.field("displacement", out=out_u)
     barrier()
     t0 = time.perf_counter()
     dev.set_state(displacement=h_u, velocity=h_v)
@@ -626,7 +631,7 @@ def _jfnk_arm(pd, mpnn, nkm, body, device, pc, G, increments, n_steps, weights, 
 
 
 def jfnk_compare(device, increments, n_steps=20, weights=JFNK_WEIGHTS, arms=JFNK_ARMS,
-                 gmres_maxiter=8000, newton_maxiter=12, groups=(4,)):
+                 gmres_maxiter=8000, newton_maxiter=12, groups=(4,), repeats=1):
     """The 500k-point three-point-bending beam (250 x 50 x 40 points, dx = 1 mm, E = 70 GPa,
     no fracture, mid-span line pushed 0.5 mm down over n_steps load increments): wall time
     of the first `increments` increments to a 1e-8 relative nonlinear residual per increment,
@@ -635,7 +640,9 @@ def jfnk_compare(device, increments, n_steps=20, weights=JFNK_WEIGHTS, arms=JFNK
     every lane mapping in `groups` (lanes per point of the force kernels): the mapping sets the
     FP64 summation order, and the finite-difference products carry that rounding into the
     Krylov counts, so several mappings give the spread of a count; the first one is the
-    reported run."""
+    reported run. With repeats > 1 every arm runs that many times (the solves are
+    deterministic: the same Krylov counts) and reports its fastest time, so that a transient
+    clock drop of a power-capped GPU does not decide the comparison; all times are listed."""
     import pdcuda as pd
     from pdcuda import mpnn
     from pdcuda import newton_krylov as nkm
@@ -646,8 +653,16 @@ def jfnk_compare(device, increments, n_steps=20, weights=JFNK_WEIGHTS, arms=JFNK
     for pc in arms:
         runs = []
         for G in groups:
-            runs.append(_jfnk_arm(pd, mpnn, nkm, body, device, pc, G, increments, n_steps, weights,
-                                  gmres_maxiter, newton_maxiter, budget))
+            rep = []
+            for _ in range(max(repeats, 1)):
+                rep.append(_jfnk_arm(pd, mpnn, nkm, body, device, pc, G, increments, n_steps,
+                                     weights, gmres_maxiter, newton_maxiter, budget))
+            done = [r for r in rep if r is not None]
+            best = (min(done, key=lambda r: (not r.get("converged", True), r["s"]))
+                    if done else None)
+            if best is not None and len(rep) > 1:
+                best["repeats_s"] = [None if r is None else r["s"] for r in rep]
+            runs.append(best)
         r0 = runs[0]
         if r0 is not None and len(runs) > 1:
             r0["spread"] = {str(G): (None if r is None else {"s": r["s"], "gmres_iters": r["gmres_iters"]})
@@ -673,7 +688,8 @@ def run_jfnk(args, rank, world):
                        arms=tuple(args.jfnk_arms.split(",")),
                        gmres_maxiter=args.jfnk_gmres_maxiter,
                        newton_maxiter=args.jfnk_newton_maxiter,
-                       groups=tuple(int(g) for g in args.jfnk_groups.split(",")))
+                       groups=tuple(int(g) for g in args.jfnk_groups.split(",")),
+                       repeats=max(args.jfnk_repeats, 1))
     arms = res["arms"]
     ok = lambda a: a is not None and a.get("converged", True)
     ran = [arms[k] for k in ("learned_poly", "block_poly", "block_jacobi") if arms.get(k)]
@@ -735,6 +751,8 @@ def main():
                     help="load increments of the JFNK comparison (default: 20 with --config "
                          "jfnk500k, 2 in the default run, 0 = skip)")
     ap.add_argument("--jfnk-arms", default=",".join(JFNK_ARMS))
+    ap.add_argument("--jfnk-repeats", type=int, default=-1,
+                    help="runs per arm, fastest reported (default: 2 beside the VV line, 1 alone)")
     ap.add_argument("--jfnk-gmres-maxiter", type=int, default=8000)
     ap.add_argument("--jfnk-newton-maxiter", type=int, default=12)
     ap.add_argument("--jfnk-groups", default="4",
@@ -901,6 +919,10 @@ def main():
     # (page-locked host buffers)
     bufs = [pinned(n_pts, 3), pinned(n_pts, 3), pinned(n_pts, 3), pinned(n_pts)]
     h_u, h_v, out_u, out_d = (b[1] for b in bufs)
+    # untimed warm-up through the same calls (the rebuilt handle captures its graph here)
+    dev.set_state(displacement=h_u, velocity=h_v)
+    dev.run(1, max(args.warmup, 3), dt)
+    dev.field("displacement", out=out_u)
     barrier()
     t0 = time.perf_counter()
     dev.set_state(displacement=h_u, velocity=h_v)
@@ -919,7 +941,8 @@ def main():
     dev.close()
     jfnk = None
     if rank == 0 and world == 1 and args.jfnk_increments > 0:
-        jfnk = jfnk_compare(local, args.jfnk_increments)
+        jfnk = jfnk_compare(local, args.jfnk_increments,
+                            repeats=args.jfnk_repeats if args.jfnk_repeats > 0 else 2)
 
     if rank == 0:
         line = {

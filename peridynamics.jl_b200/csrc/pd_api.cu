@@ -603,6 +603,22 @@ static pd_status clear_error(pd_handle* h) {
   return PD_OK;
 }
 
+// the handle's transfer staging buffer, at least `bytes` long (a point field: 9 doubles a point
+// at most)
+static pd_status staging(pd_handle* h, size_t bytes, void** p) {
+  if (h->xfer_bytes < bytes) {
+    dfree(h, h->xfer);
+    h->xfer = nullptr;
+    h->xfer_bytes = 0;
+    unsigned char* q = nullptr;
+    PD_TRY(dalloc(h, &q, bytes));
+    h->xfer = q;
+    h->xfer_bytes = bytes;
+  }
+  *p = h->xfer;
+  return PD_OK;
+}
+
 // cur[i].xyz = in[3i..3i+2] (- X0[i].xyz with sub_x0); the fourth component is kept
 __global__ void k_set_cur(double4* cur, const double4* X0, const double* in, long long n, int sub_x0) {
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -633,9 +649,13 @@ extern "C" pd_status pd_set_state(pd_handle* h, const double* position, const do
   // packed on the device
   const double* src = nullptr;
   int sub_x0 = 0;
+  // every copy and kernel is ordered on the handle's stream (from page-locked host memory the
+  // copies run at full PCIe rate); one synchronize at the end
+  const size_t vec = sizeof(double) * 3 * n;
+  const cudaMemcpyKind h2d = cudaMemcpyHostToDevice;
   if (h->precision == PD_PREC_FP64) {
     src = position;
-    if (displacement) PD_CUDA(cudaMemcpy(h->g.u, displacement, sizeof(double) * 3 * n, cudaMemcpyHostToDevice));
+    if (displacement) PD_CUDA(cudaMemcpyAsync(h->g.u, displacement, vec, h2d, h->stream));
   } else if (displacement) {
     src = displacement;
   } else if (position) {
@@ -643,24 +663,21 @@ extern "C" pd_status pd_set_state(pd_handle* h, const double* position, const do
     sub_x0 = 1;
   }
   if (src) {
-    double* tmp = nullptr;
-    PD_CUDA(cudaMalloc(&tmp, sizeof(double) * 3 * n));
-    cudaError_t e = cudaMemcpy(tmp, src, sizeof(double) * 3 * n, cudaMemcpyHostToDevice);
-    if (e == cudaSuccess) {
-      k_set_cur<<<(unsigned)((n + 255) / 256), 256, 0, h->stream>>>(h->d.cur, h->d.X0, tmp, n, sub_x0);
-      e = cudaGetLastError();
-    }
-    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
-    cudaFree(tmp);
-    if (e != cudaSuccess) return fail(PD_ERR_CUDA, cudaGetErrorString(e));
+    void* tmp = nullptr;
+    PD_TRY(staging(h, vec, &tmp));
+    PD_CUDA(cudaMemcpyAsync(tmp, src, vec, h2d, h->stream));
+    k_set_cur<<<(unsigned)((n + 255) / 256), 256, 0, h->stream>>>(h->d.cur, h->d.X0, (const double*)tmp,
+                                                                  n, sub_x0);
+    PD_CUDA(cudaGetLastError());
     launch_split_u(h->d, h->stream);
     PD_CUDA(cudaGetLastError());
   }
-  if (velocity) PD_CUDA(cudaMemcpy(h->g.v, velocity, sizeof(double) * 3 * n, cudaMemcpyHostToDevice));
-  if (velocity_half) PD_CUDA(cudaMemcpy(h->g.vh, velocity_half, sizeof(double) * 3 * n, cudaMemcpyHostToDevice));
-  if (acceleration) PD_CUDA(cudaMemcpy(h->g.a, acceleration, sizeof(double) * 3 * n, cudaMemcpyHostToDevice));
+  if (velocity) PD_CUDA(cudaMemcpyAsync(h->g.v, velocity, vec, h2d, h->stream));
+  if (velocity_half) PD_CUDA(cudaMemcpyAsync(h->g.vh, velocity_half, vec, h2d, h->stream));
+  if (acceleration) PD_CUDA(cudaMemcpyAsync(h->g.a, acceleration, vec, h2d, h->stream));
+  PD_CUDA(cudaStreamSynchronize(h->stream));
   if (b_ext) {
-    PD_CUDA(cudaMemcpy(h->g.bext, b_ext, sizeof(double) * 3 * n, cudaMemcpyHostToDevice));
+    PD_CUDA(cudaMemcpy(h->g.bext, b_ext, vec, h2d));
     for (long long i = 0; i < n; i++) {
       const bool nz = b_ext[3 * i] != 0 || b_ext[3 * i + 1] != 0 || b_ext[3 * i + 2] != 0 ||
                       std::signbit(b_ext[3 * i]) || std::signbit(b_ext[3 * i + 1]) || std::signbit(b_ext[3 * i + 2]);
@@ -710,17 +727,19 @@ extern "C" pd_status pd_get_field(pd_handle* h, int32_t field, void* out, size_t
   }
   if (bytes != need) return fail(PD_ERR_ARG, "output size is " + std::to_string(bytes) + " bytes, need " + std::to_string(need));
   if (n == 0) return PD_OK;
+  // device -> host on the handle's stream; exported point fields go through the staging buffer
   auto copy = [&](const void* src) -> pd_status {
-    PD_CUDA(cudaMemcpy(out, src, need, cudaMemcpyDeviceToHost));
+    PD_CUDA(cudaMemcpyAsync(out, src, need, cudaMemcpyDeviceToHost, h->stream));
+    PD_CUDA(cudaStreamSynchronize(h->stream));
     return PD_OK;
   };
   void* tmp = nullptr;
   pd_status st = PD_OK;
   switch (field) {
     case PD_FIELD_POSITION: case PD_FIELD_DISPLACEMENT:
-      PD_CUDA(cudaMalloc(&tmp, need));
+      PD_TRY(staging(h, need, &tmp));
       launch_export_position(h->d, h->g, (double*)tmp, field == PD_FIELD_POSITION ? 0 : 1, h->stream);
-      PD_CUDA(cudaStreamSynchronize(h->stream));
+      PD_CUDA(cudaGetLastError());
       st = copy(tmp);
       break;
     case PD_FIELD_VELOCITY: st = copy(h->g.v); break;
@@ -737,9 +756,9 @@ extern "C" pd_status pd_get_field(pd_handle* h, int32_t field, void* out, size_t
       }
       break;
     case PD_FIELD_DAMAGE:
-      PD_CUDA(cudaMalloc(&tmp, need));
+      PD_TRY(staging(h, need, &tmp));
       launch_export_damage(h->d, h->damage_valid ? 1 : 0, (double*)tmp, h->stream);
-      PD_CUDA(cudaStreamSynchronize(h->stream));
+      PD_CUDA(cudaGetLastError());
       st = copy(tmp);
       break;
     case PD_FIELD_N_ACTIVE_BONDS: {
@@ -756,13 +775,18 @@ extern "C" pd_status pd_get_field(pd_handle* h, int32_t field, void* out, size_t
       for (long long i = 0; i < n; i++) o[i] = off[i + 1] - off[i];
       break;
     }
-    case PD_FIELD_BOND_ACTIVE:
+    case PD_FIELD_BOND_ACTIVE: {
       if (nb == 0) break;
+      // one byte a bond: a temporary, not kept
       PD_CUDA(cudaMalloc(&tmp, need));
       launch_export_bond_active(h->d, (unsigned char*)tmp, 0, h->stream);
-      PD_CUDA(cudaStreamSynchronize(h->stream));
-      st = copy(tmp);
+      cudaError_t e = cudaGetLastError();
+      if (e == cudaSuccess) e = cudaMemcpyAsync(out, tmp, need, cudaMemcpyDeviceToHost, h->stream);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+      cudaFree(tmp);
+      if (e != cudaSuccess) return fail(PD_ERR_CUDA, cudaGetErrorString(e));
       break;
+    }
     case PD_FIELD_DEFGRAD:
       if (h->precision == PD_PREC_FP64) st = copy(h->d.F64);
       else {
@@ -774,13 +798,12 @@ extern "C" pd_status pd_get_field(pd_handle* h, int32_t field, void* out, size_t
       }
       break;
     case PD_FIELD_CAUCHY_STRESS:
-      PD_CUDA(cudaMalloc(&tmp, need));
+      PD_TRY(staging(h, need, &tmp));
       launch_cauchy64(h->d, h->d.F64, h->precision == PD_PREC_FP64 ? 0 : 1, (double*)tmp, h->stream);
-      PD_CUDA(cudaStreamSynchronize(h->stream));
+      PD_CUDA(cudaGetLastError());
       st = copy(tmp);
       break;
   }
-  if (tmp) cudaFree(tmp);
   PD_CUDA(cudaGetLastError());
   return st;
 }

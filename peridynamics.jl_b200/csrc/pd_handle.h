@@ -94,6 +94,10 @@ struct pd_handle {
   // staged Velocity Verlet run (pd_vv_begin .. pd_vv_end)
   long long stage_n = 0;
   double stage_dto = -1.0;
+  // device staging for host transfers of point fields (pd_set_state, pd_get_field): grown on
+  // demand and kept, so that a state upload or a field read allocates nothing
+  void* xfer = nullptr;
+  size_t xfer_bytes = 0;
 };
 
 template <class T>

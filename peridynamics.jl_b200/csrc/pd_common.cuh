@@ -182,7 +182,8 @@ __device__ __forceinline__ void clear_bit(unsigned int* bits, long long b) {
   const int cnt = valid ? (int)(d.off[i + 1] - d.off[i]) : 0;
 
 // ---------------------------------------------------------------------------------------
-// compensated (Kahan-Babuska / Neumaier) FP32 accumulation and its lane-group reduction
+// compensated (Kahan) FP32 accumulation and its lane-group reduction (partners combined with
+// TwoSum)
 // ---------------------------------------------------------------------------------------
 struct KSum {
   float s, c;

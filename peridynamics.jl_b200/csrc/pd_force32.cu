@@ -5,7 +5,7 @@
 //   eta = xi + du                       deformed bond vector from the stored FP32 offset xi
 //   l   = |eta|
 //   e   = l - L = (2 xi.du + du.du) / (l + L)   (no cancellation at stretches ~1e-4)
-// Per-point sums use Neumaier-compensated FP32 accumulation and a fixed-order compensated
+// Per-point sums use Kahan-compensated FP32 accumulation and a fixed-order compensated
 // reduction over the G lanes of a point, so results are deterministic.
 //
 // The state-based materials run in gather form (phase A per point, phase B per point reading

@@ -62,6 +62,16 @@ __device__ __forceinline__ float omega_r(int kernel, float delta, float L, float
   return omega_of_f(kernel, delta, L);
 }
 
+// LIN: the reference's default linear kernel delta / L chosen at compile time. The phase-A
+// kernels instantiate it: without the general form's code per bond, OSB phase A took 3 % and
+// CMat phase A 5.6 % less time on the 1M-point blocks (the same values bit for bit). Phase B
+// keeps the general form, which measured faster there.
+template <bool LIN>
+__device__ __forceinline__ float omega_t(int kernel, float delta, float L, float rL) {
+  if constexpr (LIN) return delta * rL;
+  else return omega_r(kernel, delta, L, rL);
+}
+
 __device__ __forceinline__ void flag_nan32(const DevBody& d, int kstep, float x, float y, float z) {
   if (isnan(x) || isnan(y) || isnan(z)) {
     long long step = d.ctrl->base + kstep;
@@ -380,7 +390,7 @@ __global__ void PD_LB k_osb_b32(DevBody d, int kstep) {
 #ifndef PD_MINB_UB
 #define PD_MINB_UB 4
 #endif
-template <int G, bool ESC, bool FULLM>
+template <int G, bool ESC, bool FULLM, bool LIN>
 __global__ void __launch_bounds__(256, PD_MINB_UA) k_osb_a32u(DevBody d, int kstep) {
   if (d.ctrl->err) return;
   PD_SLICE_LOOP(G) {
@@ -416,12 +426,12 @@ __global__ void __launch_bounds__(256, PD_MINB_UA) k_osb_a32u(DevBody d, int kst
         bond32(u ? g1 : g0, hi, lo, hj, u ? lj1 : lj0, B);
         const bool act = (((u ? w1 : w0) >> lane) & 1u) && !fails32(B, epsc);
         if (act) {
-          float om = omega_r(d.kernel, delta, B.L, B.rL) * hj.w;
+          float om = omega_t<LIN>(d.kernel, delta, B.L, B.rL) * hj.w;
           if (ESC) om *= u ? s1 : s0;
           if (FULLM) m.add(om * (B.gx * B.gx + B.gy * B.gy + B.gz * B.gz));
           th.add(om * B.L * B.e);
         } else if (!FULLM && (((u ? w1 : w0) >> lane) & 1u)) {  // breaks now (see k_osb_a32)
-          float om = omega_r(d.kernel, delta, B.L, B.rL) * hj.w;
+          float om = omega_t<LIN>(d.kernel, delta, B.L, B.rL) * hj.w;
           if (ESC) om *= u ? s1 : s0;
           dm += om * (B.gx * B.gx + B.gy * B.gy + B.gz * B.gz);
         }
@@ -606,7 +616,7 @@ __device__ void pk1_32(int cmodel, const DevParam& p, const float* H, float* P) 
 #ifndef PD_MINB_CAI
 #define PD_MINB_CAI 3
 #endif
-template <int G, bool FULLK>
+template <int G, bool FULLK, bool LIN>
 __global__ void __launch_bounds__(256, FULLK ? PD_MINB_CA : PD_MINB_CAI) k_c_a32(DevBody d, int kstep) {
   if (d.ctrl->err) return;
   PD_SLICE_LOOP(G) {
@@ -642,7 +652,7 @@ __global__ void __launch_bounds__(256, FULLK ? PD_MINB_CA : PD_MINB_CAI) k_c_a32
         bond32(g, hi, lo, hj, lj, B);
         act = ((word >> lane) & 1u) && !fails32(B, epsc);
         if (act) {
-          const float t = omega_r(d.kernel, P.deltaf, B.L, B.rL) * hj.w * vs;
+          const float t = omega_t<LIN>(d.kernel, P.deltaf, B.L, B.rL) * hj.w * vs;
           const float X[3] = {B.gx * id, B.gy * id, B.gz * id};
           const float U[3] = {B.dux * id, B.duy * id, B.duz * id};
           if constexpr (FULLK) {
@@ -655,7 +665,7 @@ __global__ void __launch_bounds__(256, FULLK ? PD_MINB_CA : PD_MINB_CAI) k_c_a32
             for (int q = 0; q < 3; q++) Hs[q + 3 * c].add(t * U[q] * X[c]);
         } else if (!FULLK && ((word >> lane) & 1u)) {
           // the bond breaks now: its term leaves the stored shape tensor
-          const float t = omega_r(d.kernel, P.deltaf, B.L, B.rL) * hj.w * vs;
+          const float t = omega_t<LIN>(d.kernel, P.deltaf, B.L, B.rL) * hj.w * vs;
           const float X[3] = {B.gx * id, B.gy * id, B.gz * id};
           dK[0] += t * X[0] * X[0]; dK[1] += t * X[1] * X[1]; dK[2] += t * X[2] * X[2];
           dK[3] += t * X[0] * X[1]; dK[4] += t * X[0] * X[2]; dK[5] += t * X[1] * X[2];
@@ -863,8 +873,14 @@ static int launch_osb32(const DevBody& d, const LaunchCfg& c, int G, int grid, i
   int launches = 0;
   if (c.pipe == 4) {
     if (A) {
-      if (c.fullk) { PD_DISPATCH_G(G, (k_osb_a32u<GG, ESC, true><<<grid, c.block, 0, s>>>(d, kstep))); }
-      else { PD_DISPATCH_G(G, (k_osb_a32u<GG, ESC, false><<<grid, c.block, 0, s>>>(d, kstep))); }
+      if (d.kernel == KER_LINEAR) {
+        if (c.fullk) { PD_DISPATCH_G(G, (k_osb_a32u<GG, ESC, true, true><<<grid, c.block, 0, s>>>(d, kstep))); }
+        else { PD_DISPATCH_G(G, (k_osb_a32u<GG, ESC, false, true><<<grid, c.block, 0, s>>>(d, kstep))); }
+      } else if (c.fullk) {
+        PD_DISPATCH_G(G, (k_osb_a32u<GG, ESC, true, false><<<grid, c.block, 0, s>>>(d, kstep)));
+      } else {
+        PD_DISPATCH_G(G, (k_osb_a32u<GG, ESC, false, false><<<grid, c.block, 0, s>>>(d, kstep)));
+      }
       launches++;
     }
     if (B) {
@@ -903,8 +919,14 @@ int launch_force32(const DevBody& d, const LaunchCfg& c, int kstep, int phase, c
     return launch_osb32<false>(d, c, G, grid, kstep, A, B, s);
   }
   if (A) {
-    if (c.fullk) { PD_DISPATCH_G(G, (k_c_a32<GG, true><<<grid, c.block, 0, s>>>(d, kstep))); }
-    else { PD_DISPATCH_G(G, (k_c_a32<GG, false><<<grid, c.block, 0, s>>>(d, kstep))); }
+    if (d.kernel == KER_LINEAR) {
+      if (c.fullk) { PD_DISPATCH_G(G, (k_c_a32<GG, true, true><<<grid, c.block, 0, s>>>(d, kstep))); }
+      else { PD_DISPATCH_G(G, (k_c_a32<GG, false, true><<<grid, c.block, 0, s>>>(d, kstep))); }
+    } else if (c.fullk) {
+      PD_DISPATCH_G(G, (k_c_a32<GG, true, false><<<grid, c.block, 0, s>>>(d, kstep)));
+    } else {
+      PD_DISPATCH_G(G, (k_c_a32<GG, false, false><<<grid, c.block, 0, s>>>(d, kstep)));
+    }
     launches++;
   }
   if (B) { PD_DISPATCH_G(G, (k_c_b32<GG><<<grid, c.block, 0, s>>>(d, kstep))); launches++; }

@@ -854,9 +854,16 @@ extern "C" pd_status pd_set_bcs(pd_handle* h, int32_t n_bcs, const pd_bc_desc* b
   PD_CUDA(cudaStreamSynchronize(h->stream));
   // free the previous lists
   dfree(h, (void*)h->bc.point); dfree(h, (void*)h->bc.entry_off); dfree(h, (void*)h->bc.entry);
-  dfree(h, (void*)h->bc.info); dfree(h, (void*)h->bc.data);
+  dfree(h, (void*)h->bc.info); dfree(h, (void*)h->bc.data); dfree(h, (void*)h->bc.slot);
   h->bc = BCDev{};
   h->bc.table = h->table;
+  // the position of every constrained point in the condition list (-1: none)
+  std::vector<int> slot(n, -1);
+  for (size_t p = 0; p < pts.size(); p++) slot[pts[p]] = (int)p;
+  int* ds = nullptr;
+  PD_TRY(dalloc(h, &ds, n));
+  if (n > 0) PD_CUDA(cudaMemcpy(ds, slot.data(), sizeof(int) * n, cudaMemcpyHostToDevice));
+  h->bc.slot = ds;
   int *dp = nullptr, *de = nullptr;
   BCEntry* den = nullptr;
   BCInfo* di = nullptr;
@@ -999,9 +1006,8 @@ static void issue_steps(pd_handle* h, int steps, double dto, std::vector<cudaEve
   auto rec = [&]() { if (ev) cudaEventRecord((*ev)[e++], h->stream); };
   for (int k = 0; k < steps; k++) {
     rec();
-    launch_kick_drift(h->d, h->g, k == 0 ? 0 : 1, dto, k, h->stream);
+    launch_kick_drift(h->d, h->g, h->bc, k == 0 ? 0 : 1, dto, k, h->stream);
     h->launches++;
-    if (h->bc.n_points > 0) { launch_bc(h->d, h->g, h->bc, dto, k, h->stream); h->launches++; }
     rec();
     launch_force(h, k, 1);
     rec();

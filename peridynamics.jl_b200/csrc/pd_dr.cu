@@ -244,12 +244,8 @@ static void dr_issue(pd_handle* h, long long first_step, long long n_steps, cuda
   for (long long k = 0; k < n_steps; k++) {
     const long long step = first_step + k;
     if (ev) cudaEventRecord(ev[3 * k], h->stream);
-    launch_kick_drift(h->d, h->g, 2, dt, (int)k, h->stream);
+    launch_kick_drift(h->d, h->g, h->bc, 2, dt, (int)k, h->stream);
     h->launches++;
-    if (h->bc.n_points > 0) {
-      launch_bc(h->d, h->g, h->bc, dt, (int)k, h->stream);
-      h->launches++;
-    }
     if (ev) cudaEventRecord(ev[3 * k + 1], h->stream);
     pd_launch_force(h, (int)k, 0);
     if (ev) cudaEventRecord(ev[3 * k + 2], h->stream);

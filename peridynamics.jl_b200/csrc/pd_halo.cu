@@ -213,12 +213,8 @@ extern "C" pd_status pd_vv_stage(pd_handle* h, int32_t stage, int64_t kstep) {
   const int k = (int)kstep;
   switch (stage) {
     case 0:
-      launch_kick_drift(h->d, h->g, k == 0 ? 0 : 1, h->stage_dto, k, h->stream);
+      launch_kick_drift(h->d, h->g, h->bc, k == 0 ? 0 : 1, h->stage_dto, k, h->stream);
       h->launches++;
-      if (h->bc.n_points > 0) {
-        launch_bc(h->d, h->g, h->bc, h->stage_dto, k, h->stream);
-        h->launches++;
-      }
       break;
     case 1:
       pd_launch_force(h, k, 1);

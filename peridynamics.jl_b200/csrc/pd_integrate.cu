@@ -5,11 +5,11 @@
 // One step n of the reference (velocity_verlet.jl:181-197, 239-295) is
 //   v_half = v + a dt/2;  BC(t_n);  u += v_half dt, x += v_half dt;  force(t_n);
 //   a = (b_int + b_ext) / rho;  v = v_half + a dt/2.
-// The device runs it as [kick-drift] [boundary conditions] [force]: the kick-drift kernel of
-// step n computes a_{n-1} and v_{n-1} in registers from the previous force (or reads the
-// stored v, a at the start of a run), writes v_half_n and moves every point without
-// conditions; the condition kernel overwrites v_half / b_ext of the constrained points and
-// moves them; a finish kernel stores a and v after the last force of a run. The stored state
+// The device runs it as [kick-drift with conditions] [force]: the kick-drift kernel of step n
+// computes a_{n-1} and v_{n-1} in registers from the previous force (or reads the stored v, a
+// at the start of a run), forms v_half_n, applies the point's conditions at t_n (v_half / b_ext
+// components of a constrained point, found through the condition slot of the point) and moves
+// the point; a finish kernel stores a and v after the last force of a run. The stored state
 // between runs is exactly the reference's (v, a, v_half, u, x).
 #include "pd_common.cuh"
 #include "pd_launch.h"
@@ -46,7 +46,7 @@ __global__ void k_split_u(DevBody d) {
   split_u(d, i, d.cur[i]);
 }
 
-__global__ void k_kick_drift(DevBody d, IntDev g, int mode, double dt_override, int kstep) {
+__global__ void k_kick_drift(DevBody d, IntDev g, BCDev bc, int mode, double dt_override, int kstep) {
   if (d.ctrl->err) return;
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= d.n) return;
@@ -72,39 +72,34 @@ __global__ void k_kick_drift(DevBody d, IntDev g, int mode, double dt_override, 
     }
     g.vh[q] = vh[k];
   }
-  if (!(meta & META_HAS_BC)) drift(d, g, i, vh, dt);
-}
-
-// apply_boundary_conditions! (boundary_conditions.jl:37-51, 98-108, 198-226) at t = n dt for
-// the constrained points, then their update_disp_and_pos!
-__global__ void k_bc(DevBody d, IntDev g, BCDev bc, double dt_override, int kstep) {
-  if (d.ctrl->err) return;
-  const int p = blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= bc.n_points) return;
-  const long long i = bc.point[p];
-  const long long step = d.ctrl->base + kstep;
-  const long long row = step - d.ctrl->table_first;
-  const DevParam& P = d.params[d.meta[i] & META_PID_MASK];
-  const double dt = dt_override > 0 ? dt_override : P.dt;
-  for (int e = bc.entry_off[p]; e < bc.entry_off[p + 1]; e++) {
-    const BCEntry en = bc.entry[e];
-    const BCInfo in = bc.info[en.bc];
-    double v;
-    if (in.kind == 2) {
-      v = bc.data[in.col + en.q];
-    } else {
-      if (row < 0 || row >= d.ctrl->table_n) {
-        atomicExch(&d.ctrl->err, 2);
-        d.ctrl->err_step = step;
-        return;
+  if (meta & META_HAS_BC) {
+    // apply_boundary_conditions! (boundary_conditions.jl:37-51, 98-108, 198-226) at t = n dt
+    const int p = bc.slot[i];
+    const long long step = d.ctrl->base + kstep;
+    const long long row = step - d.ctrl->table_first;
+    for (int e = bc.entry_off[p]; e < bc.entry_off[p + 1]; e++) {
+      const BCEntry en = bc.entry[e];
+      const BCInfo in = bc.info[en.bc];
+      double v;
+      if (in.kind == 2) {
+        v = bc.data[in.col + en.q];
+      } else {
+        if (row < 0 || row >= d.ctrl->table_n) {
+          atomicExch(&d.ctrl->err, 2);
+          d.ctrl->err_step = step;
+          return;
+        }
+        v = bc.table[row * bc.per_step + in.col + (in.kind == 1 ? en.q : 0)];
       }
-      v = bc.table[row * bc.per_step + in.col + (in.kind == 1 ? en.q : 0)];
+      if (!isfinite(v)) continue;
+      if (in.field == 0) {
+        vh[in.dim] = v;
+        g.vh[3 * i + in.dim] = v;
+      } else {
+        g.bext[3 * i + in.dim] = v;
+      }
     }
-    if (!isfinite(v)) continue;
-    double* field = in.field == 0 ? g.vh : g.bext;
-    field[3 * i + in.dim] = v;
   }
-  double vh[3] = {g.vh[3 * i], g.vh[3 * i + 1], g.vh[3 * i + 2]};
   drift(d, g, i, vh, dt);
 }
 
@@ -131,15 +126,9 @@ static inline int blocks_for(long long n, int t) {
   return (int)(b < 1 ? 1 : b);
 }
 
-void launch_kick_drift(const DevBody& d, const IntDev& g, int mode, double dt_override, int kstep,
-                       cudaStream_t s) {
-  k_kick_drift<<<blocks_for(d.n, 256), 256, 0, s>>>(d, g, mode, dt_override, kstep);
-}
-
-void launch_bc(const DevBody& d, const IntDev& g, const BCDev& bc, double dt_override, int kstep,
-               cudaStream_t s) {
-  if (bc.n_points == 0) return;
-  k_bc<<<blocks_for(bc.n_points, 128), 128, 0, s>>>(d, g, bc, dt_override, kstep);
+void launch_kick_drift(const DevBody& d, const IntDev& g, const BCDev& bc, int mode,
+                       double dt_override, int kstep, cudaStream_t s) {
+  k_kick_drift<<<blocks_for(d.n, 256), 256, 0, s>>>(d, g, bc, mode, dt_override, kstep);
 }
 
 void launch_split_u(const DevBody& d, cudaStream_t s) {

@@ -29,6 +29,7 @@ struct BCEntry {
 struct BCDev {
   int n_points;          // points that carry conditions
   const int* point;      // [n_points]
+  const int* slot;       // [n]: position of the point in point[] (read for flagged points only)
   const int* entry_off;  // [n_points + 1]
   const BCEntry* entry;
   const BCInfo* info;
@@ -55,12 +56,11 @@ bool tma_supported(const DevBody& d);
 int launch_force32_tma(const DevBody& d, int pipe, int kstep, int phase, cudaStream_t s);
 void launch_cauchy64(const DevBody& d, const double* F, int from_h32, double* out, cudaStream_t s);
 
-// integration: mode 0 = kick from the stored (v, a), mode 1 = kick from the last force,
-// mode 2 = no kick (dynamic relaxation: drift with the stored v_half)
-void launch_kick_drift(const DevBody& d, const IntDev& g, int mode, double dt_override, int kstep,
-                       cudaStream_t s);
-void launch_bc(const DevBody& d, const IntDev& g, const BCDev& bc, double dt_override, int kstep,
-               cudaStream_t s);
+// integration with the boundary conditions, one launch per step: mode 0 = kick from the stored
+// (v, a), mode 1 = kick from the last force, mode 2 = no kick (dynamic relaxation: drift with
+// the stored v_half)
+void launch_kick_drift(const DevBody& d, const IntDev& g, const BCDev& bc, int mode,
+                       double dt_override, int kstep, cudaStream_t s);
 void launch_finish(const DevBody& d, const IntDev& g, double dt_override, cudaStream_t s);
 void launch_split_u(const DevBody& d, cudaStream_t s);
 // the split of rows[0 .. n) (halo rows that received a displacement)

@@ -269,7 +269,11 @@ class ClockSampler:
     def __init__(self, index):
         self.index = index
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_{index}.csv")
+        # raw samples: PD_BENCH_CLOCKS_DIR if set, else the temporary directory (the JSON
+        # line carries their summary)
+        import tempfile
+        base = os.environ.get("PD_BENCH_CLOCKS_DIR") or tempfile.gettempdir()
+        self.path = os.path.join(base, f"clocks_{index}.csv")
 
     def __enter__(self):
         try:

@@ -32,6 +32,8 @@ UNIT = "bond-updates/s"
 CONFIGS = {
     # name: (nx, ny, nz, dx, material, random broken fraction, bc velocity)
     "osb8m": (400, 200, 100, 5e-4, "OSB", 0.05, 1.0),
+    # mode-I tensile plate, BBMaterial, 40 x 20 x 4 points (see make_plate)
+    "plate3200": (40, 20, 4, 2.5e-3, "BB", 0.0, 0.6),
     # quasi-static Newton-Krylov: bond-based three-point bending beam (x span, y height)
     "jfnk500k": (250, 50, 40, 1e-3, "BB", 0.0, 0.0),
     "osb1m": (200, 100, 50, 1e-3, "OSB", 0.0, 0.6),
@@ -44,6 +46,8 @@ CONFIGS = {
     # dynamic relaxation of an OSB block in uniform tension (see make_dr_block)
     "dr1m": (200, 100, 50, 1e-3, "OSB", 0.0, 0.0),
 }
+# configs of one body (the multi-GPU run partitions them; --replicas runs copies instead)
+SINGLE_BODY = ("osb8m", "plate3200", "osb1m", "bb1m", "c1m")
 DR_STRAIN = 5e-5
 # algorithmic bytes per point of the damping and velocity-update kernels of one relaxation step
 # (damping: u, v_half, b_int, b_int_old, v_half_old, Lambda; update: Lambda, b_int, b_ext,
@@ -78,6 +82,10 @@ def load_peaks():
 def make_body(cfg, jitter_seed=None, correction=None):
     import pdcuda as pd
     nx, ny, nz, dx, mat, frac, vbc = CONFIGS[cfg]
+    if cfg == "plate3200":
+        if correction == "energy":
+            raise ValueError("the plate runs without the surface correction")
+        return make_plate(pd.BBMaterial(), nx, ny, nz, dx, v=vbc), frac
     lx, ly, lz = nx * dx, ny * dx, nz * dx
     pos, vol = pd.uniform_box(lx, ly, lz, dx)
     corr = pd.EnergySurfaceCorrection if correction == "energy" else None
@@ -97,6 +105,29 @@ def make_body(cfg, jitter_seed=None, correction=None):
     pd.velocity_bc(lambda t: -vbc, body, "ymin", "y")
     pd.velocity_bc(lambda t: vbc, body, "ymax", "y")
     return body, frac
+
+
+def make_plate(mat, nx=40, ny=20, nz=4, dx=2.5e-3, E=70e9, rho=2700.0, Gc=100.0, v=0.6, nu=None):
+    """Mode-I tensile plate (the defaults: 40 x 20 x 4 points, 3,200, at dx = 2.5 mm, a plate of
+    0.1 x 0.05 x 0.01 m with its corner at the origin), horizon 3.015 dx: bonds crossing
+    x = 0.5 lx for y < 0.2 ly are filtered (precrack! without damage update), the top and
+    bottom two rows are pulled at +-v in y."""
+    import pdcuda as pd
+    lx, ly, lz = nx * dx, ny * dx, nz * dx
+    pos, vol = pd.uniform_box(lx, ly, lz, dx, center=(lx / 2, ly / 2, lz / 2))
+    body = pd.Body(mat, pos, vol)
+    args = dict(horizon=3.015 * dx, rho=rho, E=E, Gc=Gc)
+    if nu is not None:
+        args["nu"] = nu
+    pd.material(body, **args)
+    pd.point_set(body, "crack_a", where=lambda p: (p[0] <= lx / 2) & (p[1] < 0.2 * ly))
+    pd.point_set(body, "crack_b", where=lambda p: (p[0] > lx / 2) & (p[1] < 0.2 * ly))
+    pd.precrack(body, "crack_a", "crack_b", update_dmg=False)
+    pd.point_set(body, "top", where=lambda p: p[1] > ly - 2 * dx)
+    pd.point_set(body, "bottom", where=lambda p: p[1] < 2 * dx)
+    pd.velocity_bc(lambda t: v, body, "top", "y")
+    pd.velocity_bc(lambda t: -v, body, "bottom", "y")
+    return body
 
 
 def make_dr_block(nx, ny, nz, dx, mat="OSB"):
@@ -220,62 +251,184 @@ def run_precision_study(args, local):
     print(json.dumps(line), flush=True)
 
 
+def run_spot_checks(args, local):
+    """--check-every K: the FP32-compensated run of --steps steps (CUDA graphs, timed on the
+    device) with the plain FP64 path of the same body advanced beside it; every K steps the two
+    are compared: displacement and velocity (largest and RMS difference relative to the FP64
+    field), bond states that differ, bonds broken in each, and the bonds within 1e-8 and 1e-12
+    of the critical stretch (FP64 positions)."""
+    import pdcuda as pd
+    body, frac = make_body(args.config)
+    devs = {}
+    for prec in ("fp64", "fp32"):
+        d = pd.DeviceBody(body, precision=prec, device=local)
+        if frac > 0:
+            d.break_random_pairs(frac, 0x5EED)
+        d.autotune()
+        devs[prec] = d
+    d64, d32 = devs["fp64"], devs["fp32"]
+    dt = d32.stable_timestep(0.7)
+    dt64 = d64.stable_timestep(0.7)
+    every = args.check_every
+    d32.set_graph(min(args.graph, every) if args.graph > 0 else 0)
+    for d in (d32, d64):
+        d.force(0.0, dt)
+    n_bonds = d32.info()[1]
+    active0 = int(np.count_nonzero(d64.field("bond_active")))
+    rel = lambda a, b: float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
+    rms = lambda a, b: float(np.sqrt(((a - b) ** 2).sum() / max((b ** 2).sum(), 1e-300)))
+    checks, ms32, ms64, done = [], 0.0, 0.0, 0
+    with ClockSampler(local) as clk:
+        while done < args.steps:
+            k = min(every, args.steps - done)
+            ms32 += d32.run_timed(done + 1, k, dt, phases=False)
+            ms64 += d64.run_timed(done + 1, k, dt, phases=False)
+            done += k
+            u32, u64 = d32.field("displacement"), d64.field("displacement")
+            v32, v64 = d32.field("velocity"), d64.field("velocity")
+            s32, s64 = d32.field("bond_active"), d64.field("bond_active")
+            checks.append({"step": done,
+                           "displacement": {"max_rel": rel(u32, u64), "rms_rel": rms(u32, u64)},
+                           "velocity": {"max_rel": rel(v32, v64), "rms_rel": rms(v32, v64)},
+                           "broken_in_run": {"fp64": active0 - int(np.count_nonzero(s64)),
+                                             "fp32": active0 - int(np.count_nonzero(s32))},
+                           "states_differ": int(np.count_nonzero(s32 != s64)),
+                           "near_critical_fp64": {"1e-8": d64.near_critical(1e-8),
+                                                  "1e-12": d64.near_critical(1e-12)}})
+            print(json.dumps({"spot_check": checks[-1]}), flush=True)
+    nx, ny, nz, dx, mat, _, vbc = CONFIGS[args.config]
+    line = {"study": "FP32-compensated run with FP64 spot checks (both on the GPU; the FP64 path "
+                     "equals the oracle bit for bit in serial order, to 1e-10 in lane groups)",
+            "workload": f"{args.config}: {mat} {nx}x{ny}x{nz} points, dx={dx}, {frac:.0%} pairs "
+                        f"broken, +-{vbc} m/s on the y faces",
+            "bonds": n_bonds, "steps": args.steps, "check_every": every, "dt": dt,
+            "dt_equal": dt == dt64,
+            "graph_steps": min(args.graph, every) if args.graph > 0 else 0,
+            "fp32": {"ms_per_step": ms32 / args.steps, "bond_updates_per_s": n_bonds * args.steps / (ms32 / 1e3),
+                     "mapping": d32.mapping()},
+            "fp64": {"ms_per_step": ms64 / args.steps, "bond_updates_per_s": n_bonds * args.steps / (ms64 / 1e3),
+                     "mapping": d64.mapping()},
+            "checks": checks, "clocks": clk.summary()}
+    print(json.dumps(line), flush=True)
+    d32.close()
+    d64.close()
+
+
 def run_ensemble(args, rank, world, local, dist):
     """--config ens64: all specimens advanced together, every one with its own CFL step; one
-    step = one Velocity Verlet step of every specimen. Ranks own disjoint specimen sets
-    (replicas: no exchange)."""
+    step = one Velocity Verlet step of every specimen. The specimens are cut into --ens-classes
+    size classes, each one device body with its own autotuned mapping, all advanced by one CUDA
+    graph. Ranks own disjoint specimen sets (replicas: no exchange)."""
     import pdcuda as pd
     from pdcuda.replicas import partition_specimens, reduce_max, reduce_sum
     bodies = make_ensemble()
     mine = partition_specimens([b.n_points for b in bodies], world)[rank]
+    gsteps = min(args.graph if args.graph else 50, args.steps)
     t0 = time.perf_counter()
     ens = pd.Ensemble([bodies[k] for k in mine], precision=args.precision, device=local,
-                      graph_steps=args.graph if args.graph else 50)
+                      graph_steps=gsteps, classes=args.ens_classes)
     setup_s = time.perf_counter() - t0
-    g, b = ens.dev.autotune()
-    mapping = ens.dev.mapping()
-    if args.graph:
-        ens.dev.set_graph(args.graph)
+    ens.autotune()
     ens.run(args.warmup)
-    n_pts, n_bonds, _ = ens.dev.info()
+    step = args.warmup + 1
+    ens.run(gsteps, first_step=step)   # untimed: captures the graph of the timed blocks
+    step += gsteps
+    n_pts, n_bonds = ens.info()
+    launches0 = ens.launch_count()
     if dist:
         dist.barrier()
     with ClockSampler(local) as clk:
-        ms, a, bph, integ = ens.run_timed(args.warmup + 1, args.steps)
+        ms = ens.run_timed(step, args.steps, phases=False)
+        step += args.steps
+        launches = ens.launch_count() - launches0
+        # per-kernel durations: every class alone for the same number of steps, eagerly
+        per_class = ens.class_phase_times(step, args.steps)
+        step += args.steps
     ms_max = reduce_max(ms, dist, f"cuda:{local}")
     bonds_all = reduce_sum(n_bonds, dist, f"cuda:{local}")
     value = bonds_all * args.steps / (ms_max / 1e3)
+    classes = ens.class_info()
+    for c, t in zip(classes, per_class):
+        c["ms_per_step_alone"] = {"total": t[0] / args.steps, "phase_a": t[1] / args.steps,
+                                  "phase_b": t[2] / args.steps, "integrate": t[3] / args.steps}
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None,
                 "dtype": "f32" if args.precision == "fp32" else "f64", "data": "synthetic",
                 "config": {"workload": "ens64: 64 CMat NeoHooke specimens of 20k-200k points (seeded), "
-                                       "edge cracks, +-0.6 m/s, own CFL step each, one device body",
+                                       "edge cracks, +-0.6 m/s, own CFL step each, size classes in "
+                                       "one CUDA graph",
                            "specimens": len(mine), "points": n_pts, "bonds": n_bonds,
-                           "mapping": dict(zip(("group", "block", "pipe"), mapping)),
-                           "graph_steps": args.graph if args.graph else 50,
+                           "classes": classes, "graph_steps": gsteps,
                            "setup_s": setup_s, "parallelism": f"replicas x{world}"},
-                "ms": {"phase_a": a / args.steps, "phase_b": bph / args.steps,
-                       "integrate": integ / args.steps},
-                "clocks": clk.summary()}
+                "ms": {"phase_a": sum(t[1] for t in per_class) / args.steps,
+                       "phase_b": sum(t[2] for t in per_class) / args.steps,
+                       "integrate": sum(t[3] for t in per_class) / args.steps,
+                       "note": "per-kernel sums of the classes run alone, eagerly"},
+                "gpu_launches": launches, "clocks": clk.summary()}
         print(json.dumps(line), flush=True)
     ens.close()
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    """SM clock and clock-event reasons sampled during the timed region.
 
-    def __init__(self, index):
-        self.index = index
-        self.proc = None
-        # raw samples: PD_BENCH_CLOCKS_DIR if set, else the temporary directory (the JSON
-        # line carries their summary)
+    NVML is polled every 10 ms from a thread, so that a timed region of a fraction of a second
+    still gets a dozen samples; nvidia-smi at its 200 ms period is the fallback. The raw
+    samples go to PD_BENCH_CLOCKS_DIR if set, else the temporary directory (the JSON line
+    carries their summary)."""
+
+    REASONS = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+
+    def __init__(self, index, period_s=0.01):
         import tempfile
+        self.index = index
+        self.period = period_s
+        self.proc = None
+        self.thread = None
+        self.rows = []        # (sm_mhz, max_mhz, power_w, reasons tuple)
+        self.source = None
         base = os.environ.get("PD_BENCH_CLOCKS_DIR") or tempfile.gettempdir()
         self.path = os.path.join(base, f"clocks_{index}.csv")
 
+    def _nvml_handle(self):
+        import pynvml as N
+        N.nvmlInit()
+        try:   # the NVML device of this CUDA device (CUDA_VISIBLE_DEVICES may renumber)
+            import torch
+            uuid = str(torch.cuda.get_device_properties(self.index).uuid)
+            return N, N.nvmlDeviceGetHandleByUUID(uuid if uuid.startswith("GPU-") else "GPU-" + uuid)
+        except Exception:
+            return N, N.nvmlDeviceGetHandleByIndex(self.index)
+
+    def _poll(self, N, h):
+        import threading
+        bits = (N.nvmlClocksEventReasonHwSlowdown, N.nvmlClocksEventReasonHwThermalSlowdown,
+                N.nvmlClocksEventReasonSwThermalSlowdown, N.nvmlClocksEventReasonSwPowerCap)
+        mx = float(N.nvmlDeviceGetMaxClockInfo(h, N.NVML_CLOCK_SM))
+        while not self.stop.is_set():
+            try:
+                sm = float(N.nvmlDeviceGetClockInfo(h, N.NVML_CLOCK_SM))
+                r = N.nvmlDeviceGetCurrentClocksEventReasons(h)
+                pw = N.nvmlDeviceGetPowerUsage(h) / 1000.0
+                self.rows.append((sm, mx, pw, tuple(nm for b, nm in zip(bits, self.REASONS) if r & b)))
+            except Exception:
+                pass
+            self.stop.wait(self.period)
+        assert isinstance(self.stop, threading.Event)
+
     def __enter__(self):
+        import threading
+        try:
+            N, h = self._nvml_handle()
+            self.stop = threading.Event()
+            self.thread = threading.Thread(target=self._poll, args=(N, h), daemon=True)
+            self.thread.start()
+            self.source = "nvml 10 ms"
+            return self
+        except Exception:
+            self.thread = None
         try:
             os.makedirs(os.path.dirname(self.path), exist_ok=True)
             self.f = open(self.path, "w")
@@ -286,11 +439,22 @@ class ClockSampler:
                  "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
                  "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
                 stderr=subprocess.DEVNULL)
+            self.source = "nvidia-smi 200 ms"
         except Exception:
             self.proc = None
         return self
 
     def __exit__(self, *a):
+        if self.thread is not None:
+            self.stop.set()
+            self.thread.join(timeout=5)
+            try:
+                os.makedirs(os.path.dirname(self.path), exist_ok=True)
+                with open(self.path, "w") as f:
+                    for sm, mx, pw, rs in self.rows:
+                        f.write(f"{sm},{mx},{pw},{'|'.join(rs)}\n")
+            except Exception:
+                pass
         if self.proc is not None:
             self.proc.terminate()
             try:
@@ -298,22 +462,36 @@ class ClockSampler:
             except Exception:
                 self.proc.kill()
             self.f.close()
+            try:
+                for r in open(self.path).read().strip().splitlines():
+                    r = r.split(",")
+                    self.rows.append((float(r[1]), float(r[2]), float(r[3]),
+                                      tuple(nm for k, nm in enumerate(self.REASONS)
+                                            if r[5 + k].strip() == "Active")))
+            except Exception:
+                pass
 
     def summary(self):
-        try:
-            rows = [r.split(",") for r in open(self.path).read().strip().splitlines()]
-            sm = [float(r[1]) for r in rows]
-            mx = float(rows[0][2])
-            reasons = set()
-            names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-            for r in rows:
-                for k, nm in enumerate(names):
-                    if r[5 + k].strip() == "Active":
-                        reasons.add(nm)
-            return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons),
-                    "samples": len(sm)}
-        except Exception as e:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "error": str(e)}
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0,
+                    "source": self.source}
+        sm = [r[0] for r in self.rows]
+        reasons = sorted({nm for r in self.rows for nm in r[3]})
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": self.rows[0][1], "reasons": reasons,
+                "samples": len(sm), "sm_mhz_min": min(sm), "power_w_max": max(r[2] for r in self.rows),
+                "source": self.source}
+
+
+def cpu_model():
+    """The host CPU's model name (/proc/cpuinfo)."""
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except Exception:
+        pass
+    import platform
+    return platform.processor() or "unknown"
 
 
 def oracle_sample(cfg, threads):
@@ -338,9 +516,32 @@ def oracle_sample(cfg, threads):
     return b, dt, (sx, sy, sz)
 
 
-def cpu_baseline(cfg, threads, budget_s=15.0, correction="none"):
+def plate_oracle(threads):
+    """The oracle twin of the mode-I plate (all of it), its CFL step and its conditions."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    from twin import oracle_bcs, oracle_body
+    body, _ = make_body("plate3200")
+    O.set_threads(threads)
+    ob = oracle_body(body)
+    dt = ob.stable_timestep(0.7)
+    ob.force_density(0.0, dt)
+    return ob, dt, lambda first, n: oracle_bcs(body, first, n, dt)
+
+
+def cpu_baseline(cfg, threads, budget_s=15.0, correction="none", steps=500):
     """bond-updates/s of the oracle sample over whole Velocity Verlet steps (a run of about
-    budget_s seconds)."""
+    budget_s seconds); the plate runs whole (all its points, `steps` steps)."""
+    if cfg == "plate3200":
+        ob, dt, bcs = plate_oracle(threads)
+        table = bcs(1, steps)
+        t0 = time.perf_counter()
+        ob.run_vv(1, steps, dt, table)
+        el = time.perf_counter() - t0
+        return {"value": ob.n_bonds * steps / el, "unit": UNIT, "cores": threads,
+                "cpu_model": cpu_model(), "kind": "port",
+                "sample": f"the whole job: {ob.n} points, {ob.n_bonds} bonds, {steps} FP64 VV "
+                          f"steps in {el:.2f} s"}
     b, dt, (sx, sy, sz) = oracle_sample(cfg, threads)
     if correction == "energy":
         b.init_surface_correction()
@@ -351,7 +552,7 @@ def cpu_baseline(cfg, threads, budget_s=15.0, correction="none"):
         el = time.perf_counter() - t0
         if el > budget_s or steps >= 5000:
             break
-    return {"value": b.n_bonds * steps / el, "unit": UNIT, "cores": threads, "kind": "port",
+    return {"value": b.n_bonds * steps / el, "unit": UNIT, "cores": threads, "cpu_model": cpu_model(), "kind": "port",
             "sample": f"{sx}x{sy}x{sz} sub-block ({b.n} points, {b.n_bonds} bonds) of the same "
                       f"lattice and parameters, {steps} FP64 VV steps in {el:.1f} s"}
 
@@ -393,7 +594,7 @@ def dr_cpu_baseline(cfg, threads, budget_s=15.0):
         el = time.perf_counter() - t0
         if el > budget_s or steps >= 5000:
             break
-    return {"value": b.n_bonds * steps / el, "unit": UNIT, "cores": threads, "kind": "port",
+    return {"value": b.n_bonds * steps / el, "unit": UNIT, "cores": threads, "cpu_model": cpu_model(), "kind": "port",
             "sample": f"{sx}x{sy}x{sz} sub-block ({b.n} points, {b.n_bonds} bonds) of the same "
                       f"lattice, parameters and loading, {steps} FP64 relaxation steps in {el:.1f} s "
                       f"(force on all threads, damping sums in numpy)"}
@@ -534,6 +735,35 @@ def run_halo(args, rank, world, local, dist):
     body_bonds = reduce_sum(owned_bonds, dist, f"cuda:{local}")
     value = body_bonds * args.steps / (ms_max / 1e3)
     mapping = [dict(zip(("group", "block", "pipe"), p.dev.mapping())) for p in parts]
+    step = args.warmup + 1 + args.steps
+
+    # roofline of the dominant kernel on this process's partitions: the second force kernel
+    # (state-based) or the only one (BB), algorithmic bytes of the bonds and rows it sweeps
+    prec = args.precision
+    dom = "force_b" if "force_b" in ms else "force_a"
+    pt_bytes = {"fp32": 32 + 8 + 16 + 12 + 4, "fp64": 64 + 8 + 32 + 24 + 4}[prec]
+    alg = all_bonds * B_BOND[prec] + rows * pt_bytes
+    dom_ms = ms[dom] / args.steps
+    peak, peak_kind = load_peaks()
+    achieved = alg / (dom_ms / 1e3) / 1e9
+
+    # end to end through the public API with host buffers: every partition's state uploaded
+    # from page-locked host memory, the steps, its owned displacement and damage read back
+    bufs = [(pinned(len(p.rows), 3), pinned(len(p.rows), 3)) for p in parts]
+    for p, (hu, hv) in zip(parts, bufs):
+        p.dev.set_state(displacement=hu[1], velocity=hv[1])
+    pb.run(step, max(args.warmup, 3), dt)
+    step += max(args.warmup, 3)
+    if dist:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for p, (hu, hv) in zip(parts, bufs):
+        p.dev.set_state(displacement=hu[1], velocity=hv[1])
+    pb.run(step, args.steps, dt)
+    back = [(p.owned_field("displacement"), p.owned_field("damage")) for p in parts]
+    e2e_s = reduce_max(time.perf_counter() - t0, dist, f"cuda:{local}")
+    h2d = reduce_sum(sum(hu[1].nbytes + hv[1].nbytes for hu, hv in bufs), dist, f"cuda:{local}")
+    d2h = reduce_sum(sum(u.nbytes + d.nbytes for u, d in back), dist, f"cuda:{local}")
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -548,6 +778,13 @@ def run_halo(args, rank, world, local, dist):
             "halo": {"ms_per_step": {k: v / args.steps for k, v in ms.items()},
                      "rows_here": rows, "halo_rows_here": halo_rows,
                      "bonds_here": all_bonds, "owned_bonds_here": owned_bonds},
+            "roofline": {"bound": "hbm", "kernel": f"{mat.lower()} {dom} (rank 0's partitions)",
+                         "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": None, "peak_kind": peak_kind,
+                         "alg_bytes_per_launch": alg, "ms_per_launch": dom_ms},
+            "e2e": {"value": body_bonds * args.steps / e2e_s, "unit": UNIT,
+                    "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps},
+            "cpu_baseline": None,
             "gpu_launches": launches, "clocks": clk.summary(),
         }
         print(json.dumps(line), flush=True)
@@ -563,6 +800,11 @@ def run_reference(args, rank, world):
     if args.config == "dr1m":
         b, dr, bcs, (sx, sy, sz) = dr_oracle_sample(args.config, threads)
         step = lambda n: dr.step(n, bcs)
+    elif args.config == "plate3200":
+        b, dt, bcs = plate_oracle(threads)
+        table = bcs(1, max(args.warmup, 0) + args.steps)
+        step = lambda n: b.run_vv(n, 1, dt, table)   # the table starts at step 1
+        sx, sy, sz = CONFIGS["plate3200"][:3]
     else:
         b, dt, (sx, sy, sz) = oracle_sample(args.config, threads)
         step = lambda n: b.run_vv(n, 1, dt)
@@ -583,7 +825,7 @@ def run_reference(args, rank, world):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic", "impl": "reference",
             "config": {"workload": args.config, "points": nx * ny * nz, "material": mat},
-            "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "cpu_model": cpu_model(), "kind": "port",
                              "sample": sample},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
             "note": "Julia is not installed: the reference arm is the CPU restatement of the "
@@ -715,9 +957,8 @@ def jfnk_cpu_baseline(force_evals, budget_s=20.0):
     """The oracle's FP64 force evaluation (all host threads) on the same beam, timed on a few
     evaluations; the projection multiplies by the block-Jacobi arm's force-evaluation count."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    sys.path.insert(0, os.path.join(ROOT, "tests"))
     import oracle as O
-    from helpers import oracle_body
+    from twin import oracle_body
     from pdcuda.train_preconditioner import bending_beam
     threads = os.cpu_count() or 1
     O.set_threads(threads)
@@ -727,7 +968,7 @@ def jfnk_cpu_baseline(force_evals, budget_s=20.0):
         ob.force_density()
         k += 1
     per = (time.perf_counter() - t0) / k
-    return {"value": per, "unit": "s per force evaluation", "cores": threads, "kind": "port",
+    return {"value": per, "unit": "s per force evaluation", "cores": threads, "cpu_model": cpu_model(), "kind": "port",
             "sample": f"{k} FP64 force evaluations of the 500k-point beam",
             "projected_block_jacobi_s": per * force_evals}
 
@@ -742,14 +983,23 @@ def main():
     ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
     ap.add_argument("--fp64-steps", type=int, default=-1, help="steps of the FP64 comparison (0 = skip)")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--graph", type=int, default=0)
+    ap.add_argument("--graph", type=int, default=50,
+                    help="steps per CUDA graph of the timed Velocity Verlet run (0: eager)")
+    ap.add_argument("--replicas", action="store_true",
+                    help="with --gpus N > 1 on a single-body config: N independent copies of the "
+                         "body (weak scaling) instead of one body in N partitions")
+    ap.add_argument("--ens-classes", type=int, default=3,
+                    help="ens64: size classes of specimens, each with its own mapping")
+    ap.add_argument("--check-every", type=int, default=0,
+                    help="FP32 run of --steps steps compared with an FP64 run of the same body "
+                         "every this many steps (spot checks; prints a precision line)")
     ap.add_argument("--correction", default="none", choices=["none", "energy"],
                     help="BB / OSB with EnergySurfaceCorrection")
     ap.add_argument("--halo", action="store_true",
                     help="one body in partitions with halo exchange (one per rank) instead of replicas")
     ap.add_argument("--halo-parts", type=int, default=1,
                     help="with --halo on one GPU: partitions held by the one process")
-    ap.add_argument("--halo-decomposition", default="index", choices=["index", "slabs"],
+    ap.add_argument("--halo-decomposition", default="slabs", choices=["index", "slabs"],
                     help="index: the reference's contiguous point ranges; slabs: along the longest side")
     ap.add_argument("--jfnk-increments", type=int, default=-1,
                     help="load increments of the JFNK comparison (default: 20 with --config "
@@ -794,6 +1044,16 @@ def main():
     if args.config == "pulse1m":
         if rank == 0 and args.impl == "ours":
             run_precision_study(args, local)
+        if dist:
+            dist.barrier()
+            dist.destroy_process_group()
+        return
+    if (world > 1 and args.impl == "ours" and not args.replicas and not args.halo
+            and args.config in SINGLE_BODY and args.check_every <= 0):
+        args.halo = True     # one body on N GPUs: partitions with halo exchange
+    if args.check_every > 0:
+        if rank == 0 and args.impl == "ours":
+            run_spot_checks(args, local)
         if dist:
             dist.barrier()
             dist.destroy_process_group()
@@ -853,18 +1113,27 @@ def main():
     n_pts, n_bonds, sym = dev.info()
     group, block = dev.autotune()
     dev_mapping = dev.mapping()
-    dev.set_graph(args.graph)
     step = 1
     dev.run(step, args.warmup, dt)
     step += args.warmup
+    # the timed steps run as CUDA graphs of `gsteps` steps; one untimed block captures the graph
+    gsteps = min(args.graph, args.steps) if args.graph > 0 else 0
+    dev.set_graph(gsteps)
+    if gsteps:
+        dev.run(step, gsteps, dt)
+        step += gsteps
 
     peak, peak_kind = load_peaks()
     launches0 = dev.launch_count()
     barrier()
     with ClockSampler(local) as clk:
-        ms_total, ms_a, ms_b, ms_int = dev.run_timed(step, args.steps, dt)
-    step += args.steps
-    launches = dev.launch_count() - launches0
+        ms_total = dev.run_timed(step, args.steps, dt, phases=False)
+        step += args.steps
+        launches = dev.launch_count() - launches0
+        # per-kernel durations for the roofline: the same number of steps again, issued eagerly
+        # with events around every kernel on the handle's stream
+        _, ms_a, ms_b, ms_int = dev.run_timed(step, args.steps, dt)
+        step += args.steps
     barrier()
     ms_max = max_over_ranks(ms_total)
     value = n_bonds * args.steps * world / (ms_max / 1e3)
@@ -917,7 +1186,7 @@ def main():
         # the tuned mapping of the timed run, so that e2e runs the same kernels
         dev.set_mapping(dev_mapping[0], dev_mapping[1])
         dev.set_pipeline(dev_mapping[2])
-        dev.set_graph(args.graph)
+        dev.set_graph(gsteps)
 
     # end to end through the public API with host buffers: upload the state, run, read back
     # (page-locked host buffers)
@@ -925,7 +1194,7 @@ def main():
     h_u, h_v, out_u, out_d = (b[1] for b in bufs)
     # untimed warm-up through the same calls (the rebuilt handle captures its graph here)
     dev.set_state(displacement=h_u, velocity=h_v)
-    dev.run(1, max(args.warmup, 3), dt)
+    dev.run(1, max(args.warmup, 3, gsteps), dt)
     dev.field("displacement", out=out_u)
     barrier()
     t0 = time.perf_counter()
@@ -959,8 +1228,10 @@ def main():
                                    + (", EnergySurfaceCorrection" if args.correction == "energy" else ""),
                        "points": n_pts, "bonds": n_bonds, "precision": prec,
                        "mapping": dict(zip(("group", "block", "pipe"), dev_mapping)),
-                       "symmetric_pairs": bool(sym),
-                       "l2": "inputs larger than L2 (bond arrays of ~19 GB)",
+                       "symmetric_pairs": bool(sym), "graph_steps": gsteps,
+                       "l2": ("inputs larger than L2 (bond arrays of "
+                              f"{n_bonds * B_BOND[prec] / 1e9:.1f} GB)" if n_bonds * B_BOND[prec] > 126e6
+                              else "inputs smaller than L2: the plate job as stated (L2 not flushed)"),
                        "parallelism": f"replicas x{world}"},
             "roofline": {"bound": "hbm", "kernel": f"{mat.lower()} force {dom}",
                          "achieved": achieved, "peak": peak, "unit": "GB/s",
@@ -975,6 +1246,10 @@ def main():
             "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "gpu_launches": launches, "clocks": clocks, "cpu_baseline": cpu,
             "jfnk": jfnk,
+            "timing": ("value: the timed steps as CUDA graphs of graph_steps steps between two "
+                       "events; roofline: the same number of steps issued eagerly with events "
+                       "around every kernel" if gsteps else
+                       "value and roofline: eager launches with events around every kernel"),
         }
         print(json.dumps(line), flush=True)
     if dist:

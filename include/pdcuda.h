@@ -238,10 +238,29 @@ pd_status pd_nan_step(pd_handle *h, int64_t *step);
 /* pd_run_vv with CUDA events on the handle's stream around every kernel (no graph):
  * elapsed milliseconds of the whole run, of the first force kernel (BB: the force kernel;
  * OSB / CMat: phase A), of the second force kernel (OSB / CMat phase B) and of the
- * integration kernels, summed over the steps. Same effect on the state as pd_run_vv. */
+ * integration kernels, summed over the steps. Same effect on the state as pd_run_vv. When
+ * ms_phase_a, ms_phase_b and ms_integrate are all NULL, the steps are issued as pd_run_vv
+ * issues them (CUDA-graph blocks when pd_set_graph is on) and only ms_total is measured,
+ * between two events on the handle's stream. */
 pd_status pd_run_vv_timed(pd_handle *h, int64_t first_step, int64_t n_steps, double dt,
                           double *ms_total, double *ms_phase_a, double *ms_phase_b,
                           double *ms_integrate);
+
+/* Groups of bodies advanced together. No counterpart in the reference, which runs a study's
+ * jobs one after the other (Study / submit!, src/core/study.jl:193-283); here the size classes
+ * of an ensemble, each body with its own mapping (pd_autotune / pd_set_mapping), advance in one
+ * CUDA graph: the launches of every body on its own stream, forked from and joined into the
+ * stream of handles[0]. The bodies share one device and have distinct streams; the group keeps
+ * the handle pointers (destroy the group first). */
+typedef struct pd_group pd_group;
+pd_status pd_group_create(pd_handle *const *handles, int32_t n, pd_group **out);
+/* pd_run_vv for every body of the group (same steps, dt as pd_run_vv: <= 0 takes each
+ * parameter set's step from pd_set_param_timesteps), in CUDA graphs of steps_per_graph steps
+ * (0: eager launches); ms_total (may be NULL): device time of the run on handles[0]'s stream.
+ * Returns after the steps completed; PD_ERR_NAN etc. as pd_run_vv, the first failing body's. */
+pd_status pd_group_run_vv(pd_group *g, int64_t first_step, int64_t n_steps, double dt,
+                          int32_t steps_per_graph, double *ms_total);
+pd_status pd_group_destroy(pd_group *g);
 
 /* Chooses the point-to-lane mapping (points per thread / warp) and block size of the force
  * kernels by timing each candidate on this body. Leaves the state unchanged. */
@@ -256,7 +275,11 @@ pd_status pd_set_mapping(pd_handle *h, int32_t group, int32_t block);
  * the sliced bond arrays staged in shared memory by TMA bulk copies (4 rows x 3 stages,
  * 4 rows x 4 stages, 8 rows x 3 stages per warp; one lane per point, BB or OSB); 4 = direct
  * loads two rows at a time, all their neighbour gathers in flight together (BB, OSB; results
- * identical to 0). pd_autotune times all that apply. */
+ * identical to 0); 5 = OSB with the x and y components of every bond vector in packed FP32
+ * pairs and the bond states selecting instead of branching (one lane per point; phase B
+ * needs symmetric bond states and one parameter set, phase A no surface correction; where
+ * they do not apply the phase runs as 4; same FP32 form, roundings differ from 4 in the
+ * order of a few operations). pd_autotune times all that apply. */
 pd_status pd_set_pipeline(pd_handle *h, int32_t pipe);
 
 /* The current mapping (group 0 = serial order), block size and bond-stream variant. */
@@ -494,17 +517,24 @@ pd_status pd_mpnn_adam(pd_mpnn *net, float lr);
  * on the allocator, or memory carved out of a fixed arena (the reference itself asserts that
  * its force loop allocates nothing, test/perf/perf.jl).
  * Every array is a device pointer owned by the caller, in the reference's CSR bond order
- * (bond lists sorted by neighbour, symmetric, one parameter set): ref_position, position
- * [3n], volume [n], bond_offsets [n+1], neighbors, bond_length, fail_permit [n_bonds];
+ * (every bond list sorted by neighbour, one parameter set): ref_position, position [3n],
+ * volume [n], bond_offsets [n+1], neighbors, bond_length, fail_permit [n_bonds];
  * bond_active [n_bonds] is updated by the failure test; b_int [3n] and n_active [n] are
- * written. Kernels run on `stream` (NULL: the default stream); the call does not wait.
+ * written. Bond states need not agree in the two directions of a pair: the term of
+ * neighbour j on point i uses j's own bond j -> i (its state and length), found by a binary
+ * search of j's sorted list, as the reference's scatter does; a neighbour without a bond to
+ * i adds nothing. Kernels run on `stream` (NULL: the default stream); the call does not
+ * wait. A CUDA error left pending by earlier work of the calling thread is reported
+ * (PD_ERR_CUDA) before anything is launched and stays pending.
  * Limit: n <= 262144 points. The per-point coefficients live in a static device array of
  * that size (8 MiB, held by every GPU that loads the library until the process exits);
  * larger bodies are rejected with PD_ERR_ARG. All calls share that array: calls whose
  * kernels may overlap on the GPU (other streams, other host threads) race. Every entry a
  * call reads is written earlier in the same call, so nothing has to start at zero. The
- * first call on each device looks up the array's device address with that device current;
- * make that first call before any stream capture. Errors: pd_static_last_error(). */
+ * first call in each CUDA context (normally a device's primary context) looks up the
+ * array's device address with that context current and keeps it for the context; make that
+ * first call before any stream capture. A context destroyed and created again at the same
+ * handle (cudaDeviceReset) is not told apart from the old one. Errors: pd_static_last_error(). */
 pd_status pd_osb_force_static(int64_t n, const double *ref_position, const double *position,
                               const double *volume, const int64_t *bond_offsets,
                               const int32_t *neighbors, const double *bond_length,

@@ -83,6 +83,7 @@ def lib():
         L.or_point_params.restype = C.c_int
         L.or_point_params.argtypes = [i32] + [dbl] * 10 + [vp, C.c_char_p, i32]
         L.or_set_threads.argtypes = [i32]
+        L.or_set_serial_order.argtypes = [i32]
         L.or_esc_mfactor.argtypes = [vp, vp, vp]
         L.or_esc_scfactor.argtypes = [vp, vp, vp]
         L.or_esc_lame.argtypes = [vp, vp, i64, vp]
@@ -231,3 +232,9 @@ class OracleBody:
 
 def set_threads(n):
     lib().or_set_threads(int(n))
+
+
+def set_serial_order(on):
+    """True: the state-based force loops keep the serial loop's summation order on any thread
+    count (bit for bit the one-thread result); False: the threads backend's chunked scatter."""
+    lib().or_set_serial_order(1 if on else 0)

@@ -27,8 +27,13 @@
 #endif
 
 static int g_threads = 1;
+static int g_serial_order = 0;
 
 void or_set_threads(int32_t n) { g_threads = n < 1 ? 1 : n; }
+
+/* 1: the state-based force loops keep the serial loop's summation order on every thread
+ * count (or_force_density's serial-order gather); 0: the threads backend's chunked scatter */
+void or_set_serial_order(int32_t on) { g_serial_order = on != 0; }
 
 /* ------------------------------------------------------------------------------------ */
 /* small 3-vector / 3x3 helpers in the order StaticArrays.jl unrolls them                */
@@ -561,12 +566,260 @@ static void c_force_point(const or_sys *sys, or_state *st, double *bsink, int64_
     }
 }
 
+/* ------------------------------------------------------------------------------------ */
+/* The serial loop's arithmetic on many threads. In the serial loop of bond_system.jl:       */
+/* 285-297 point i's force row receives, in this order: the scattered terms -p V_k of every  */
+/* point k < i bonded to i (in increasing k, one term per k), its own terms p V_j (its bond   */
+/* order), then the scattered terms of the points k > i. A point's failure test and damage    */
+/* touch only its own bonds, and its force terms read only its own bonds, so the failure      */
+/* tests of all points can run first, then every point's state (OSB: weighted volume,         */
+/* dilatation, c1, c2; CMat: F, P K^-1 and the kill decision), then every force row gathered  */
+/* in the serial order: bit for bit the serial loop, on any number of threads.               */
+/* ------------------------------------------------------------------------------------ */
+
+/* position of i in the sorted bond list of j (the bond j -> i), or -1 */
+static int64_t reverse_bond(const or_sys *sys, int64_t j, int64_t i) {
+    int64_t lo = sys->off[j], hi = sys->off[j + 1];
+    while (lo < hi) {
+        int64_t mid = (lo + hi) >> 1;
+        if (sys->nbr[mid] < i) lo = mid + 1; else hi = mid;
+    }
+    return (lo < sys->off[j + 1] && sys->nbr[lo] == i) ? lo : -1;
+}
+
+/* OSB point state: weighted volume, dilatation (ordinary_state_based.jl:176-204) */
+static void osb_state_point(const or_sys *sys, const or_state *st, int64_t i, double *wd) {
+    const double *X = sys->X;
+    double wvol = 0.0;
+    for (int64_t b = sys->off[i]; b < sys->off[i + 1]; b++) {
+        int32_t j = sys->nbr[b];
+        double D[3] = {X[3 * j] - X[3 * i], X[3 * j + 1] - X[3 * i + 1], X[3 * j + 2] - X[3 * i + 2]};
+        double om = sys->omega[b] * (st->bond_active[b] ? 1.0 : 0.0);
+        wvol += om * SCF(sys, b) * dot3(D, D) * sys->vol[j];
+    }
+    double dil = 0.0;
+    if (wvol != 0.0) {
+        double c1d = 3.0 / wvol;
+        for (int64_t b = sys->off[i]; b < sys->off[i + 1]; b++) {
+            int32_t j = sys->nbr[b];
+            double Lb = sys->L[b], l = st->bond_length[b];
+            double om = sys->omega[b] * (st->bond_active[b] ? 1.0 : 0.0);
+            dil += om * SCF(sys, b) * c1d * Lb * (l - Lb) * sys->vol[j];
+        }
+    }
+    wd[0] = wvol;
+    wd[1] = dil;
+}
+
+/* c1, c2 of a point with one parameter set (ordinary_state_based.jl:135-136), stored beside
+ * its weighted volume and dilatation: wd = {wvol, dil, c1, c2} per point */
+static void osb_coeffs_point(const or_sys *sys, int64_t i, double *wd) {
+    const or_params *pi = P_of(sys, i);
+    wd[2] = 0.0;
+    wd[3] = 0.0;
+    if (wd[0] != 0.0 && !sys->multi) {
+        wd[2] = 15.0 * pi->G / wd[0];
+        wd[3] = wd[1] * (3.0 * pi->K / wd[0] - wd[2] / 3.0);
+    }
+}
+
+/* the force term p of bond b = (o -> q) of point o, as osb_force_point computes it */
+static inline void osb_bond_term(const or_sys *sys, const or_state *st, int64_t o, int64_t b,
+                                 const double *wd, double *p) {
+    const double *x = st->pos;
+    const or_params *po = P_of(sys, o);
+    int32_t q = sys->nbr[b];
+    double wvol = wd[4 * o], dil = wd[4 * o + 1], c1, c2;
+    if (sys->multi) {
+        const or_params *pq = P_of(sys, q);
+        c1 = 15.0 * (po->G + pq->G) / (2 * wvol);
+        c2 = dil * (3.0 * (po->K + pq->K) / (2 * wvol) - c1 / 3.0);
+    } else {
+        c1 = wd[4 * o + 2];
+        c2 = wd[4 * o + 3];
+    }
+    double Lb = sys->L[b], l = st->bond_length[b];
+    double d[3] = {x[3 * q] - x[3 * o], x[3 * q + 1] - x[3 * o + 1], x[3 * q + 2] - x[3 * o + 2]};
+    double om = sys->omega[b] * (st->bond_active[b] ? 1.0 : 0.0);
+    double s = om * SCF(sys, b) * (c2 * Lb + c1 * (l - Lb)) / l;
+    for (int k = 0; k < 3; k++) p[k] = s * d[k];
+}
+
+/* the terms of point i's own bonds (zero when its weighted volume is zero) */
+static void osb_terms_point(const or_sys *sys, const or_state *st, int64_t i, const double *wd,
+                            double *pb) {
+    for (int64_t b = sys->off[i]; b < sys->off[i + 1]; b++) {
+        if (wd[4 * i] == 0.0) { pb[3 * b] = pb[3 * b + 1] = pb[3 * b + 2] = 0.0; continue; }
+        osb_bond_term(sys, st, i, b, wd, pb + 3 * b);
+    }
+}
+
+/* force row of point i in the serial loop's order from the stored bond terms */
+static void gather_point(const or_sys *sys, or_state *st, int64_t i, const double *pb,
+                         const unsigned char *live, const int64_t *rev) {
+    double acc[3] = {0.0, 0.0, 0.0};
+    const int64_t b0 = sys->off[i], b1 = sys->off[i + 1];
+    for (int pass = 0; pass < 3; pass++)
+        for (int64_t b = b0; b < b1; b++) {
+            int32_t j = sys->nbr[b];
+            if (pass == 1) {
+                if (!live[i]) break;
+                for (int k = 0; k < 3; k++) acc[k] += pb[3 * b + k] * sys->vol[j];
+                continue;
+            }
+            if ((pass == 0) != (j < i) || !live[j]) continue;
+            int64_t r = rev[b];
+            if (r < 0) continue;
+            for (int k = 0; k < 3; k++) acc[k] += -pb[3 * r + k] * sys->vol[j];
+        }
+    for (int k = 0; k < 3; k++) st->b_int[3 * i + k] = acc[k];
+}
+
+/* CMat point state (correspondence.jl:183-224, 288-298): F and P K^-1 into FP (18 per point),
+ * alive[i] = 0 when the point's bonds are killed; defgrad, cauchy and the kill as
+ * c_force_point */
+static void c_state_point(const or_sys *sys, or_state *st, int64_t i, double *FP, unsigned char *alive) {
+    const double *x = st->pos, *X = sys->X;
+    const or_params *pi = P_of(sys, i);
+    double K[9] = {0}, Ft[9] = {0};
+    for (int64_t b = sys->off[i]; b < sys->off[i + 1]; b++) {
+        int32_t j = sys->nbr[b];
+        double D[3] = {X[3 * j] - X[3 * i], X[3 * j + 1] - X[3 * i + 1], X[3 * j + 2] - X[3 * i + 2]};
+        double d[3] = {x[3 * j] - x[3 * i], x[3 * j + 1] - x[3 * i + 1], x[3 * j + 2] - x[3 * i + 2]};
+        double om = sys->omega[b] * (st->bond_active[b] ? 1.0 : 0.0);
+        double temp = om * sys->vol[j];
+        for (int c = 0; c < 3; c++)
+            for (int r = 0; r < 3; r++) {
+                K[r + 3 * c] = K[r + 3 * c] + temp * (D[r] * D[c]);
+                Ft[r + 3 * c] = Ft[r + 3 * c] + temp * (d[r] * D[c]);
+            }
+    }
+    double Kinv[9], F[9];
+    or_inv3(K, Kinv);
+    matmul3(Ft, Kinv, F);
+    memcpy(st->defgrad + 9 * i, F, sizeof(F));
+    alive[i] = 1;
+    if (st->damage[i] > sys->maxdmg || has_nan9(F)) {
+        for (int64_t b = sys->off[i]; b < sys->off[i + 1]; b++) st->bond_active[b] = 0;
+        st->n_active[i] = 0;
+        alive[i] = 0;
+        return;
+    }
+    double P[9], PKinv[9], PF[9];
+    or_first_piola_kirchhoff(sys->cmodel, pi, F, P);
+    matmul3(P, Kinv, PKinv);
+    double J = or_det3(F), iJ = 1 / J, Ps[9];
+    for (int k = 0; k < 9; k++) Ps[k] = iJ * P[k];
+    matmulT3(Ps, F, PF);
+    memcpy(st->cauchy + 9 * i, PF, sizeof(PF));
+    memcpy(FP + 18 * i, F, sizeof(F));
+    memcpy(FP + 18 * i + 9, PKinv, sizeof(PKinv));
+}
+
+/* the force term t of bond b = (o -> q) of point o, as c_force_point computes it */
+static inline void c_bond_term(const or_sys *sys, const or_state *st, int64_t o, int64_t b,
+                               const double *FP, double *t) {
+    const double *x = st->pos, *X = sys->X;
+    const or_params *po = P_of(sys, o);
+    int32_t q = sys->nbr[b];
+    const double *F = FP + 18 * o, *PKinv = FP + 18 * o + 9;
+    double beta = sys->zem_cs * po->bc / po->delta;
+    double D[3] = {X[3 * q] - X[3 * o], X[3 * q + 1] - X[3 * o + 1], X[3 * q + 2] - X[3 * o + 2]};
+    double d[3] = {x[3 * q] - x[3 * o], x[3 * q + 1] - x[3 * o + 1], x[3 * q + 2] - x[3 * o + 2]};
+    double om = sys->omega[b] * (st->bond_active[b] ? 1.0 : 0.0);
+    double FD[3], z[3], W[9], WD[3];
+    matvec3(F, D, FD);
+    for (int k = 0; k < 3; k++) z[k] = d[k] - FD[k];
+    double ob = om * beta;
+    for (int k = 0; k < 9; k++) W[k] = om * PKinv[k];
+    matvec3(W, D, WD);
+    for (int k = 0; k < 3; k++) t[k] = WD[k] + ob * z[k];
+}
+
+static void c_terms_point(const or_sys *sys, const or_state *st, int64_t i, const double *FP,
+                          const unsigned char *alive, double *pb) {
+    for (int64_t b = sys->off[i]; b < sys->off[i + 1]; b++) {
+        if (!alive[i]) { pb[3 * b] = pb[3 * b + 1] = pb[3 * b + 2] = 0.0; continue; }
+        c_bond_term(sys, st, i, b, FP, pb + 3 * b);
+    }
+}
+
+/* reverse bond of every bond (-1 where the neighbour has no bond back), kept between calls
+ * for the same bond arrays */
+static int64_t *g_rev = NULL;
+static const int32_t *g_rev_nbr = NULL;
+static const int64_t *g_rev_off = NULL;
+static int64_t g_rev_nb = -1;
+
+static const int64_t *reverse_bonds(const or_sys *sys) {
+    if (g_rev && g_rev_nbr == sys->nbr && g_rev_off == sys->off && g_rev_nb == sys->n_bonds)
+        return g_rev;
+    free(g_rev);
+    g_rev = (int64_t *)malloc(sizeof(int64_t) * (size_t)(sys->n_bonds > 0 ? sys->n_bonds : 1));
+#pragma omp parallel for num_threads(g_threads) schedule(dynamic, 1024)
+    for (int64_t i = 0; i < sys->n; i++)
+        for (int64_t b = sys->off[i]; b < sys->off[i + 1]; b++) g_rev[b] = reverse_bond(sys, sys->nbr[b], i);
+    g_rev_nbr = sys->nbr;
+    g_rev_off = sys->off;
+    g_rev_nb = sys->n_bonds;
+    return g_rev;
+}
+
+static void force_density_serial_order(const or_sys *sys, or_state *st) {
+    int64_t n = sys->n;
+    const int64_t *rev = reverse_bonds(sys);
+#pragma omp parallel for num_threads(g_threads) schedule(dynamic, 1024)
+    for (int64_t i = 0; i < n; i++) {
+        st->n_active[i] = 0;
+        failure_point(sys, st, i);
+        damage_point(sys, st, i);
+    }
+    /* scratch kept between calls (a fresh allocation of this size per step costs more in page
+     * faults than the step's arithmetic) */
+    static double *pb = NULL;
+    static size_t pb_cap = 0;
+    size_t need = 3 * (size_t)(sys->n_bonds > 0 ? sys->n_bonds : 1);
+    if (need > pb_cap) {
+        free(pb);
+        pb = (double *)malloc(sizeof(double) * need);
+        pb_cap = need;
+    }
+    unsigned char *live = (unsigned char *)malloc((size_t)(n > 0 ? n : 1));
+    if (sys->material == OR_OSB) {
+        double *wd = (double *)malloc(sizeof(double) * 4 * (size_t)n);
+#pragma omp parallel for num_threads(g_threads) schedule(dynamic, 1024)
+        for (int64_t i = 0; i < n; i++) {
+            osb_state_point(sys, st, i, wd + 4 * i);
+            osb_coeffs_point(sys, i, wd + 4 * i);
+            live[i] = wd[4 * i] != 0.0;
+            osb_terms_point(sys, st, i, wd, pb);
+        }
+        free(wd);
+    } else {
+        double *FP = (double *)malloc(sizeof(double) * 18 * (size_t)n);
+#pragma omp parallel for num_threads(g_threads) schedule(dynamic, 1024)
+        for (int64_t i = 0; i < n; i++) {
+            c_state_point(sys, st, i, FP, live);
+            c_terms_point(sys, st, i, FP, live, pb);
+        }
+        free(FP);
+    }
+#pragma omp parallel for num_threads(g_threads) schedule(dynamic, 1024)
+    for (int64_t i = 0; i < n; i++) gather_point(sys, st, i, pb, live, rev);
+    free(live);
+}
+
 /* calc_force_density!: bond_system.jl:285-297 (one chunk), or the threads backend with
- * g_threads equal chunks for the scatter materials. */
+ * g_threads equal chunks for the scatter materials, or (or_set_serial_order) the serial
+ * loop's order on g_threads threads. */
 void or_force_density(const or_sys *sys, or_state *st, double t, double dt) {
     (void)t; (void)dt;
     int64_t n = sys->n;
     memset(st->b_int, 0, sizeof(double) * 3 * (size_t)n);
+    if (g_serial_order && sys->material != OR_BB) {
+        force_density_serial_order(sys, st);
+        return;
+    }
     if (sys->material == OR_BB || g_threads == 1 || n < 2 * g_threads) {
 #pragma omp parallel for num_threads(sys->material == OR_BB ? g_threads : 1) schedule(static)
         for (int64_t i = 0; i < n; i++) {

@@ -94,6 +94,7 @@ int or_point_params(int32_t material, double delta, double rho, double E, double
                     double K, double lambda, double mu, double Gc, double epsc,
                     or_params *out, char *msg, int32_t msg_len);
 void or_set_threads(int32_t n);
+void or_set_serial_order(int32_t on);
 /* EnergySurfaceCorrection (bond_system_corrections.jl): mfactor[3 i + d] of every point from the
  * current bond states (calc_mfactor!), and the per-bond factor from it (calc_scfactor!). */
 void or_esc_mfactor(const or_sys *sys, const or_state *st, double *mfactor);

@@ -29,6 +29,20 @@ static pd_status set_ctrl(pd_handle* h, size_t off, const void* src, size_t byte
   return PD_OK;
 }
 
+// Copies between host and device ordered on the stream `s` and complete on return. The
+// handles' streams are non-blocking: a plain cudaMemcpy from pageable memory may return before
+// its DMA has landed, and nothing orders a kernel on such a stream after it.
+static cudaError_t h2d(void* dst, const void* src, size_t bytes, cudaStream_t s) {
+  if (bytes == 0) return cudaSuccess;
+  cudaError_t e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s);
+  return e != cudaSuccess ? e : cudaStreamSynchronize(s);
+}
+static cudaError_t d2h(void* dst, const void* src, size_t bytes, cudaStream_t s) {
+  if (bytes == 0) return cudaSuccess;
+  cudaError_t e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, s);
+  return e != cudaSuccess ? e : cudaStreamSynchronize(s);
+}
+
 static pd_status upload_meta(pd_handle* h) {
   PD_CUDA(cudaMemcpyAsync(h->d.meta, h->hmeta.data(), sizeof(unsigned) * h->n,
                           cudaMemcpyHostToDevice, h->stream));
@@ -346,8 +360,8 @@ static pd_status begin_create(const pd_body_desc* desc, pd_handle** out, pd_hand
   double4 *dX0 = nullptr, *dcur = nullptr;
   PD_TRY(dalloc(h, &dX0, n));
   PD_TRY(dalloc(h, &dcur, n));
-  PD_CUDA(cudaMemcpy(dX0, X0.data(), sizeof(double4) * n, cudaMemcpyHostToDevice));
-  PD_CUDA(cudaMemcpy(dcur, cur.data(), sizeof(double4) * n, cudaMemcpyHostToDevice));
+  PD_CUDA(h2d(dX0, X0.data(), sizeof(double4) * n, h->stream));
+  PD_CUDA(h2d(dcur, cur.data(), sizeof(double4) * n, h->stream));
   h->d.X0 = dX0;
   h->d.cur = dcur;
   h->d.n = n;
@@ -383,10 +397,10 @@ extern "C" pd_status pd_create(const pd_body_desc* desc, pd_handle** out) {
   if (st == PD_OK && desc->bond_length) st = dalloc(h, &dL, nb);
   if (st == PD_OK && desc->fail_permit) st = dalloc(h, &dfp, nb);
   if (st != PD_OK) { pd_destroy(h); return st; }
-  cudaError_t e = cudaMemcpy(doff, desc->bond_offsets, sizeof(long long) * (n + 1), cudaMemcpyHostToDevice);
-  if (e == cudaSuccess && nb) e = cudaMemcpy(dnbr, desc->neighbors, sizeof(int) * nb, cudaMemcpyHostToDevice);
-  if (e == cudaSuccess && dL) e = cudaMemcpy(dL, desc->bond_length, sizeof(double) * nb, cudaMemcpyHostToDevice);
-  if (e == cudaSuccess && dfp) e = cudaMemcpy(dfp, desc->fail_permit, nb, cudaMemcpyHostToDevice);
+  cudaError_t e = h2d(doff, desc->bond_offsets, sizeof(long long) * (n + 1), h->stream);
+  if (e == cudaSuccess && nb) e = h2d(dnbr, desc->neighbors, sizeof(int) * nb, h->stream);
+  if (e == cudaSuccess && dL) e = h2d(dL, desc->bond_length, sizeof(double) * nb, h->stream);
+  if (e == cudaSuccess && dfp) e = h2d(dfp, desc->fail_permit, nb, h->stream);
   if (e != cudaSuccess) { pd_destroy(h); return fail(PD_ERR_CUDA, cudaGetErrorString(e)); }
   h->d.off = doff;
   st = finish_create(h, dnbr, dL, dfp);
@@ -464,9 +478,9 @@ extern "C" pd_status pd_find_bonds(int64_t n, const double* position, const doub
   ok(cudaMalloc(&doff, sizeof(long long) * (n + 1)));
   if (n_filters > 0) ok(cudaMalloc(&dm, sizeof(unsigned short) * (n ? n : 1)));
   if (e == cudaSuccess) {
-    ok(cudaMemcpy(dX, position, sizeof(double) * 3 * n, cudaMemcpyHostToDevice));
-    ok(cudaMemcpy(dd, delta, sizeof(double) * n, cudaMemcpyHostToDevice));
-    if (dm) ok(cudaMemcpy(dm, mask.data(), sizeof(unsigned short) * n, cudaMemcpyHostToDevice));
+    ok(h2d(dX, position, sizeof(double) * 3 * n, s));
+    ok(h2d(dd, delta, sizeof(double) * n, s));
+    if (dm) ok(h2d(dm, mask.data(), sizeof(unsigned short) * n, s));
   }
   if (e == cudaSuccess) ok(device_find_bonds_grid(n, dX, dd, dm, nullptr, lo, hc, nc, doff, &dnbr, &nb, &dup, s));
   if (e == cudaSuccess && dup) st = fail(PD_ERR_ARG, "point duplicate found!");
@@ -479,14 +493,14 @@ extern "C" pd_status pd_find_bonds(int64_t n, const double* position, const doub
       if (e == cudaSuccess) {
         std::vector<unsigned char> fp(n, 1);
         if (fp_point) std::copy(fp_point, fp_point + n, fp.begin());
-        ok(cudaMemcpy(dfp, fp.data(), n, cudaMemcpyHostToDevice));
+        ok(h2d(dfp, fp.data(), n, s));
         if (nb) launch_bond_props(n, dX, dfp, doff, dnbr, dL, dfpb, s);
         ok(cudaStreamSynchronize(s));
-        ok(cudaMemcpy(bond_offsets, doff, sizeof(long long) * (n + 1), cudaMemcpyDeviceToHost));
+        ok(d2h(bond_offsets, doff, sizeof(long long) * (n + 1), s));
         if (nb) {
-          ok(cudaMemcpy(neighbors, dnbr, sizeof(int) * nb, cudaMemcpyDeviceToHost));
-          ok(cudaMemcpy(bond_length, dL, sizeof(double) * nb, cudaMemcpyDeviceToHost));
-          ok(cudaMemcpy(fail_permit, dfpb, nb, cudaMemcpyDeviceToHost));
+          ok(d2h(neighbors, dnbr, sizeof(int) * nb, s));
+          ok(d2h(bond_length, dL, sizeof(double) * nb, s));
+          ok(d2h(fail_permit, dfpb, nb, s));
         }
       }
     }
@@ -537,12 +551,12 @@ static pd_status create_search(const pd_body_desc* desc, const double* search_po
   if (st != PD_OK) { std::string m = g_err; pd_destroy(h); return fail(st, m); }
   std::vector<unsigned char> fp(n, 1);
   if (fp_point) std::copy(fp_point, fp_point + n, fp.begin());
-  cudaError_t e = cudaMemcpy(dX, X.data(), sizeof(double) * 3 * n, cudaMemcpyHostToDevice);
-  if (e == cudaSuccess && dXs) e = cudaMemcpy(dXs, search_position, sizeof(double) * 3 * n, cudaMemcpyHostToDevice);
-  if (e == cudaSuccess) e = cudaMemcpy(dd, delta.data(), sizeof(double) * n, cudaMemcpyHostToDevice);
-  if (e == cudaSuccess && dm) e = cudaMemcpy(dm, mask.data(), sizeof(unsigned short) * n, cudaMemcpyHostToDevice);
-  if (e == cudaSuccess) e = cudaMemcpy(dfp, fp.data(), n, cudaMemcpyHostToDevice);
-  if (e == cudaSuccess && down) e = cudaMemcpy(down, owned, n, cudaMemcpyHostToDevice);
+  cudaError_t e = h2d(dX, X.data(), sizeof(double) * 3 * n, h->stream);
+  if (e == cudaSuccess && dXs) e = h2d(dXs, search_position, sizeof(double) * 3 * n, h->stream);
+  if (e == cudaSuccess) e = h2d(dd, delta.data(), sizeof(double) * n, h->stream);
+  if (e == cudaSuccess && dm) e = h2d(dm, mask.data(), sizeof(unsigned short) * n, h->stream);
+  if (e == cudaSuccess) e = h2d(dfp, fp.data(), n, h->stream);
+  if (e == cudaSuccess && down) e = h2d(down, owned, n, h->stream);
   int* dnbr = nullptr;
   long long nb = 0;
   int dup = 0;
@@ -652,10 +666,10 @@ extern "C" pd_status pd_set_state(pd_handle* h, const double* position, const do
   // every copy and kernel is ordered on the handle's stream (from page-locked host memory the
   // copies run at full PCIe rate); one synchronize at the end
   const size_t vec = sizeof(double) * 3 * n;
-  const cudaMemcpyKind h2d = cudaMemcpyHostToDevice;
+  const cudaMemcpyKind kh2d = cudaMemcpyHostToDevice;
   if (h->precision == PD_PREC_FP64) {
     src = position;
-    if (displacement) PD_CUDA(cudaMemcpyAsync(h->g.u, displacement, vec, h2d, h->stream));
+    if (displacement) PD_CUDA(cudaMemcpyAsync(h->g.u, displacement, vec, kh2d, h->stream));
   } else if (displacement) {
     src = displacement;
   } else if (position) {
@@ -665,19 +679,19 @@ extern "C" pd_status pd_set_state(pd_handle* h, const double* position, const do
   if (src) {
     void* tmp = nullptr;
     PD_TRY(staging(h, vec, &tmp));
-    PD_CUDA(cudaMemcpyAsync(tmp, src, vec, h2d, h->stream));
+    PD_CUDA(cudaMemcpyAsync(tmp, src, vec, kh2d, h->stream));
     k_set_cur<<<(unsigned)((n + 255) / 256), 256, 0, h->stream>>>(h->d.cur, h->d.X0, (const double*)tmp,
                                                                   n, sub_x0);
     PD_CUDA(cudaGetLastError());
     launch_split_u(h->d, h->stream);
     PD_CUDA(cudaGetLastError());
   }
-  if (velocity) PD_CUDA(cudaMemcpyAsync(h->g.v, velocity, vec, h2d, h->stream));
-  if (velocity_half) PD_CUDA(cudaMemcpyAsync(h->g.vh, velocity_half, vec, h2d, h->stream));
-  if (acceleration) PD_CUDA(cudaMemcpyAsync(h->g.a, acceleration, vec, h2d, h->stream));
+  if (velocity) PD_CUDA(cudaMemcpyAsync(h->g.v, velocity, vec, kh2d, h->stream));
+  if (velocity_half) PD_CUDA(cudaMemcpyAsync(h->g.vh, velocity_half, vec, kh2d, h->stream));
+  if (acceleration) PD_CUDA(cudaMemcpyAsync(h->g.a, acceleration, vec, kh2d, h->stream));
   PD_CUDA(cudaStreamSynchronize(h->stream));
   if (b_ext) {
-    PD_CUDA(cudaMemcpy(h->g.bext, b_ext, vec, h2d));
+    PD_CUDA(h2d(h->g.bext, b_ext, vec, h->stream));
     for (long long i = 0; i < n; i++) {
       const bool nz = b_ext[3 * i] != 0 || b_ext[3 * i + 1] != 0 || b_ext[3 * i + 2] != 0 ||
                       std::signbit(b_ext[3 * i]) || std::signbit(b_ext[3 * i + 1]) || std::signbit(b_ext[3 * i + 2]);
@@ -687,15 +701,14 @@ extern "C" pd_status pd_set_state(pd_handle* h, const double* position, const do
     PD_TRY(upload_meta(h));
   }
   if (bond_active && nb > 0) {
-    unsigned char* tmp = nullptr;
-    PD_CUDA(cudaMalloc(&tmp, nb));
-    cudaError_t e = cudaMemcpy(tmp, bond_active, nb, cudaMemcpyHostToDevice);
+    void* tmp = nullptr;
+    PD_TRY(staging(h, (size_t)nb, &tmp));
+    cudaError_t e = h2d(tmp, bond_active, nb, h->stream);
     if (e == cudaSuccess) {
-      launch_pack_bits(h->d, tmp, h->stream);
+      launch_pack_bits(h->d, (const unsigned char*)tmp, h->stream);
       h->kfull = true;
       e = cudaStreamSynchronize(h->stream);
     }
-    cudaFree(tmp);
     if (e != cudaSuccess) return fail(PD_ERR_CUDA, cudaGetErrorString(e));
     launch_count_active(h->d, h->stream);
     h->damage_valid = true;
@@ -750,7 +763,7 @@ extern "C" pd_status pd_get_field(pd_handle* h, int32_t field, void* out, size_t
       if (h->precision == PD_PREC_FP64) st = copy(h->d.b64);
       else {
         std::vector<float> f(3 * n);
-        PD_CUDA(cudaMemcpy(f.data(), h->d.b32, sizeof(float) * 3 * n, cudaMemcpyDeviceToHost));
+        PD_CUDA(d2h(f.data(), h->d.b32, sizeof(float) * 3 * n, h->stream));
         double* o = (double*)out;
         for (long long k = 0; k < 3 * n; k++) o[k] = f[k];
       }
@@ -763,14 +776,14 @@ extern "C" pd_status pd_get_field(pd_handle* h, int32_t field, void* out, size_t
       break;
     case PD_FIELD_N_ACTIVE_BONDS: {
       std::vector<int> na(n);
-      PD_CUDA(cudaMemcpy(na.data(), h->d.n_active, sizeof(int) * n, cudaMemcpyDeviceToHost));
+      PD_CUDA(d2h(na.data(), h->d.n_active, sizeof(int) * n, h->stream));
       int64_t* o = (int64_t*)out;
       for (long long i = 0; i < n; i++) o[i] = na[i];
       break;
     }
     case PD_FIELD_N_NEIGHBORS: {
       std::vector<long long> off(n + 1);
-      PD_CUDA(cudaMemcpy(off.data(), h->d.off, sizeof(long long) * (n + 1), cudaMemcpyDeviceToHost));
+      PD_CUDA(d2h(off.data(), h->d.off, sizeof(long long) * (n + 1), h->stream));
       int64_t* o = (int64_t*)out;
       for (long long i = 0; i < n; i++) o[i] = off[i + 1] - off[i];
       break;
@@ -791,7 +804,7 @@ extern "C" pd_status pd_get_field(pd_handle* h, int32_t field, void* out, size_t
       if (h->precision == PD_PREC_FP64) st = copy(h->d.F64);
       else {
         std::vector<float> f(9 * n);
-        PD_CUDA(cudaMemcpy(f.data(), h->d.H32, sizeof(float) * 9 * n, cudaMemcpyDeviceToHost));
+        PD_CUDA(d2h(f.data(), h->d.H32, sizeof(float) * 9 * n, h->stream));
         double* o = (double*)out;
         for (long long i = 0; i < n; i++)
           for (int k = 0; k < 9; k++) o[9 * i + k] = (double)f[9 * i + k] + ((k % 4) == 0 ? 1.0 : 0.0);
@@ -862,7 +875,7 @@ extern "C" pd_status pd_set_bcs(pd_handle* h, int32_t n_bcs, const pd_bc_desc* b
   for (size_t p = 0; p < pts.size(); p++) slot[pts[p]] = (int)p;
   int* ds = nullptr;
   PD_TRY(dalloc(h, &ds, n));
-  if (n > 0) PD_CUDA(cudaMemcpy(ds, slot.data(), sizeof(int) * n, cudaMemcpyHostToDevice));
+  if (n > 0) PD_CUDA(h2d(ds, slot.data(), sizeof(int) * n, h->stream));
   h->bc.slot = ds;
   int *dp = nullptr, *de = nullptr;
   BCEntry* den = nullptr;
@@ -873,11 +886,11 @@ extern "C" pd_status pd_set_bcs(pd_handle* h, int32_t n_bcs, const pd_bc_desc* b
   PD_TRY(dalloc(h, &den, ent.size()));
   PD_TRY(dalloc(h, &di, info.size()));
   PD_TRY(dalloc(h, &dd, data.size()));
-  if (!pts.empty()) PD_CUDA(cudaMemcpy(dp, pts.data(), sizeof(int) * pts.size(), cudaMemcpyHostToDevice));
-  PD_CUDA(cudaMemcpy(de, eoff.data(), sizeof(int) * eoff.size(), cudaMemcpyHostToDevice));
-  if (!ent.empty()) PD_CUDA(cudaMemcpy(den, ent.data(), sizeof(BCEntry) * ent.size(), cudaMemcpyHostToDevice));
-  if (!info.empty()) PD_CUDA(cudaMemcpy(di, info.data(), sizeof(BCInfo) * info.size(), cudaMemcpyHostToDevice));
-  if (!data.empty()) PD_CUDA(cudaMemcpy(dd, data.data(), sizeof(double) * data.size(), cudaMemcpyHostToDevice));
+  if (!pts.empty()) PD_CUDA(h2d(dp, pts.data(), sizeof(int) * pts.size(), h->stream));
+  PD_CUDA(h2d(de, eoff.data(), sizeof(int) * eoff.size(), h->stream));
+  if (!ent.empty()) PD_CUDA(h2d(den, ent.data(), sizeof(BCEntry) * ent.size(), h->stream));
+  if (!info.empty()) PD_CUDA(h2d(di, info.data(), sizeof(BCInfo) * info.size(), h->stream));
+  if (!data.empty()) PD_CUDA(h2d(dd, data.data(), sizeof(double) * data.size(), h->stream));
   h->bc.n_points = (int)pts.size();
   h->bc.point = dp;
   h->bc.entry_off = de;
@@ -930,7 +943,7 @@ extern "C" pd_status pd_stable_timestep(pd_handle* h, double safety_factor, doub
     PD_CUDA(cudaMalloc(&tmp, sizeof(double) * n));
     launch_timestep(h->d, tmp, h->stream);
     cudaError_t e = cudaStreamSynchronize(h->stream);
-    if (e == cudaSuccess) e = cudaMemcpy(dtp.data(), tmp, sizeof(double) * n, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = d2h(dtp.data(), tmp, sizeof(double) * n, h->stream);
     cudaFree(tmp);
     if (e != cudaSuccess) return fail(PD_ERR_CUDA, cudaGetErrorString(e));
   }
@@ -1056,7 +1069,7 @@ static pd_status run_vv(pd_handle* h, int64_t first_step, int64_t n_steps, doubl
       if (!(p.dt > 0)) return fail(PD_ERR_ARG, "dt <= 0 and no per-parameter time steps set");
   if (h->needs_table) {
     Ctrl c;
-    PD_CUDA(cudaMemcpy(&c, h->d.ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost));
+    PD_CUDA(d2h(&c, h->d.ctrl, sizeof(Ctrl), h->stream));
     if (c.table_first > first_step || c.table_first + c.table_n < first_step + n_steps)
       return fail(PD_ERR_ARG, "boundary condition values do not cover steps " + std::to_string(first_step) +
                                   ".." + std::to_string(first_step + n_steps - 1));
@@ -1085,6 +1098,183 @@ extern "C" pd_status pd_run_vv(pd_handle* h, int64_t first_step, int64_t n_steps
   return run_vv(h, first_step, n_steps, dt, nullptr);
 }
 
+// ---------------------------------------------------------------------------------------
+// Groups of bodies advanced together (the size classes of an ensemble): the steps of every
+// body of the group in one CUDA graph, each body's launches on its own stream, forked from and
+// joined into the first body's stream.
+// ---------------------------------------------------------------------------------------
+struct pd_group {
+  std::vector<pd_handle*> hs;
+  int device = 0;
+  cudaEvent_t fork = nullptr;
+  std::vector<cudaEvent_t> join;
+  cudaGraphExec_t gexec = nullptr;
+  int gsteps = 0;
+  double gdt = 0;
+  std::vector<GraphKey> keys;  // per body: mapping and state version the graph was made for
+  std::vector<long long> nodes;  // per body: kernels of one graph launch
+};
+
+static void group_release_graph(pd_group* g) {
+  if (g->gexec) cudaGraphExecDestroy(g->gexec);
+  g->gexec = nullptr;
+  g->keys.clear();
+}
+
+extern "C" pd_status pd_group_create(pd_handle* const* handles, int32_t n, pd_group** out) {
+  if (!handles || n < 1 || !out) return fail(PD_ERR_ARG, "handles, n >= 1 and out are required");
+  for (int k = 0; k < n; k++) {
+    if (!handles[k]) return fail(PD_ERR_ARG, "handle is NULL");
+    if (handles[k]->device != handles[0]->device)
+      return fail(PD_ERR_ARG, "the bodies of a group share one device");
+    for (int q = 0; q < k; q++)
+      if (handles[q] == handles[k] || handles[q]->stream == handles[k]->stream)
+        return fail(PD_ERR_ARG, "the bodies of a group are distinct and on distinct streams");
+  }
+  PD_CUDA(cudaSetDevice(handles[0]->device));
+  pd_group* g = new pd_group();
+  g->hs.assign(handles, handles + n);
+  g->device = handles[0]->device;
+  cudaError_t e = cudaEventCreateWithFlags(&g->fork, cudaEventDisableTiming);
+  g->join.assign(n, nullptr);
+  for (int k = 0; k < n && e == cudaSuccess; k++) e = cudaEventCreateWithFlags(&g->join[k], cudaEventDisableTiming);
+  if (e != cudaSuccess) {
+    pd_group_destroy(g);
+    return fail(PD_ERR_CUDA, std::string("pd_group_create: ") + cudaGetErrorString(e));
+  }
+  *out = g;
+  return PD_OK;
+}
+
+extern "C" pd_status pd_group_destroy(pd_group* g) {
+  if (!g) return PD_OK;
+  cudaSetDevice(g->device);
+  group_release_graph(g);
+  if (g->fork) cudaEventDestroy(g->fork);
+  for (cudaEvent_t e : g->join)
+    if (e) cudaEventDestroy(e);
+  delete g;
+  return PD_OK;
+}
+
+// the steps [0, steps) of every body, each on its own stream between the fork and the join
+static void group_issue(pd_group* g, int steps, double dto) {
+  cudaStream_t origin = g->hs[0]->stream;
+  cudaEventRecord(g->fork, origin);
+  for (size_t k = 1; k < g->hs.size(); k++) cudaStreamWaitEvent(g->hs[k]->stream, g->fork, 0);
+  for (pd_handle* h : g->hs) issue_steps(h, steps, dto, nullptr);
+  for (size_t k = 1; k < g->hs.size(); k++) {
+    cudaEventRecord(g->join[k], g->hs[k]->stream);
+    cudaStreamWaitEvent(origin, g->join[k], 0);
+  }
+}
+
+static GraphKey group_key(const pd_handle* h, int steps, double dto) {
+  GraphKey key;
+  key.steps = steps; key.group = h->cfg.group; key.block = h->cfg.block; key.exact = h->cfg.exact;
+  key.bcpts = h->bc.n_points; key.dt = dto; key.version = h->version; key.pipe = h->cfg.pipe;
+  return key;
+}
+
+extern "C" pd_status pd_group_run_vv(pd_group* g, int64_t first_step, int64_t n_steps, double dt,
+                                     int32_t steps_per_graph, double* ms_total) {
+  if (!g) return fail(PD_ERR_ARG, "group is NULL");
+  if (n_steps < 0 || steps_per_graph < 0 || steps_per_graph > 4096)
+    return fail(PD_ERR_ARG, "n_steps >= 0 and 0 <= steps_per_graph <= 4096");
+  if (ms_total) *ms_total = 0.0;
+  if (n_steps == 0) return PD_OK;
+  PD_CUDA(cudaSetDevice(g->device));
+  const double dto = dt > 0 ? dt : -1.0;
+  for (pd_handle* h : g->hs) {
+    if (dto < 0)
+      for (auto& p : h->hp)
+        if (!(p.dt > 0)) return fail(PD_ERR_ARG, "dt <= 0 and no per-parameter time steps set");
+    if (h->needs_table) {
+      Ctrl c;
+      PD_CUDA(d2h(&c, h->d.ctrl, sizeof(Ctrl), h->stream));
+      if (c.table_first > first_step || c.table_first + c.table_n < first_step + n_steps)
+        return fail(PD_ERR_ARG, "boundary condition values do not cover steps " +
+                                    std::to_string(first_step) + ".." +
+                                    std::to_string(first_step + n_steps - 1));
+    }
+    PD_TRY(clear_error(h));
+    PD_CUDA(cudaStreamSynchronize(h->stream));
+  }
+  cudaStream_t origin = g->hs[0]->stream;
+  cudaEvent_t t0 = nullptr, t1 = nullptr;
+  if (ms_total) {
+    PD_CUDA(cudaEventCreate(&t0));
+    PD_CUDA(cudaEventCreate(&t1));
+    cudaEventRecord(t0, origin);
+  }
+  pd_status st = PD_OK;
+  const int K = steps_per_graph;
+  int64_t done = 0;
+  while (done < n_steps && st == PD_OK) {
+    const long long base = first_step + done;
+    const int steps = (int)std::min<int64_t>(n_steps - done, K > 0 ? K : (int64_t)(1 << 30));
+    // every body's first step of the block, written on the origin stream before the launch
+    for (pd_handle* h : g->hs) {
+      cudaError_t e = cudaMemcpyAsync(reinterpret_cast<char*>(h->d.ctrl) + offsetof(Ctrl, base), &base,
+                                      sizeof(long long), cudaMemcpyHostToDevice, origin);
+      if (e != cudaSuccess) { st = fail(PD_ERR_CUDA, cudaGetErrorString(e)); break; }
+    }
+    if (st != PD_OK) break;
+    if (K > 0 && steps == K) {
+      std::vector<GraphKey> keys;
+      for (pd_handle* h : g->hs) keys.push_back(group_key(h, steps, dto));
+      if (!(g->gexec && keys == g->keys)) {
+        group_release_graph(g);
+        std::vector<long long> before;
+        for (pd_handle* h : g->hs) before.push_back(h->launches);
+        cudaGraph_t graph;
+        cudaError_t e = cudaStreamBeginCapture(origin, cudaStreamCaptureModeThreadLocal);
+        if (e == cudaSuccess) {
+          group_issue(g, steps, dto);
+          e = cudaStreamEndCapture(origin, &graph);
+        }
+        g->nodes.assign(g->hs.size(), 0);
+        for (size_t k = 0; k < g->hs.size(); k++) {
+          g->nodes[k] = g->hs[k]->launches - before[k];
+          g->hs[k]->launches = before[k];
+        }
+        if (e != cudaSuccess) { st = fail(PD_ERR_CUDA, std::string("group graph capture: ") + cudaGetErrorString(e)); break; }
+        e = cudaGraphInstantiate(&g->gexec, graph, 0);
+        cudaGraphDestroy(graph);
+        if (e != cudaSuccess) {
+          g->gexec = nullptr;
+          st = fail(PD_ERR_CUDA, std::string("group graph instantiate: ") + cudaGetErrorString(e));
+          break;
+        }
+        g->keys = keys;
+      }
+      cudaError_t e = cudaGraphLaunch(g->gexec, origin);
+      if (e != cudaSuccess) { st = fail(PD_ERR_CUDA, std::string("group graph launch: ") + cudaGetErrorString(e)); break; }
+      for (size_t k = 0; k < g->hs.size(); k++) g->hs[k]->launches += g->nodes[k];
+    } else {
+      group_issue(g, steps, dto);
+      cudaError_t e = cudaGetLastError();
+      if (e != cudaSuccess) { st = fail(PD_ERR_CUDA, cudaGetErrorString(e)); break; }
+    }
+    done += steps;
+  }
+  if (ms_total) cudaEventRecord(t1, origin);
+  cudaError_t se = cudaStreamSynchronize(origin);
+  if (st == PD_OK && se != cudaSuccess) st = fail(PD_ERR_CUDA, cudaGetErrorString(se));
+  if (ms_total && st == PD_OK) {
+    float x = 0.f;
+    cudaEventElapsedTime(&x, t0, t1);
+    *ms_total = x;
+  }
+  if (t0) cudaEventDestroy(t0);
+  if (t1) cudaEventDestroy(t1);
+  for (pd_handle* h : g->hs) {
+    h->damage_valid = true;
+    if (st == PD_OK) st = check_err(h);
+  }
+  return st;
+}
+
 extern "C" pd_status pd_run_vv_timed(pd_handle* h, int64_t first_step, int64_t n_steps, double dt,
                                      double* ms_total, double* ms_phase_a, double* ms_phase_b,
                                      double* ms_integrate) {
@@ -1092,6 +1282,28 @@ extern "C" pd_status pd_run_vv_timed(pd_handle* h, int64_t first_step, int64_t n
   if (n_steps <= 0) return fail(PD_ERR_ARG, "n_steps must be > 0");
   if (n_steps > (1 << 20)) return fail(PD_ERR_ARG, "at most 2^20 timed steps per call");
   PD_CUDA(cudaSetDevice(h->device));
+  if (!ms_phase_a && !ms_phase_b && !ms_integrate) {
+    // the run as pd_run_vv issues it (CUDA-graph blocks when pd_set_graph is on), between two
+    // events on the handle's stream
+    cudaEvent_t e0, e1;
+    PD_CUDA(cudaEventCreate(&e0));
+    cudaError_t ce = cudaEventCreate(&e1);
+    if (ce != cudaSuccess) { cudaEventDestroy(e0); PD_CUDA(ce); }
+    cudaEventRecord(e0, h->stream);
+    pd_status st = run_vv(h, first_step, n_steps, dt, nullptr);
+    cudaEventRecord(e1, h->stream);
+    if (st == PD_OK || st == PD_ERR_NAN) {
+      cudaError_t se = cudaEventSynchronize(e1);
+      float x = 0.f;
+      if (se == cudaSuccess) cudaEventElapsedTime(&x, e0, e1);
+      if (ms_total) *ms_total = x;
+      if (se != cudaSuccess && st == PD_OK)
+        st = fail(PD_ERR_CUDA, std::string("pd_run_vv_timed: ") + cudaGetErrorString(se));
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return st;
+  }
   const size_t nev = (size_t)4 * n_steps + 2;
   std::vector<cudaEvent_t> ev(nev);
   for (auto& e : ev) PD_CUDA(cudaEventCreate(&e));
@@ -1176,14 +1388,17 @@ extern "C" pd_status pd_autotune(pd_handle* h, int32_t* group_out, int32_t* bloc
     if (st != PD_OK) { cudaEventDestroy(e0); cudaEventDestroy(e1); return st; }
     const bool tma = h->precision == PD_PREC_FP32_KAHAN && G == 1 && tma_supported(h->d);
     const bool two = h->precision == PD_PREC_FP32_KAHAN && h->material != PD_MAT_CMAT;
-    // candidates: blocks of 128 / 256 with plain loads, then (FP32 OSB) the two-row kernels,
-    // then (one lane per point) the TMA-staged bond stream
-    for (int v = 0; v < 7; v++) {
+    const bool packed = h->precision == PD_PREC_FP32_KAHAN && G == 1 && pk_supported(h->d, 1);
+    // candidates: blocks of 128 / 256 with plain loads, then (FP32 BB / OSB) the two-row
+    // kernels, then (one lane per point) the TMA-staged bond stream, then (FP32 OSB, one lane
+    // per point) the packed-pair kernels
+    for (int v = 0; v < 9; v++) {
       if ((v == 2 || v == 3) && !two) continue;
-      if (v >= 4 && !tma) continue;
-      const int B = v < 4 ? blocks[v % 2] : 128;
+      if (v >= 4 && v < 7 && !tma) continue;
+      if (v >= 7 && !packed) continue;
+      const int B = v < 4 ? blocks[v % 2] : v < 7 ? 128 : blocks[v - 7];
       h->cfg.group = G; h->cfg.block = B; h->cfg.exact = false;
-      h->cfg.pipe = v < 2 ? 0 : v < 4 ? 4 : v - 3;
+      h->cfg.pipe = v < 2 ? 0 : v < 4 ? 4 : v < 7 ? v - 3 : 5;
       float ms;
       pd_status ts = time_cfg(&ms);
       if (ts != PD_OK) { cudaEventDestroy(e0); cudaEventDestroy(e1); return ts; }
@@ -1254,8 +1469,8 @@ extern "C" pd_status pd_break_bonds(pd_handle* h, const uint8_t* set_a, const ui
     if (set_a[i] && set_b[i]) return fail(PD_ERR_ARG, "point sets intersect");
   unsigned char* tmp = nullptr;
   PD_CUDA(cudaMalloc(&tmp, 2 * n));
-  cudaError_t e = cudaMemcpy(tmp, set_a, n, cudaMemcpyHostToDevice);
-  if (e == cudaSuccess) e = cudaMemcpy(tmp + n, set_b, n, cudaMemcpyHostToDevice);
+  cudaError_t e = h2d(tmp, set_a, n, h->stream);
+  if (e == cudaSuccess) e = h2d(tmp + n, set_b, n, h->stream);
   if (e == cudaSuccess) {
     launch_break_sets(h->d, tmp, tmp + n, h->stream);
     h->kfull = true;
@@ -1304,7 +1519,7 @@ extern "C" pd_status pd_break_random_pairs_ids(pd_handle* h, double fraction, ui
   long long* gid = nullptr;
   if (point_ids) {
     PD_TRY(dalloc(h, &gid, h->n));
-    PD_CUDA(cudaMemcpy(gid, point_ids, sizeof(long long) * h->n, cudaMemcpyHostToDevice));
+    PD_CUDA(h2d(gid, point_ids, sizeof(long long) * h->n, h->stream));
   }
   launch_break_random(h->d, fraction, (unsigned long long)seed, gid, h->stream);
   h->kfull = true;
@@ -1327,9 +1542,11 @@ extern "C" pd_status pd_get_mapping(pd_handle* h, int32_t* group, int32_t* block
 
 extern "C" pd_status pd_set_pipeline(pd_handle* h, int32_t pipe) {
   if (!h) return fail(PD_ERR_ARG, "handle is NULL");
-  if (pipe < 0 || pipe > 4) return fail(PD_ERR_ARG, "pipe must be 0 to 4");
+  if (pipe < 0 || pipe > 5) return fail(PD_ERR_ARG, "pipe must be 0 to 5");
   if (pipe == 4 && (h->precision != PD_PREC_FP32_KAHAN || h->material == PD_MAT_CMAT))
     return fail(PD_ERR_ARG, "the two-row kernels are the FP32 BB and OSB ones");
+  if (pipe == 5 && (h->precision != PD_PREC_FP32_KAHAN || h->material != PD_MAT_OSB))
+    return fail(PD_ERR_ARG, "the packed-pair kernels are the FP32 OSB ones");
   if (pipe >= 1 && pipe <= 3 && (h->precision != PD_PREC_FP32_KAHAN || !tma_supported(h->d)))
     return fail(PD_ERR_ARG, "the staged bond stream needs the FP32 path, one lane per point and BB or OSB");
   h->cfg.pipe = pipe;

@@ -230,7 +230,9 @@ extern "C" pd_status pd_dr_density_matrix(pd_handle* h, double* out) {
   if (!h || !out) return pd_fail(PD_ERR_ARG, "NULL argument");
   if (!h->dr) return pd_fail(PD_ERR_ARG, "dynamic relaxation not initialised (pd_dr_init)");
   PD_CUDA(cudaSetDevice(h->device));
-  PD_CUDA(cudaMemcpy(out, h->dr->lam, sizeof(double) * h->n, cudaMemcpyDeviceToHost));
+  // ordered after pd_dr_init's kernels on the handle's (non-blocking) stream
+  PD_CUDA(cudaMemcpyAsync(out, h->dr->lam, sizeof(double) * h->n, cudaMemcpyDeviceToHost, h->stream));
+  PD_CUDA(cudaStreamSynchronize(h->stream));
   return PD_OK;
 }
 

@@ -917,6 +917,19 @@ int launch_force32(const DevBody& d, const LaunchCfg& c, int kstep, int phase, c
     return 1;
   }
   if (d.material == MAT_OSB) {
+    if (c.pipe == 5) {
+      // the packed kernels where they apply, the two-row kernels for the other phase
+      LaunchCfg c4 = c;
+      c4.pipe = 4;
+      const bool pa = A && pk_supported(d, 1), pb = B && pk_supported(d, 2);
+      if (A) launches += pa ? launch_force32_pk(d, c, kstep, 1, s)
+                            : (d.sc32 ? launch_osb32<true>(d, c4, G, grid, kstep, true, false, s)
+                                      : launch_osb32<false>(d, c4, G, grid, kstep, true, false, s));
+      if (B) launches += pb ? launch_force32_pk(d, c, kstep, 2, s)
+                            : (d.sc32 ? launch_osb32<true>(d, c4, G, grid, kstep, false, true, s)
+                                      : launch_osb32<false>(d, c4, G, grid, kstep, false, true, s));
+      return launches;
+    }
     if (d.sc32) return launch_osb32<true>(d, c, G, grid, kstep, A, B, s);
     return launch_osb32<false>(d, c, G, grid, kstep, A, B, s);
   }

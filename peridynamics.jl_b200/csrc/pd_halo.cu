@@ -192,7 +192,9 @@ extern "C" pd_status pd_vv_begin(pd_handle* h, int64_t first_step, int64_t n_ste
       if (!(p.dt > 0)) return pd_fail(PD_ERR_ARG, "dt <= 0 and no per-parameter time steps set");
   if (h->needs_table) {
     Ctrl c;
-    PD_CUDA(cudaMemcpy(&c, h->d.ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost));
+    // ordered after the handle's pending work (its stream is non-blocking)
+    PD_CUDA(cudaMemcpyAsync(&c, h->d.ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, h->stream));
+    PD_CUDA(cudaStreamSynchronize(h->stream));
     if (c.table_first > first_step || c.table_first + c.table_n < first_step + n_steps)
       return pd_fail(PD_ERR_ARG, "boundary condition values do not cover steps " + std::to_string(first_step) +
                                      ".." + std::to_string(first_step + n_steps - 1));

@@ -10,7 +10,8 @@ struct LaunchCfg {
   int block;  // threads per block
   bool exact; // FP64: one lane per point in the reference's serial summation order
   int pipe;   // FP32: 0 = plain loads, 1-3 = TMA-staged bond stream (pd_force32_tma.cu),
-              // 4 = two rows of neighbour gathers in flight (BB, OSB)
+              // 4 = two rows of neighbour gathers in flight (BB, OSB), 5 = OSB with packed
+              // x/y pairs (pd_force32_pk.cu; one lane per point, else as 4)
   int fullk;  // FP32 OSB / CMat: sum the weighted volumes / shape tensors in full (else
               // update the stored ones)
 };
@@ -54,6 +55,9 @@ int launch_force64(const DevBody& d, const LaunchCfg& c, int kstep, int phase, c
 int launch_force32(const DevBody& d, const LaunchCfg& c, int kstep, int phase, cudaStream_t s);
 bool tma_supported(const DevBody& d);
 int launch_force32_tma(const DevBody& d, int pipe, int kstep, int phase, cudaStream_t s);
+// packed-pair OSB kernels (pipe 5, pd_force32_pk.cu): phase 1 = A, 2 = B, 0 = both
+bool pk_supported(const DevBody& d, int phase);
+int launch_force32_pk(const DevBody& d, const LaunchCfg& c, int kstep, int phase, cudaStream_t s);
 void launch_cauchy64(const DevBody& d, const double* F, int from_h32, double* out, cudaStream_t s);
 
 // integration with the boundary conditions, one launch per step: mode 0 = kick from the stored

@@ -713,6 +713,9 @@ extern "C" pd_status pd_mpnn_create(int32_t device, pd_mpnn** out) {
     cudaMemset(net->grad, 0, sizeof(float) * N_PARAMS);
     cudaMemset(net->am, 0, sizeof(float) * N_PARAMS);
     cudaMemset(net->av, 0, sizeof(float) * N_PARAMS);
+    // the network's kernels run on the handles' non-blocking streams, which are not ordered
+    // after work on the legacy default stream: complete it here
+    if (cudaDeviceSynchronize() != cudaSuccess) st = PD_ERR_CUDA;
   }
   if (st != PD_OK) {
     for (void* p : net->allocs) cudaFree(p);
@@ -739,6 +742,7 @@ extern "C" pd_status pd_mpnn_set_params(pd_mpnn* net, const float* theta) {
   PD_CUDA(cudaMemset(net->grad, 0, sizeof(float) * N_PARAMS));
   PD_CUDA(cudaMemset(net->am, 0, sizeof(float) * N_PARAMS));
   PD_CUDA(cudaMemset(net->av, 0, sizeof(float) * N_PARAMS));
+  PD_CUDA(cudaDeviceSynchronize());  // see pd_mpnn_create
   net->adam_t = 0;
   net->weights_dirty = true;
   return PD_OK;
@@ -747,6 +751,7 @@ extern "C" pd_status pd_mpnn_set_params(pd_mpnn* net, const float* theta) {
 extern "C" pd_status pd_mpnn_get_params(pd_mpnn* net, float* theta) {
   if (!net || !theta) return pd_fail(PD_ERR_ARG, "NULL argument");
   PD_CUDA(cudaSetDevice(net->device));
+  PD_CUDA(cudaDeviceSynchronize());  // the last update may still run on a handle's stream
   PD_CUDA(cudaMemcpy(theta, net->theta, sizeof(float) * N_PARAMS, cudaMemcpyDeviceToHost));
   return PD_OK;
 }
@@ -842,7 +847,9 @@ extern "C" pd_status pd_mpnn_loss_grad(pd_mpnn* net, pd_handle* h, int32_t n_rec
 extern "C" pd_status pd_mpnn_zero_grad(pd_mpnn* net) {
   if (!net) return pd_fail(PD_ERR_ARG, "NULL argument");
   PD_CUDA(cudaSetDevice(net->device));
+  PD_CUDA(cudaDeviceSynchronize());
   PD_CUDA(cudaMemset(net->grad, 0, sizeof(float) * N_PARAMS));
+  PD_CUDA(cudaDeviceSynchronize());  // see pd_mpnn_create
   return PD_OK;
 }
 

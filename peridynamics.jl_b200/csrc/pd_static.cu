@@ -14,8 +14,11 @@
 // The arithmetic is the FP64 serial-order evaluation of pd_force64.cu (one thread per point,
 // the reference's order of operations and of the scattered terms), on the reference's CSR
 // bond arrays instead of the sliced layout.
+#include <cuda.h>
+
 #include <mutex>
 #include <string>
+#include <vector>
 
 #include "pdcuda.h"
 #include "pd_common.cuh"
@@ -95,23 +98,37 @@ __global__ void k_static_osb_a(StaticArgs a) {
   a.n_active[i] = na;
 }
 
+// position of point i in the sorted bond list of point j (the reverse bond j -> i), or -1
+__device__ __forceinline__ long long s_reverse(const StaticArgs& a, long long j, long long i) {
+  long long lo = a.off[j], hi = a.off[j + 1];
+  while (lo < hi) {
+    const long long mid = (lo + hi) >> 1;
+    if (a.nbr[mid] < i) lo = mid + 1; else hi = mid;
+  }
+  return (lo < a.off[j + 1] && a.nbr[lo] == i) ? lo : -1;
+}
+
 // force_density_point! (ordinary_state_based.jl:128-149) gathered in the serial order of the
-// scattered terms: neighbours j < i, the own bonds, neighbours j > i (sorted bond lists)
+// scattered terms: neighbours j < i, the own bonds, neighbours j > i (sorted bond lists). The
+// term of neighbour j is the one its own loop scatters (b_j's bond j -> i: its bond state and
+// its length), so bond states need not be the same in both directions.
 __global__ void k_static_osb_b(StaticArgs a) {
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= a.n) return;
   const double4 ci = a.state[i];
   double bx = 0.0, by = 0.0, bz = 0.0;
   const long long b0 = a.off[i], b1 = a.off[i + 1];
-  // the term of the bond j -> i of neighbour j (same bond state and length as i -> j)
   auto nbr_term = [&](long long b) {
     const long long j = a.nbr[b];
     const double4 cj = a.state[j];
     if (cj.z == 0.0) return;
+    const long long r = s_reverse(a, j, i);
+    if (r < 0) return;  // j has no bond to i: nothing is scattered into i
     double d[3];
     const double l = s_len(a.x, j, i, d);
-    const double om = a.bond_active[b] ? s_omega(a.kernel, a.delta, a.L[b]) : 0.0;
-    const double s = om * 1.0 * (cj.y * a.L[b] + cj.x * (l - a.L[b])) / l;
+    const double Lr = a.L[r];
+    const double om = a.bond_active[r] ? s_omega(a.kernel, a.delta, Lr) : 0.0;
+    const double s = om * 1.0 * (cj.y * Lr + cj.x * (l - Lr)) / l;
     bx += -(s * d[0]) * a.vol[j];
     by += -(s * d[1]) * a.vol[j];
     bz += -(s * d[2]) * a.vol[j];
@@ -142,10 +159,32 @@ using namespace pd;
 
 static thread_local std::string g_static_err;
 
-// Address of g_osb_state on each device, looked up once per device with that device current.
+// Device address of g_osb_state in each CUDA context that called, looked up once per context
+// with it current. The context is read through the driver's cuCtxGetCurrent (taken from the
+// runtime's driver entry points, so the library needs no link to libcuda); where that is not
+// available the key is the device's primary context, identified by the device index.
+struct StaticSlot {
+  CUcontext ctx;
+  int dev;
+  void* ptr;
+};
 static std::mutex g_static_mutex;
-static void* g_static_ptr[128];
-static bool g_static_ready[128];
+static std::vector<StaticSlot> g_static_slots;
+typedef CUresult (*CtxGetCurrentFn)(CUcontext*);
+
+static CtxGetCurrentFn ctx_get_current() {
+  static CtxGetCurrentFn fn = nullptr;
+  static bool looked = false;
+  if (!looked) {
+    looked = true;
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = (CtxGetCurrentFn)p;
+  }
+  return fn;
+}
 
 extern "C" const char* pd_static_last_error(void) { return g_static_err.c_str(); }
 
@@ -171,26 +210,45 @@ extern "C" pd_status pd_osb_force_static(int64_t n, const double* ref_position, 
     g_static_err = "every array must be a device pointer";
     return PD_ERR_ARG;
   }
+  // an error left by earlier CUDA work of this thread would be reported as this call's after
+  // the launches: report it now, launch nothing, and leave it pending for its owner
+  cudaError_t e = cudaPeekAtLastError();
+  if (e != cudaSuccess) {
+    g_static_err = std::string("a CUDA error from before this call is pending (") +
+                   cudaGetErrorString(e) + "); no kernel was launched";
+    return PD_ERR_CUDA;
+  }
   int dev = 0;
-  cudaError_t e = cudaGetDevice(&dev);
-  if (e != cudaSuccess || dev < 0 || dev >= 128) {
+  e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) {
     g_static_err = std::string("cudaGetDevice: ") + cudaGetErrorString(e);
     return PD_ERR_CUDA;
+  }
+  CUcontext ctx = nullptr;
+  if (CtxGetCurrentFn get = ctx_get_current()) {
+    if (get(&ctx) != CUDA_SUCCESS) ctx = nullptr;
   }
   void* state = nullptr;
   {
     std::lock_guard<std::mutex> lock(g_static_mutex);
-    if (!g_static_ready[dev]) {
-      // set-up of this device (the current one): the host-side name of the array is not a
+    for (const StaticSlot& sl : g_static_slots)
+      if (sl.dev == dev && sl.ctx == ctx) { state = sl.ptr; break; }
+    if (!state) {
+      // set-up in this context (the current one): the host-side name of the array is not a
       // device address, so its device address is looked up once
-      e = cudaGetSymbolAddress(&g_static_ptr[dev], g_osb_state);
+      e = cudaGetSymbolAddress(&state, g_osb_state);
       if (e != cudaSuccess) {
-        g_static_err = std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e);
+        g_static_err = std::string("cudaGetSymbolAddress of the scratch array on device ") +
+                       std::to_string(dev) + ": " + cudaGetErrorString(e);
         return PD_ERR_CUDA;
       }
-      g_static_ready[dev] = true;
+      if (ctx == nullptr && ctx_get_current() != nullptr) {
+        // cudaGetSymbolAddress made the primary context current
+        CUcontext now = nullptr;
+        if (ctx_get_current()(&now) == CUDA_SUCCESS) ctx = now;
+      }
+      g_static_slots.push_back({ctx, dev, state});
     }
-    state = g_static_ptr[dev];
   }
   StaticArgs a;
   a.n = n;

@@ -50,6 +50,7 @@ EXPORTS = (
     "pd_mpnn_infer", "pd_mpnn_loss_grad", "pd_mpnn_spectral_grad", "pd_mpnn_zero_grad",
     "pd_mpnn_adam",
     "pd_osb_force_static", "pd_static_last_error",
+    "pd_group_create", "pd_group_run_vv", "pd_group_destroy",
 )
 
 
@@ -185,6 +186,9 @@ def lib():
         "pd_mpnn_spectral_grad": [vp, vp, i32, vp, i32, vp, dbl, dbl, vp, vp],
         "pd_mpnn_zero_grad": [vp],
         "pd_mpnn_adam": [vp, C.c_float],
+        "pd_group_create": [vp, i32, vp],
+        "pd_group_run_vv": [vp, i64, i64, dbl, i32, vp],
+        "pd_group_destroy": [vp],
     }
     for name, args in sig.items():
         f = getattr(L, name)

@@ -274,10 +274,17 @@ class DeviceBody:
         st = L.lib().pd_run_vv(self.h, first_step, n_steps, dt)
         self._raise(st, None, dt)
 
-    def run_timed(self, first_step, n_steps, dt):
-        """run() with CUDA events around every kernel: (total, phase A, phase B, integrate) ms."""
+    def run_timed(self, first_step, n_steps, dt, phases=True):
+        """run() with CUDA events around every kernel: (total, phase A, phase B, integrate) ms.
+        phases=False: the steps as run() issues them (CUDA graphs when set_graph is on), timed
+        as a whole; returns the total ms."""
         self.tabulate_bcs(first_step, n_steps, dt)
         out = [C.c_double() for _ in range(4)]
+        if not phases:
+            st = L.lib().pd_run_vv_timed(self.h, first_step, n_steps, dt, C.byref(out[0]),
+                                         None, None, None)
+            self._raise(st, None, dt)
+            return out[0].value
         st = L.lib().pd_run_vv_timed(self.h, first_step, n_steps, dt, *[C.byref(o) for o in out])
         self._raise(st, None, dt)
         return tuple(o.value for o in out)

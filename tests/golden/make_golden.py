@@ -12,7 +12,9 @@ import os
 import re
 import sys
 
-ROOT = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+if len(sys.argv) != 2:
+    raise SystemExit("usage: python tests/golden/make_golden.py <path of the Peridynamics.jl tree>")
+ROOT = sys.argv[1]
 OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "reference_values.json")
 NUM = r"(-?\d+\.\d+(?:e-?\d+)?)"
 

@@ -92,3 +92,53 @@ def test_ensemble_with_filter_cracks_matches_specimens_run_alone():
         assert np.array_equal(ens.field("n_neighbors", k), ob.n_neighbors)
         assert np.array_equal(ens.field("displacement", k).T, ob.u)
     ens.close()
+
+
+@pytest.mark.parametrize("name,factory", [("OSB", pd.OSBMaterial),
+                                          ("C", lambda: pd.CMaterial(model=pd.NeoHooke()))])
+def test_size_classes_in_one_graph_match_specimens_run_alone(name, factory):
+    """Specimens cut into size classes (each class one device body with its own mapping),
+    advanced by one CUDA graph per block of steps: every specimen's trajectory is the one it
+    has alone — bit for bit in serial FP64 order (CMat within 1e-10: CUDA's and the C library's
+    log may differ in the last bit), within the FP32 tolerance with different lane mappings per
+    class."""
+    rng = np.random.default_rng(11)
+    bodies = []
+    for k in range(5):
+        nx, ny = int(rng.integers(8, 20)), int(rng.integers(5, 10))
+        bodies.append(specimen(factory, nx, ny, 3, E=float(rng.uniform(50e9, 200e9)),
+                               rho=float(rng.uniform(2000, 8000)),
+                               crack_frac=float(rng.uniform(0.1, 0.4)), seed=k))
+    n_steps = 48
+    refs = []
+    for b in bodies:
+        ob = oracle_body(b)
+        dt = ob.stable_timestep(0.7)
+        ob.force_density(0.0, dt)
+        assert ob.run_vv(1, n_steps, dt, oracle_bcs(b, 1, n_steps, dt)) == 0
+        refs.append((ob, dt))
+    for prec in ("fp64", "fp32"):
+        ens = pd.Ensemble(bodies, precision=prec, graph_steps=16, classes=3)
+        assert len(ens.devs) == 3 and sorted(sum(ens.members, [])) == list(range(5))
+        sizes = [max(bodies[k].n_points for k in m) for m in ens.members]
+        assert sizes == sorted(sizes)
+        if prec == "fp64":
+            ens.set_mapping(0)
+        else:
+            for d, g in zip(ens.devs, (1, 4, 32)):
+                d.set_mapping(g)
+        launches0 = ens.launch_count()
+        ens.run(n_steps)
+        assert ens.launch_count() > launches0
+        for k, (ob, dt) in enumerate(refs):
+            assert ens.dt[k] == dt
+            u = ens.field("displacement", k).T
+            if prec == "fp64":
+                if name == "C":
+                    assert np.abs(u - ob.u).max() <= 1e-10 * np.abs(ob.u).max()
+                else:
+                    assert np.array_equal(u, ob.u), (name, k)
+                assert np.array_equal(ens.field("bond_active", k), ob.bond_active[:ob.n_bonds])
+            else:
+                assert np.abs(u - ob.u).max() <= 1e-5 * np.abs(ob.u).max(), (name, k)
+        ens.close()

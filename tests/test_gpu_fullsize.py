@@ -156,6 +156,80 @@ def test_fp32_against_fp64_under_fracture(sims):
     assert rel_max <= 5e-2
 
 
+# stretch window of the one-step comparison: the FP32 stretch of a bond differs from the FP64
+# one by a few units of FP32 rounding of |du| / L (<= 1e-2 where bonds are about to fail), so
+# well below 1e-9; bonds whose FP64 stretch lies within this window of the critical stretch
+# are the ones whose decision the FP32 arithmetic may flip
+FLIP_WINDOW = 1e-8
+CHECK_STEPS = (1, 5, 10, 20, 30, 40, 50, 60)
+
+
+def test_fp32_failure_decisions_differ_only_within_rounding(blocks):
+    """Failure decisions of one FP32 step taken from the FP64 state, under fracture: the FP64
+    run (8 m/s) is stopped at several steps, its state (displacement, velocity, acceleration,
+    bond states) is loaded into an FP32 handle, and both take the next step. Both forms
+    integrate in FP64, so the displacements of that step are identical and the only
+    difference is the FP32 bond arithmetic: every bond state that differs afterwards must lie
+    within FLIP_WINDOW of the critical stretch in the FP64 run (counted by the device's
+    near-critical diagnostic at the positions of the decision). A flipped pair changes the
+    forces of its two points and, through their weighted volume and dilatation, of every
+    point bonded to them; the velocities of all other points agree to 1e-6."""
+    from scipy.spatial import cKDTree
+    body = blocks[8.0]
+    tree = cKDTree(body._pos)
+    delta = body.point_params[0].delta
+    d64 = pd.DeviceBody(body, precision="fp64")
+    d32 = pd.DeviceBody(body, precision="fp32")
+    offsets = np.concatenate(([0], np.cumsum(d64.field("n_neighbors"))))
+    try:
+        for d in (d64, d32):
+            d.break_random_pairs(BROKEN, SEED)
+        dt = d64.stable_timestep(0.7)
+        assert d32.stable_timestep(0.7) == dt
+        d64.force(0.0, dt)
+        done, rows = 0, []
+        for s in CHECK_STEPS:
+            if s - 1 > done:
+                d64.run(done + 1, s - 1 - done, dt)
+                done = s - 1
+            d32.set_state(displacement=d64.field("displacement"), velocity=d64.field("velocity"),
+                          acceleration=d64.field("acceleration"),
+                          bond_active=d64.field("bond_active"))
+            before = int(np.count_nonzero(d64.field("bond_active")))
+            d64.run(s, 1, dt)
+            d32.run(s, 1, dt)
+            done = s
+            s64, s32 = d64.field("bond_active"), d32.field("bond_active")
+            broke = before - int(np.count_nonzero(s64))
+            flipped = np.nonzero(s64 != s32)[0]
+            differ = len(flipped)
+            near = d64.near_critical(FLIP_WINDOW)
+            u64, u32 = d64.field("displacement"), d32.field("displacement")
+            v64, v32 = d64.field("velocity"), d32.field("velocity")
+            # points whose force a flipped pair changes: its endpoints (the owners of the two
+            # directed bonds) and every point within a horizon of them
+            touched = np.zeros(body.n_points, bool)
+            if differ:
+                ends = np.searchsorted(offsets, flipped, side="right") - 1
+                for nb in tree.query_ball_point(body._pos[np.unique(ends)], 1.0001 * delta):
+                    touched[nb] = True
+            keep = ~touched
+            v_rest = (np.abs(v32[:, keep] - v64[:, keep]).max() / np.abs(v64).max())
+            rows.append((s, broke, differ, near, rel_diff(u32, u64), rel_diff(v32, v64), v_rest))
+            print(f"step {s}: broke {broke}, differing {differ}, within {FLIP_WINDOW:g} of the "
+                  f"critical stretch {near}, displacement {rows[-1][4]:.2e}, velocity "
+                  f"{rows[-1][5]:.2e} (points away from flips: {v_rest:.2e}, "
+                  f"{int(touched.sum())} points near flips)")
+            assert np.array_equal(u32, u64)   # the same FP64 drift from the same state
+            assert differ <= near
+            assert near <= 1e-5 * d64.n_bonds  # the window is narrow enough to mean something
+            assert v_rest <= 1e-6
+        assert sum(r[1] for r in rows) > 100_000   # fracture is under way at the checks
+    finally:
+        d64.close()
+        d32.close()
+
+
 def test_fp32_is_deterministic(blocks, sims):
     ref = sims("fp32", 8.0)
     again = simulate(blocks[8.0], "fp32")

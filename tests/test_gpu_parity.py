@@ -369,3 +369,93 @@ def test_bb_two_row_kernel_equals_one_row(group):
     for a, b in zip(*res):
         assert np.array_equal(a, b)
 
+
+
+def packed_and_two_row(body, u=None, steps=0, bond_active=None):
+    """Forces, states and (after `steps` Velocity Verlet steps) displacements of the packed-pair
+    kernels (pipe 5) and of the two-row kernels (pipe 4), one lane per point."""
+    out = []
+    for pipe in (4, 5):
+        dev = pd.DeviceBody(body, precision="fp32")
+        dev.set_mapping(1, 256)
+        dev.set_pipeline(pipe)
+        assert dev.mapping() == (1, 256, pipe)
+        if bond_active is not None:
+            dev.set_state(bond_active=bond_active)
+        if u is not None:
+            dev.set_state(displacement=u)
+        dt = dev.stable_timestep(0.7)
+        dev.force(0.0, dt)
+        r = {f: dev.field(f) for f in ("b_int", "n_active_bonds", "bond_active", "damage")}
+        if steps:
+            dev.run(1, steps, dt)
+            r["displacement"] = dev.field("displacement")
+            r["bond_active_run"] = dev.field("bond_active")
+        out.append(r)
+        dev.close()
+    return out
+
+
+def test_packed_osb_kernels_force_against_oracle():
+    """Pipe 5 on a deformed cube with fracture: the oracle's force density within the FP32
+    tolerance, the same failure decisions as the two-row kernels."""
+    body = cube_body(pd.OSBMaterial(), n=9, fracture=True)
+    u = deform(body._pos, amplitude=0.002)
+    ob = oracle_body(body)
+    ob.pos[:] = body._pos + u
+    ob.force_density()
+    four, five = packed_and_two_row(body, u)
+    assert rel_err(five["b_int"].T, ob.b_int) < 2e-5
+    assert rel_err(five["b_int"], four["b_int"]) < 1e-6
+    for f in ("n_active_bonds", "bond_active", "damage"):
+        assert np.array_equal(five[f], four[f]), f
+
+
+def test_packed_osb_kernels_trajectory_against_oracle():
+    body = plate_body(pd.OSBMaterial(), nx=24, ny=12, nz=3, nu=0.25)
+    ob, _ = run_pair(body, 150, "fp64", mapping=0)
+    four, five = packed_and_two_row(body, steps=150)
+    assert rel_err(five["displacement"].T, ob.u) < 1e-5
+    broken_ref = np.count_nonzero(ob.bond_active[:ob.n_bonds] == 0)
+    broken = np.count_nonzero(five["bond_active_run"] == 0)
+    assert abs(broken - broken_ref) <= max(2, 0.01 * broken_ref)
+
+
+def test_packed_osb_kernels_with_one_directional_states():
+    """Bond states that differ between the two directions of a pair: phase A runs packed, phase
+    B falls back to the two-row kernel (it reads the reverse bonds' states)."""
+    body = cube_body(pd.OSBMaterial(), n=8)
+    ob = oracle_body(body)
+    ba = (np.random.default_rng(5).random(ob.n_bonds) > 0.2).astype(np.uint8)
+    u = deform(body._pos)
+    four, five = packed_and_two_row(body, u, bond_active=ba)
+    assert rel_err(five["b_int"], four["b_int"]) < 1e-6
+    assert np.array_equal(five["n_active_bonds"], four["n_active_bonds"])
+
+
+def test_bond_state_upload_is_ordered_before_its_use():
+    """pd_set_state's bond states reach the device before the kernels on the handle's
+    (non-blocking) stream read them, also when freshly allocated device memory holds old data:
+    device memory is filled with ones and returned to the driver first, then bond states that
+    differ between the two directions of some pairs are uploaded into new handles, whose FP64
+    serial-order force must equal the oracle's every time."""
+    import torch
+    junk = torch.full((1 << 30,), -1, dtype=torch.int32, device="cuda:0")   # 4 GiB
+    torch.cuda.synchronize()
+    del junk
+    torch.cuda.empty_cache()
+    body = cube_body(pd.OSBMaterial(kernel=pd.const_one_kernel), n=10, fracture=True, Gc=6e6)
+    ob = oracle_body(body)
+    ba = (np.random.default_rng(7).random(ob.n_bonds) > 0.15).astype(np.uint8)
+    ob.bond_active[:ob.n_bonds] = ba
+    x = body._pos + deform(body._pos, amplitude=4e-3)
+    ob.pos[:] = x
+    ob.force_density()
+    for _ in range(8):
+        dev = pd.DeviceBody(body, precision="fp64")
+        dev.set_mapping(0)
+        dev.set_state(position=x, bond_active=ba)
+        dev.force()
+        assert np.array_equal(dev.field("b_int").T, ob.b_int)
+        assert np.array_equal(dev.field("bond_active"), ob.bond_active[:ob.n_bonds])
+        dev.close()

@@ -917,7 +917,7 @@ int launch_force32(const DevBody& d, const LaunchCfg& c, int kstep, int phase, c
     return 1;
   }
   if (d.material == MAT_OSB) {
-    if (c.pipe >= 5) {
+    if (c.pipe == 5) {
       // the packed kernels where they apply, the two-row kernels for the other phase
       LaunchCfg c4 = c;
       c4.pipe = 4;

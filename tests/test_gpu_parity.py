@@ -371,15 +371,17 @@ def test_bb_two_row_kernel_equals_one_row(group):
 
 
 
-def packed_and_two_row(body, u=None, steps=0, bond_active=None):
+
+
+def packed_and_two_row(body, u=None, steps=0, bond_active=None, block=256):
     """Forces, states and (after `steps` Velocity Verlet steps) displacements of the packed-pair
     kernels (pipe 5) and of the two-row kernels (pipe 4), one lane per point."""
     out = []
     for pipe in (4, 5):
         dev = pd.DeviceBody(body, precision="fp32")
-        dev.set_mapping(1, 256)
+        dev.set_mapping(1, block)
         dev.set_pipeline(pipe)
-        assert dev.mapping() == (1, 256, pipe)
+        assert dev.mapping() == (1, block, pipe)
         if bond_active is not None:
             dev.set_state(bond_active=bond_active)
         if u is not None:
@@ -396,15 +398,16 @@ def packed_and_two_row(body, u=None, steps=0, bond_active=None):
     return out
 
 
-def test_packed_osb_kernels_force_against_oracle():
-    """Pipe 5 on a deformed cube with fracture: the oracle's force density within the FP32
-    tolerance, the same failure decisions as the two-row kernels."""
+@pytest.mark.parametrize("block", [128, 256])
+def test_packed_osb_kernels_force_against_oracle(block):
+    """The packed variants on a deformed cube with fracture: the oracle's force density within
+    the FP32 tolerance, the same failure decisions as the two-row kernels."""
     body = cube_body(pd.OSBMaterial(), n=9, fracture=True)
     u = deform(body._pos, amplitude=0.002)
     ob = oracle_body(body)
     ob.pos[:] = body._pos + u
     ob.force_density()
-    four, five = packed_and_two_row(body, u)
+    four, five = packed_and_two_row(body, u, block=block)
     assert rel_err(five["b_int"].T, ob.b_int) < 2e-5
     assert rel_err(five["b_int"], four["b_int"]) < 1e-6
     for f in ("n_active_bonds", "bond_active", "damage"):

@@ -988,6 +988,9 @@ def main():
     ap.add_argument("--replicas", action="store_true",
                     help="with --gpus N > 1 on a single-body config: N independent copies of the "
                          "body (weak scaling) instead of one body in N partitions")
+    ap.add_argument("--mapping", default="",
+                    help="lanes per point, block size, bond-stream variant (e.g. 1,128,5) instead "
+                         "of the autotuner's choice")
     ap.add_argument("--ens-classes", type=int, default=3,
                     help="ens64: size classes of specimens, each with its own mapping")
     ap.add_argument("--check-every", type=int, default=0,
@@ -1111,7 +1114,12 @@ def main():
 
     body, dev, dt = build(args.precision)
     n_pts, n_bonds, sym = dev.info()
-    group, block = dev.autotune()
+    if args.mapping:
+        g_, b_, p_ = (int(x) for x in args.mapping.split(","))
+        dev.set_mapping(g_, b_)
+        dev.set_pipeline(p_)
+    else:
+        dev.autotune()
     dev_mapping = dev.mapping()
     step = 1
     dev.run(step, args.warmup, dt)

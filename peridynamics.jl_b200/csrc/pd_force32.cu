@@ -19,6 +19,7 @@
 // terms of E = (H + H^T + H^T H) / 2 without cancelling subtractions.
 #include "pd_common.cuh"
 #include "pd_launch.h"
+#include "pd_pack.cuh"
 
 namespace pd {
 
@@ -835,6 +836,298 @@ __global__ void __launch_bounds__(256, PD_MINB_CB) k_c_b32(DevBody d, int kstep)
   }
 }
 
+// -------------------------------------------------------------------------------------------
+// CMat phases with packed pairs and the next row pair's bond stream in flight (bond-stream
+// variant 5; one lane per point, one parameter set; phase B for symmetric bond states). The
+// per-bond sums are those of k_c_a32 / k_c_b32: the x and y rows of every 3x3 sum are one
+// packed compensated pair, z is scalar; bond states select the contributions (inactive bonds
+// and padding slots gather their own point and add zero). The per-point epilogue of phase A is
+// k_c_a32's. Phase B: with one influence value for both directions, t_ij + the term of j is
+// w V_j ((A_i + A_j) xi + (beta_i + beta_j) du).
+// -------------------------------------------------------------------------------------------
+#ifndef PD_MINB_CQA
+#define PD_MINB_CQA 3
+#endif
+#ifndef PD_MINB_CQB
+#define PD_MINB_CQB 3
+#endif
+
+struct BondC {
+  float2 dxy;   // displacement difference, x and y
+  float dz;
+  float L, rL, eps;
+};
+
+__device__ __forceinline__ void bond_c(const float4& g, const float4& hj, const float4& lj,
+                                       const float2 nhi, const float nhz, const float2 nlo,
+                                       const float nlz, BondC& B) {
+  using namespace pack;
+  B.dxy = add2(add2(xy(hj), nhi), add2(xy(lj), nlo));
+  B.dz = (hj.z + nhz) + (lj.z + nlz);
+  const float2 exy = add2(xy(g), B.dxy);
+  const float ez = g.z + B.dz;
+  const float2 e2 = mul2(exy, exy);
+  const float l2 = fmaf(ez, ez, e2.x + e2.y);
+  const float l = l2 * rsqrtf(l2);
+  const float2 gd = mul2(xy(g), B.dxy);
+  const float xd = fmaf(g.z, B.dz, gd.x + gd.y);
+  const float2 d2 = mul2(B.dxy, B.dxy);
+  const float dd = fmaf(B.dz, B.dz, d2.x + d2.y);
+  B.L = fabsf(g.w);
+  B.rL = __fdividef(1.f, B.L);
+  B.eps = __fdividef(fmaf(2.f, xd, dd), l + B.L) * B.rL;
+}
+
+template <bool FULLK, bool LIN, int MB>
+__global__ void __launch_bounds__(256, MB) k_c_a32q(DevBody d, int kstep) {
+  using namespace pack;
+  if (d.ctrl->err) return;
+  const int lane = threadIdx.x & 31;
+  const long long warp0 = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+  for (long long s = warp0; s < d.nslices; s += nwarps) {
+    const long long i = s * 32 + lane;
+    const bool valid = i < d.n;
+    const int self = valid ? (int)i : 0;
+    const long long sbase = d.soff[s];
+    const int rows = (int)((d.soff[s + 1] - sbase) >> 5);
+    const int cnt = valid ? (int)(d.off[i + 1] - d.off[i]) : 0;
+    const unsigned meta = valid ? d.meta[i] : 0u;
+    const DevParam& P = d.params[meta & META_PID_MASK];
+    const float4 hi = d.uhi[self], lo = d.ulo[self];
+    const float2 nhi = make_float2(-hi.x, -hi.y), nlo = make_float2(-lo.x, -lo.y);
+    const float nhz = -hi.z, nlz = -lo.z;
+    const float epsc = P.epscf, id = P.inv_delta, vs = P.vscale;
+    const float2 id2 = make_float2(id, id);
+    const int* pn = d.nbr + sbase + lane;
+    const float4* pg = d.geo + sbase + lane;
+    unsigned* pw = d.bits + (sbase >> 5);
+    KSum2 K01, K23, K45;        // FULLK: (xx, yy), (zz, xy), (xz, yz)
+    KSum2 Hxy[3];               // rows x, y of column c of the displacement-gradient sum
+    KSum1 Hz[3];
+    float dK[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    int na = 0;
+    int nj0 = self, nj1 = self;
+    float4 ng0 = make_float4(0.f, 0.f, 0.f, 1.f), ng1 = ng0;
+    unsigned nw0 = 0u, nw1 = 0u;
+    auto load_pair = [&](int r) {
+      const bool two = r + 1 < rows;
+      nw0 = pw[r];
+      nw1 = two ? pw[r + 1] : 0u;
+      nj0 = __ldg(pn + 32 * r);
+      ng0 = __ldg(pg + 32 * r);
+      if (two) { nj1 = __ldg(pn + 32 * r + 32); ng1 = __ldg(pg + 32 * r + 32); }
+      else { nj1 = self; ng1 = make_float4(0.f, 0.f, 0.f, 1.f); }
+    };
+    if (rows > 0) load_pair(0);
+    for (int r = 0; r < rows; r += 2) {
+      const bool two = r + 1 < rows;
+      const unsigned w0 = nw0, w1 = nw1;
+      const bool a0 = (w0 >> lane) & 1u, a1 = (w1 >> lane) & 1u;
+      const int j0 = a0 ? nj0 : self, j1 = a1 ? nj1 : self;
+      const float4 g0 = ng0, g1 = ng1;
+      const float4 hj0 = __ldg(d.uhi + j0), lj0 = __ldg(d.ulo + j0);
+      const float4 hj1 = __ldg(d.uhi + j1), lj1 = __ldg(d.ulo + j1);
+      if (r + 2 < rows) load_pair(r + 2);
+      bool act0, act1;
+#pragma unroll
+      for (int u = 0; u < 2; u++) {
+        const float4& g = u ? g1 : g0;
+        const float4& hj = u ? hj1 : hj0;
+        const bool a = u ? a1 : a0;
+        BondC B;
+        bond_c(g, hj, u ? lj1 : lj0, nhi, nhz, nlo, nlz, B);
+        const bool act = a && !(B.eps > epsc && g.w > 0.f);
+        const float om = omega_t<LIN>(d.kernel, P.deltaf, B.L, B.rL) * hj.w * vs;
+        const float t = act ? om : 0.f;
+        const float2 X = mul2(xy(g), id2);
+        const float Xz = g.z * id;
+        const float2 tU = mul2(make_float2(t, t), mul2(B.dxy, id2));
+        const float tUz = t * (B.dz * id);
+        Hxy[0].add(mul2(tU, make_float2(X.x, X.x))); Hz[0].add(tUz * X.x);
+        Hxy[1].add(mul2(tU, make_float2(X.y, X.y))); Hz[1].add(tUz * X.y);
+        Hxy[2].add(mul2(tU, make_float2(Xz, Xz)));   Hz[2].add(tUz * Xz);
+        if constexpr (FULLK) {
+          const float2 tX = mul2(make_float2(t, t), X);
+          const float tXz = t * Xz;
+          K01.add(mul2(tX, X));
+          K23.add(make_float2(tXz * Xz, tX.x * X.y));
+          K45.add(mul2(tX, make_float2(Xz, Xz)));
+        } else if (a && !act) {
+          // the bond breaks now: its term leaves the stored shape tensor
+          dK[0] += om * X.x * X.x; dK[1] += om * X.y * X.y; dK[2] += om * Xz * Xz;
+          dK[3] += om * X.x * X.y; dK[4] += om * X.x * Xz; dK[5] += om * X.y * Xz;
+        }
+        if (u) act1 = act; else act0 = act;
+      }
+      na += (int)act0 + (int)act1;
+      const unsigned c0 = __ballot_sync(0xffffffffu, act0);
+      const unsigned c1 = __ballot_sync(0xffffffffu, act1);
+      if (lane == 0) {
+        if (c0 != w0) pw[r] = c0;
+        if (two && c1 != w1) pw[r + 1] = c1;
+      }
+    }
+    bool killed = false;
+    if (valid) {
+      float k6[6];
+      float2* ks = reinterpret_cast<float2*>(d.K32 + 6 * i);
+      if constexpr (FULLK) {
+        const float2 v01 = K01.value(), v23 = K23.value(), v45 = K45.value();
+        k6[0] = v01.x; k6[1] = v01.y; k6[2] = v23.x; k6[3] = v23.y; k6[4] = v45.x; k6[5] = v45.y;
+        ks[0] = make_float2(k6[0], k6[1]); ks[1] = make_float2(k6[2], k6[3]); ks[2] = make_float2(k6[4], k6[5]);
+      } else {
+        const float2 b0 = ks[0], b1 = ks[1], b2 = ks[2];
+        k6[0] = b0.x; k6[1] = b0.y; k6[2] = b1.x; k6[3] = b1.y; k6[4] = b2.x; k6[5] = b2.y;
+        if (dK[0] != 0.f || dK[1] != 0.f || dK[2] != 0.f) {  // a bond broke
+#pragma unroll
+          for (int q = 0; q < 6; q++) k6[q] -= dK[q];
+          ks[0] = make_float2(k6[0], k6[1]); ks[1] = make_float2(k6[2], k6[3]); ks[2] = make_float2(k6[4], k6[5]);
+        }
+      }
+      const float Km[9] = {k6[0], k6[3], k6[4],
+                           k6[3], k6[1], k6[5],
+                           k6[4], k6[5], k6[2]};
+      float Kinv[9], Hm[9], H[9];
+      finv3(Km, Kinv);
+#pragma unroll
+      for (int c = 0; c < 3; c++) {
+        const float2 v = Hxy[c].value();
+        Hm[3 * c] = v.x; Hm[3 * c + 1] = v.y; Hm[3 * c + 2] = Hz[c].value();
+      }
+      fmatmul(Hm, Kinv, H);
+      bool hasnan = false;
+      for (int q = 0; q < 9; q++) { d.H32[9 * i + q] = H[q]; hasnan |= isnan(H[q]); }
+      const double damage = 1.0 - (double)na / (double)cnt;
+      killed = (meta & META_KILLED) || (!(meta & META_HALO) && (damage > d.maxdmg || hasnan));
+      float4* cs = d.cst32 + 3 * i;
+      if (killed) {
+        if (!(meta & META_KILLED)) d.meta[i] = meta | META_KILLED;
+        na = 0;
+        cs[0] = make_float4(0.f, 0.f, 0.f, 0.f);
+        cs[1] = make_float4(0.f, 0.f, 0.f, 0.f);
+        cs[2] = make_float4(0.f, 0.f, 0.f, 0.f);
+      } else {
+        float Pm[9], PK[9], A[9];
+        pk1_32(d.cmodel, P, H, Pm);
+        fmatmul(Pm, Kinv, PK);
+        const float id5 = id * id * id * id * id;
+        for (int q = 0; q < 9; q++) A[q] = PK[q] * id5 - P.betaf * H[q];
+        cs[0] = make_float4(A[0], A[1], A[2], A[3]);
+        cs[1] = make_float4(A[4], A[5], A[6], A[7]);
+        cs[2] = make_float4(A[8], P.betaf, 0.f, 0.f);
+      }
+      d.n_active[i] = na;
+    }
+    if (!d.sym) {
+      // directed bond states: a killed point loses all its bonds (correspondence.jl:293)
+      const unsigned kill_mask = __ballot_sync(0xffffffffu, valid && killed);
+      if (kill_mask && lane == 0)
+        for (int r = 0; r < rows; r++) d.bits[(sbase >> 5) + r] &= ~kill_mask;
+    }
+  }
+}
+
+template <bool LIN, int MB>
+__global__ void __launch_bounds__(256, MB) k_c_b32q(DevBody d, int kstep) {
+  using namespace pack;
+  if (d.ctrl->err) return;
+  const int lane = threadIdx.x & 31;
+  const long long warp0 = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+  for (long long s = warp0; s < d.nslices; s += nwarps) {
+    const long long i = s * 32 + lane;
+    const bool valid = i < d.n;
+    const int self = valid ? (int)i : 0;
+    const long long sbase = d.soff[s];
+    const int rows = (int)((d.soff[s + 1] - sbase) >> 5);
+    const DevParam& P = d.params[d.meta[self] & META_PID_MASK];
+    const float delta = P.deltaf;
+    const float4 hi = d.uhi[self], lo = d.ulo[self];
+    const float2 nhi = make_float2(-hi.x, -hi.y), nlo = make_float2(-lo.x, -lo.y);
+    const float nhz = -hi.z, nlz = -lo.z;
+    const float4 ci0 = d.cst32[3 * (long long)self], ci1 = d.cst32[3 * (long long)self + 1],
+                 ci2 = d.cst32[3 * (long long)self + 2];
+    const int* pn = d.nbr + sbase + lane;
+    const float4* pg = d.geo + sbase + lane;
+    const unsigned* pw = d.bits + (sbase >> 5);
+    KSum2 bxy;
+    KSum1 bz;
+    int nj0 = self, nj1 = self;
+    float4 ng0 = make_float4(0.f, 0.f, 0.f, 1.f), ng1 = ng0;
+    unsigned nw0 = 0u, nw1 = 0u;
+    auto load_pair = [&](int r) {
+      const bool two = r + 1 < rows;
+      nw0 = __ldg(pw + r);
+      nw1 = two ? __ldg(pw + r + 1) : 0u;
+      nj0 = __ldg(pn + 32 * r);
+      ng0 = __ldg(pg + 32 * r);
+      if (two) { nj1 = __ldg(pn + 32 * r + 32); ng1 = __ldg(pg + 32 * r + 32); }
+      else { nj1 = self; ng1 = make_float4(0.f, 0.f, 0.f, 1.f); }
+    };
+    if (rows > 0) load_pair(0);
+    for (int r = 0; r < rows; r += 2) {
+      const bool a0 = (nw0 >> lane) & 1u, a1 = (nw1 >> lane) & 1u;
+      const int j0 = a0 ? nj0 : self, j1 = a1 ? nj1 : self;
+      const float4 g0 = ng0, g1 = ng1;
+      const float4 hj0 = __ldg(d.uhi + j0), lj0 = __ldg(d.ulo + j0);
+      const float4 hj1 = __ldg(d.uhi + j1), lj1 = __ldg(d.ulo + j1);
+      const float4* cj0 = d.cst32 + 3 * (long long)j0;
+      const float4* cj1 = d.cst32 + 3 * (long long)j1;
+      const float4 c00 = __ldg(cj0), c01 = __ldg(cj0 + 1), c02 = __ldg(cj0 + 2);
+      const float4 c10 = __ldg(cj1), c11 = __ldg(cj1 + 1), c12 = __ldg(cj1 + 2);
+      if (r + 2 < rows) load_pair(r + 2);
+#pragma unroll
+      for (int u = 0; u < 2; u++) {
+        const float4& g = u ? g1 : g0;
+        const float4& hj = u ? hj1 : hj0;
+        const float4& lj = u ? lj1 : lj0;
+        const float4& c0 = u ? c10 : c00;
+        const float4& c1 = u ? c11 : c01;
+        const float4& c2 = u ? c12 : c02;
+        const float2 dxy = add2(add2(xy(hj), nhi), add2(xy(lj), nlo));
+        const float dz = (hj.z + nhz) + (lj.z + nlz);
+        // S = A_i + A_j (column-major: columns (S0 S1 S2), (S3 S4 S5), (S6 S7 S8)); beta_i + beta_j
+        const float2 S01 = add2(make_float2(ci0.x, ci0.y), make_float2(c0.x, c0.y));
+        const float2 S23 = add2(make_float2(ci0.z, ci0.w), make_float2(c0.z, c0.w));
+        const float2 S45 = add2(make_float2(ci1.x, ci1.y), make_float2(c1.x, c1.y));
+        const float2 S67 = add2(make_float2(ci1.z, ci1.w), make_float2(c1.z, c1.w));
+        const float2 S8b = add2(make_float2(ci2.x, ci2.y), make_float2(c2.x, c2.y));
+        // rows x, y: S01 xi_x + (S3, S4) xi_y + S67 xi_z + beta du
+        const float2 S34 = make_float2(S23.y, S45.x);
+        float2 txy = mul2(make_float2(S8b.y, S8b.y), dxy);
+        txy = add2(txy, mul2(S01, make_float2(g.x, g.x)));
+        txy = add2(txy, mul2(S34, make_float2(g.y, g.y)));
+        txy = add2(txy, mul2(S67, make_float2(g.z, g.z)));
+        const float tz = fmaf(S23.x, g.x, fmaf(S45.y, g.y, fmaf(S8b.x, g.z, S8b.y * dz)));
+        const float L = fabsf(g.w);
+        float f = omega_of_f(LIN ? KER_LINEAR : d.kernel, delta, L) * hj.w;
+        f = (u ? a1 : a0) ? f : 0.f;
+        bxy.add(mul2(make_float2(f, f), txy));
+        bz.add(f * tz);
+      }
+    }
+    if (valid) {
+      const float2 v = bxy.value();
+      const float z = bz.value();
+      d.b32[3 * i] = v.x;
+      d.b32[3 * i + 1] = v.y;
+      d.b32[3 * i + 2] = z;
+      flag_nan32(d, kstep, v.x, v.y, z);
+    }
+  }
+}
+
+// the packed correspondence kernels: one lane per point, one parameter set; phase B also needs
+// symmetric bond states
+static bool cq_supported(const DevBody& d, int phase) {
+  if (d.material != MAT_CMAT || d.lg != 1 || d.multi) return false;
+  if (phase == 2 && !d.sym) return false;
+  return true;
+}
+
+bool packed_supported(const DevBody& d, int phase) { return pk_supported(d, phase) || cq_supported(d, phase); }
+
 // ------------------------------------------------------------------------------------------
 #define PD_DISPATCH_G(G, CALL)                          \
   switch (G) {                                          \
@@ -917,7 +1210,7 @@ int launch_force32(const DevBody& d, const LaunchCfg& c, int kstep, int phase, c
     return 1;
   }
   if (d.material == MAT_OSB) {
-    if (c.pipe == 5) {
+    if (c.pipe >= 5) {
       // the packed kernels where they apply, the two-row kernels for the other phase
       LaunchCfg c4 = c;
       c4.pipe = 4;
@@ -933,7 +1226,27 @@ int launch_force32(const DevBody& d, const LaunchCfg& c, int kstep, int phase, c
     if (d.sc32) return launch_osb32<true>(d, c, G, grid, kstep, A, B, s);
     return launch_osb32<false>(d, c, G, grid, kstep, A, B, s);
   }
-  if (A) {
+  const bool lin = d.kernel == KER_LINEAR;
+  if (A && c.pipe >= 5 && cq_supported(d, 1)) {
+    if (c.pipe == 5) {
+      if (c.fullk) {
+        if (lin) k_c_a32q<true, true, 3><<<grid, c.block, 0, s>>>(d, kstep);
+        else k_c_a32q<true, false, 3><<<grid, c.block, 0, s>>>(d, kstep);
+      } else {
+        if (lin) k_c_a32q<false, true, 3><<<grid, c.block, 0, s>>>(d, kstep);
+        else k_c_a32q<false, false, 3><<<grid, c.block, 0, s>>>(d, kstep);
+      }
+    } else {
+      if (c.fullk) {
+        if (lin) k_c_a32q<true, true, 2><<<grid, c.block, 0, s>>>(d, kstep);
+        else k_c_a32q<true, false, 2><<<grid, c.block, 0, s>>>(d, kstep);
+      } else {
+        if (lin) k_c_a32q<false, true, 2><<<grid, c.block, 0, s>>>(d, kstep);
+        else k_c_a32q<false, false, 2><<<grid, c.block, 0, s>>>(d, kstep);
+      }
+    }
+    launches++;
+  } else if (A) {
     if (d.kernel == KER_LINEAR) {
       if (c.fullk) { PD_DISPATCH_G(G, (k_c_a32<GG, true, true><<<grid, c.block, 0, s>>>(d, kstep))); }
       else { PD_DISPATCH_G(G, (k_c_a32<GG, false, true><<<grid, c.block, 0, s>>>(d, kstep))); }
@@ -944,7 +1257,16 @@ int launch_force32(const DevBody& d, const LaunchCfg& c, int kstep, int phase, c
     }
     launches++;
   }
-  if (B) {
+  if (B && c.pipe >= 5 && cq_supported(d, 2)) {
+    if (c.pipe == 5) {
+      if (lin) k_c_b32q<true, 3><<<grid, c.block, 0, s>>>(d, kstep);
+      else k_c_b32q<false, 3><<<grid, c.block, 0, s>>>(d, kstep);
+    } else {
+      if (lin) k_c_b32q<true, 2><<<grid, c.block, 0, s>>>(d, kstep);
+      else k_c_b32q<false, 2><<<grid, c.block, 0, s>>>(d, kstep);
+    }
+    launches++;
+  } else if (B) {
     if (d.sym) { PD_DISPATCH_G(G, (k_c_b32<GG, true><<<grid, c.block, 0, s>>>(d, kstep))); }
     else { PD_DISPATCH_G(G, (k_c_b32<GG, false><<<grid, c.block, 0, s>>>(d, kstep))); }
     launches++;

@@ -57,6 +57,8 @@ bool tma_supported(const DevBody& d);
 int launch_force32_tma(const DevBody& d, int pipe, int kstep, int phase, cudaStream_t s);
 // packed-pair OSB kernels (pipe 5, pd_force32_pk.cu): phase 1 = A, 2 = B, 0 = both
 bool pk_supported(const DevBody& d, int phase);
+// the packed kernels of OSB (pd_force32_pk.cu) or CMat (pd_force32.cu) apply to this phase
+bool packed_supported(const DevBody& d, int phase);
 int launch_force32_pk(const DevBody& d, const LaunchCfg& c, int kstep, int phase, cudaStream_t s);
 void launch_cauchy64(const DevBody& d, const double* F, int from_h32, double* out, cudaStream_t s);
 

@@ -373,11 +373,12 @@ def test_bb_two_row_kernel_equals_one_row(group):
 
 
 
-def packed_and_two_row(body, u=None, steps=0, bond_active=None, block=256):
+def packed_and_two_row(body, u=None, steps=0, bond_active=None, block=256, base=4):
     """Forces, states and (after `steps` Velocity Verlet steps) displacements of the packed-pair
-    kernels (pipe 5) and of the two-row kernels (pipe 4), one lane per point."""
+    kernels (pipe 5) and of the two-row kernels (pipe 4; CMat: the one-row kernels, pipe 0),
+    one lane per point."""
     out = []
-    for pipe in (4, 5):
+    for pipe in (base, 5):
         dev = pd.DeviceBody(body, precision="fp32")
         dev.set_mapping(1, block)
         dev.set_pipeline(pipe)
@@ -462,3 +463,27 @@ def test_bond_state_upload_is_ordered_before_its_use():
         assert np.array_equal(dev.field("b_int").T, ob.b_int)
         assert np.array_equal(dev.field("bond_active"), ob.bond_active[:ob.n_bonds])
         dev.close()
+
+
+@pytest.mark.parametrize("model", ["C-SVK", "C-NH", "C-NHP"])
+def test_packed_cmat_kernels_against_oracle(model):
+    """The packed correspondence kernels (pipe 5): force density on a deformed cube with
+    fracture within the FP32 tolerance of the oracle and 1e-6 of the one-row kernels, the same
+    failure decisions; a 150-step fracturing plate within 1e-5 of the oracle."""
+    body = cube_body(MATERIALS[model](), n=8, fracture=True)
+    u = deform(body._pos, amplitude=0.002)
+    ob = oracle_body(body)
+    ob.pos[:] = body._pos + u
+    ob.force_density()
+    one, five = packed_and_two_row(body, u, base=0)
+    assert rel_err(five["b_int"].T, ob.b_int) < 2e-5
+    assert rel_err(five["b_int"], one["b_int"]) < 1e-6
+    for f in ("n_active_bonds", "bond_active", "damage"):
+        assert np.array_equal(five[f], one[f]), f
+    body = plate_body(MATERIALS[model](), nx=24, ny=12, nz=3, nu=0.25)
+    ob, _ = run_pair(body, 150, "fp64", mapping=0)
+    one, five = packed_and_two_row(body, steps=150, base=0)
+    assert rel_err(five["displacement"].T, ob.u) < 1e-5
+    broken_ref = np.count_nonzero(ob.bond_active[:ob.n_bonds] == 0)
+    broken = np.count_nonzero(five["bond_active_run"] == 0)
+    assert abs(broken - broken_ref) <= max(2, 0.01 * broken_ref)

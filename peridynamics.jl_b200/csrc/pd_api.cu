@@ -1542,10 +1542,10 @@ extern "C" pd_status pd_get_mapping(pd_handle* h, int32_t* group, int32_t* block
 
 extern "C" pd_status pd_set_pipeline(pd_handle* h, int32_t pipe) {
   if (!h) return fail(PD_ERR_ARG, "handle is NULL");
-  if (pipe < 0 || pipe > 6) return fail(PD_ERR_ARG, "pipe must be 0 to 6");
+  if (pipe < 0 || pipe > 5) return fail(PD_ERR_ARG, "pipe must be 0 to 5");
   if (pipe == 4 && (h->precision != PD_PREC_FP32_KAHAN || h->material == PD_MAT_CMAT))
     return fail(PD_ERR_ARG, "the two-row kernels are the FP32 BB and OSB ones");
-  if (pipe >= 5 && (h->precision != PD_PREC_FP32_KAHAN || h->material == PD_MAT_BB))
+  if (pipe == 5 && (h->precision != PD_PREC_FP32_KAHAN || h->material == PD_MAT_BB))
     return fail(PD_ERR_ARG, "the packed-pair kernels are the FP32 OSB and CMat ones");
   if (pipe >= 1 && pipe <= 3 && (h->precision != PD_PREC_FP32_KAHAN || !tma_supported(h->d)))
     return fail(PD_ERR_ARG, "the staged bond stream needs the FP32 path, one lane per point and BB or OSB");

@@ -845,6 +845,10 @@ __global__ void __launch_bounds__(256, PD_MINB_CB) k_c_b32(DevBody d, int kstep)
 // k_c_a32's. Phase B: with one influence value for both directions, t_ij + the term of j is
 // w V_j ((A_i + A_j) xi + (beta_i + beta_j) du).
 // -------------------------------------------------------------------------------------------
+// occupancy bound of both packed correspondence phases: 3 resident blocks of 256 threads (80
+// registers, with 48-100 bytes of spills). Measured on the 1M-point CMat block: step 1.445 ms
+// at 3 blocks against 1.686 ms at 2 (110 registers, no spills) and 1.865 ms for the one-row
+// kernels.
 #ifndef PD_MINB_CQA
 #define PD_MINB_CQA 3
 #endif
@@ -878,8 +882,8 @@ __device__ __forceinline__ void bond_c(const float4& g, const float4& hj, const 
   B.eps = __fdividef(fmaf(2.f, xd, dd), l + B.L) * B.rL;
 }
 
-template <bool FULLK, bool LIN, int MB>
-__global__ void __launch_bounds__(256, MB) k_c_a32q(DevBody d, int kstep) {
+template <bool FULLK, bool LIN>
+__global__ void __launch_bounds__(256, PD_MINB_CQA) k_c_a32q(DevBody d, int kstep) {
   using namespace pack;
   if (d.ctrl->err) return;
   const int lane = threadIdx.x & 31;
@@ -914,9 +918,9 @@ __global__ void __launch_bounds__(256, MB) k_c_a32q(DevBody d, int kstep) {
       const bool two = r + 1 < rows;
       nw0 = pw[r];
       nw1 = two ? pw[r + 1] : 0u;
-      nj0 = __ldg(pn + 32 * r);
-      ng0 = __ldg(pg + 32 * r);
-      if (two) { nj1 = __ldg(pn + 32 * r + 32); ng1 = __ldg(pg + 32 * r + 32); }
+      nj0 = ld_stream(pn + 32 * r);
+      ng0 = ld_stream(pg + 32 * r);
+      if (two) { nj1 = ld_stream(pn + 32 * r + 32); ng1 = ld_stream(pg + 32 * r + 32); }
       else { nj1 = self; ng1 = make_float4(0.f, 0.f, 0.f, 1.f); }
     };
     if (rows > 0) load_pair(0);
@@ -1028,8 +1032,8 @@ __global__ void __launch_bounds__(256, MB) k_c_a32q(DevBody d, int kstep) {
   }
 }
 
-template <bool LIN, int MB>
-__global__ void __launch_bounds__(256, MB) k_c_b32q(DevBody d, int kstep) {
+template <bool LIN>
+__global__ void __launch_bounds__(256, PD_MINB_CQB) k_c_b32q(DevBody d, int kstep) {
   using namespace pack;
   if (d.ctrl->err) return;
   const int lane = threadIdx.x & 31;
@@ -1058,11 +1062,11 @@ __global__ void __launch_bounds__(256, MB) k_c_b32q(DevBody d, int kstep) {
     unsigned nw0 = 0u, nw1 = 0u;
     auto load_pair = [&](int r) {
       const bool two = r + 1 < rows;
-      nw0 = __ldg(pw + r);
-      nw1 = two ? __ldg(pw + r + 1) : 0u;
-      nj0 = __ldg(pn + 32 * r);
-      ng0 = __ldg(pg + 32 * r);
-      if (two) { nj1 = __ldg(pn + 32 * r + 32); ng1 = __ldg(pg + 32 * r + 32); }
+      nw0 = ld_stream(pw + r);
+      nw1 = two ? ld_stream(pw + r + 1) : 0u;
+      nj0 = ld_stream(pn + 32 * r);
+      ng0 = ld_stream(pg + 32 * r);
+      if (two) { nj1 = ld_stream(pn + 32 * r + 32); ng1 = ld_stream(pg + 32 * r + 32); }
       else { nj1 = self; ng1 = make_float4(0.f, 0.f, 0.f, 1.f); }
     };
     if (rows > 0) load_pair(0);
@@ -1210,7 +1214,7 @@ int launch_force32(const DevBody& d, const LaunchCfg& c, int kstep, int phase, c
     return 1;
   }
   if (d.material == MAT_OSB) {
-    if (c.pipe >= 5) {
+    if (c.pipe == 5) {
       // the packed kernels where they apply, the two-row kernels for the other phase
       LaunchCfg c4 = c;
       c4.pipe = 4;
@@ -1227,23 +1231,13 @@ int launch_force32(const DevBody& d, const LaunchCfg& c, int kstep, int phase, c
     return launch_osb32<false>(d, c, G, grid, kstep, A, B, s);
   }
   const bool lin = d.kernel == KER_LINEAR;
-  if (A && c.pipe >= 5 && cq_supported(d, 1)) {
-    if (c.pipe == 5) {
-      if (c.fullk) {
-        if (lin) k_c_a32q<true, true, 3><<<grid, c.block, 0, s>>>(d, kstep);
-        else k_c_a32q<true, false, 3><<<grid, c.block, 0, s>>>(d, kstep);
-      } else {
-        if (lin) k_c_a32q<false, true, 3><<<grid, c.block, 0, s>>>(d, kstep);
-        else k_c_a32q<false, false, 3><<<grid, c.block, 0, s>>>(d, kstep);
-      }
+  if (A && c.pipe == 5 && cq_supported(d, 1)) {
+    if (c.fullk) {
+      if (lin) k_c_a32q<true, true><<<grid, c.block, 0, s>>>(d, kstep);
+      else k_c_a32q<true, false><<<grid, c.block, 0, s>>>(d, kstep);
     } else {
-      if (c.fullk) {
-        if (lin) k_c_a32q<true, true, 2><<<grid, c.block, 0, s>>>(d, kstep);
-        else k_c_a32q<true, false, 2><<<grid, c.block, 0, s>>>(d, kstep);
-      } else {
-        if (lin) k_c_a32q<false, true, 2><<<grid, c.block, 0, s>>>(d, kstep);
-        else k_c_a32q<false, false, 2><<<grid, c.block, 0, s>>>(d, kstep);
-      }
+      if (lin) k_c_a32q<false, true><<<grid, c.block, 0, s>>>(d, kstep);
+      else k_c_a32q<false, false><<<grid, c.block, 0, s>>>(d, kstep);
     }
     launches++;
   } else if (A) {
@@ -1257,14 +1251,9 @@ int launch_force32(const DevBody& d, const LaunchCfg& c, int kstep, int phase, c
     }
     launches++;
   }
-  if (B && c.pipe >= 5 && cq_supported(d, 2)) {
-    if (c.pipe == 5) {
-      if (lin) k_c_b32q<true, 3><<<grid, c.block, 0, s>>>(d, kstep);
-      else k_c_b32q<false, 3><<<grid, c.block, 0, s>>>(d, kstep);
-    } else {
-      if (lin) k_c_b32q<true, 2><<<grid, c.block, 0, s>>>(d, kstep);
-      else k_c_b32q<false, 2><<<grid, c.block, 0, s>>>(d, kstep);
-    }
+  if (B && c.pipe == 5 && cq_supported(d, 2)) {
+    if (lin) k_c_b32q<true><<<grid, c.block, 0, s>>>(d, kstep);
+    else k_c_b32q<false><<<grid, c.block, 0, s>>>(d, kstep);
     launches++;
   } else if (B) {
     if (d.sym) { PD_DISPATCH_G(G, (k_c_b32<GG, true><<<grid, c.block, 0, s>>>(d, kstep))); }

@@ -18,7 +18,9 @@
 // phases are bound by the latency of the bond stream and the neighbour gathers that depend on
 // it, not by issue. The freed registers therefore hold the next row pair's stream records,
 // loaded after the current pair's gathers and before its arithmetic, so the DRAM latency of
-// the stream overlaps the gathers and arithmetic of the pair before it.
+// the stream overlaps the gathers and arithmetic of the pair before it. The stream loads are
+// streaming (evict-first) loads, so that the bond records, read once, leave L2 to the
+// neighbours' point records.
 // The arithmetic is the FP32 form of pd_force32.cu (deformed bond vector from the stored
 // reference offset, cancellation-free extension, Kahan sums); roundings differ from the
 // two-row kernels only in the order of a few operations.
@@ -111,11 +113,11 @@ __global__ void __launch_bounds__(256, PD_MINB_QB) k_osb_b32q(DevBody d, int kst
     unsigned nw0 = 0u, nw1 = 0u;
     auto load_pair = [&](int r) {
       const bool two = r + 1 < rows;
-      nw0 = __ldg(pw + r);
-      nw1 = two ? __ldg(pw + r + 1) : 0u;
-      nj0 = __ldg(pn + 32 * r);
-      ng0 = __ldg(pg + 32 * r);
-      if (two) { nj1 = __ldg(pn + 32 * r + 32); ng1 = __ldg(pg + 32 * r + 32); }
+      nw0 = ld_stream(pw + r);
+      nw1 = two ? ld_stream(pw + r + 1) : 0u;
+      nj0 = ld_stream(pn + 32 * r);
+      ng0 = ld_stream(pg + 32 * r);
+      if (two) { nj1 = ld_stream(pn + 32 * r + 32); ng1 = ld_stream(pg + 32 * r + 32); }
       else { nj1 = self; ng1 = make_float4(0.f, 0.f, 0.f, 1.f); }
     };
     if (rows > 0) load_pair(0);
@@ -190,9 +192,9 @@ __global__ void __launch_bounds__(256, PD_MINB_QA) k_osb_a32q(DevBody d, int kst
       const bool two = r + 1 < rows;
       nw0 = pw[r];
       nw1 = two ? pw[r + 1] : 0u;
-      nj0 = __ldg(pn + 32 * r);
-      ng0 = __ldg(pg + 32 * r);
-      if (two) { nj1 = __ldg(pn + 32 * r + 32); ng1 = __ldg(pg + 32 * r + 32); }
+      nj0 = ld_stream(pn + 32 * r);
+      ng0 = ld_stream(pg + 32 * r);
+      if (two) { nj1 = ld_stream(pn + 32 * r + 32); ng1 = ld_stream(pg + 32 * r + 32); }
       else { nj1 = self; ng1 = make_float4(0.f, 0.f, 0.f, 1.f); }
     };
     if (rows > 0) load_pair(0);

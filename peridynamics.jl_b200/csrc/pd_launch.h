@@ -10,8 +10,8 @@ struct LaunchCfg {
   int block;  // threads per block
   bool exact; // FP64: one lane per point in the reference's serial summation order
   int pipe;   // FP32: 0 = plain loads, 1-3 = TMA-staged bond stream (pd_force32_tma.cu),
-              // 4 = two rows of neighbour gathers in flight (BB, OSB), 5 = OSB with packed
-              // x/y pairs (pd_force32_pk.cu; one lane per point, else as 4)
+              // 4 = two rows of neighbour gathers in flight (BB, OSB), 5 = OSB / CMat with
+              // packed x/y pairs and the next row pair's stream in flight (one lane per point)
   int fullk;  // FP32 OSB / CMat: sum the weighted volumes / shape tensors in full (else
               // update the stored ones)
 };

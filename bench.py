@@ -39,6 +39,8 @@ CONFIGS = {
     "osb1m": (200, 100, 50, 1e-3, "OSB", 0.0, 0.6),
     "bb1m": (200, 100, 50, 1e-3, "BB", 0.0, 0.6),
     "c1m": (200, 100, 50, 1e-3, "C", 0.0, 0.6),
+    # the same block with ZEMWan's stabilisation (CW: NeoHooke, C : K^-1 per point)
+    "cwan1m": (200, 100, 50, 1e-3, "CW", 0.0, 0.6),
     # jittered OSB block with a velocity pulse and a slit: the FP32 / FP64 precision study
     "pulse1m": (200, 100, 50, 1e-3, "OSB", 0.0, 0.0),
     # 64 CMat NeoHooke specimens of 20k-200k points in one device body (see make_ensemble)
@@ -47,7 +49,7 @@ CONFIGS = {
     "dr1m": (200, 100, 50, 1e-3, "OSB", 0.0, 0.0),
 }
 # configs of one body (the multi-GPU run partitions them; --replicas runs copies instead)
-SINGLE_BODY = ("osb8m", "plate3200", "osb1m", "bb1m", "c1m")
+SINGLE_BODY = ("osb8m", "plate3200", "osb1m", "bb1m", "c1m", "cwan1m")
 DR_STRAIN = 5e-5
 # algorithmic bytes per point of the damping and velocity-update kernels of one relaxation step
 # (damping: u, v_half, b_int, b_int_old, v_half_old, Lambda; update: Lambda, b_int, b_ext,
@@ -56,10 +58,10 @@ DR_STRAIN = 5e-5
 B_DR_POINT = {"fp64": 304.0, "fp32": 280.0}
 # algorithmic bytes (FP32-compensated form): per directed bond nbr 4 + xi 12 + L 4 + 1/8 bit;
 # per point 140 (u, v FP64 read+write, own u, b_ext/BC, parameter id, damage) + 8 for OSB
-# (m, theta) + 72 for CMat (F, P K^-1)
+# (m, theta) + 72 for CMat (F, P K^-1) + 24 with ZEMWan (the symmetric stiffness C : K^-1)
 B_BOND = {"fp32": 20.125, "fp64": 36.125}
 B_POINT = {"fp32": 140.0, "fp64": 184.0}
-B_POINT_EXTRA = {"BB": 0.0, "OSB": 8.0, "C": 72.0}
+B_POINT_EXTRA = {"BB": 0.0, "OSB": 8.0, "C": 72.0, "CW": 96.0}
 
 
 def pinned(*shape):
@@ -89,11 +91,12 @@ def make_body(cfg, jitter_seed=None, correction=None):
     lx, ly, lz = nx * dx, ny * dx, nz * dx
     pos, vol = pd.uniform_box(lx, ly, lz, dx)
     corr = pd.EnergySurfaceCorrection if correction == "energy" else None
-    if corr is not None and mat == "C":
+    if corr is not None and mat in ("C", "CW"):
         raise ValueError("the surface correction is available for BB and OSB")
     material = {"OSB": lambda: pd.OSBMaterial(correction=corr),
                 "BB": lambda: pd.BBMaterial(correction=corr),
-                "C": lambda: pd.CMaterial(model=pd.NeoHooke())}[mat]()
+                "C": lambda: pd.CMaterial(model=pd.NeoHooke()),
+                "CW": lambda: pd.CMaterial(model=pd.NeoHooke(), zem=pd.ZEMWan())}[mat]()
     body = pd.Body(material, pos, vol)
     kw = dict(horizon=3.015 * dx, rho=2700.0, E=70e9, Gc=100.0)
     if mat != "BB":
@@ -137,7 +140,8 @@ def make_dr_block(nx, ny, nz, dx, mat="OSB"):
     import pdcuda as pd
     pos, vol = pd.uniform_box(nx * dx, ny * dx, nz * dx, dx)
     material = {"OSB": pd.OSBMaterial, "BB": pd.BBMaterial,
-                "C": lambda: pd.CMaterial(model=pd.NeoHooke())}[mat]()
+                "C": lambda: pd.CMaterial(model=pd.NeoHooke()),
+                "CW": lambda: pd.CMaterial(model=pd.NeoHooke(), zem=pd.ZEMWan())}[mat]()
     body = pd.Body(material, pos, vol)
     kw = dict(horizon=3.015 * dx, rho=2700.0, E=70e9, Gc=100.0)
     if mat != "BB":
@@ -505,11 +509,12 @@ def oracle_sample(cfg, threads):
     X = np.array(np.meshgrid(g(sx), g(sy), g(sz), indexing="ij")).reshape(3, -1).T
     X = np.ascontiguousarray(X[np.lexsort((X[:, 0], X[:, 1], X[:, 2]))])
     V = np.full(len(X), dx ** 3)
-    om = {"OSB": O.OSB, "BB": O.BB, "C": O.CMAT}[mat]
+    om = {"OSB": O.OSB, "BB": O.BB, "C": O.CMAT, "CW": O.CMAT}[mat]
     kw = {} if mat == "BB" else {"nu": 0.25}
     p = O.point_params(om, 3.015 * dx, 2700.0, E=70e9, Gc=100.0, **kw)
     O.set_threads(threads)
-    b = O.OracleBody(om, X, V, [p], cmodel=O.NEOHOOKE)
+    b = O.OracleBody(om, X, V, [p], cmodel=O.NEOHOOKE,
+                     zem=O.ZEM_WAN if mat == "CW" else O.ZEM_SILLING)
     dt = b.stable_timestep(0.7)
     b.v[:, 1] = np.where(X[:, 1] > 0, vbc, -vbc)
     b.force_density(0.0, dt)
@@ -569,7 +574,7 @@ def dr_oracle_sample(cfg, threads):
     X = np.array(np.meshgrid(g(sx), g(sy), g(sz), indexing="ij")).reshape(3, -1).T
     X = np.ascontiguousarray(X[np.lexsort((X[:, 0], X[:, 1], X[:, 2]))])
     V = np.full(len(X), dx ** 3)
-    om = {"OSB": O.OSB, "BB": O.BB, "C": O.CMAT}[mat]
+    om = {"OSB": O.OSB, "BB": O.BB, "C": O.CMAT, "CW": O.CMAT}[mat]
     kw = {} if mat == "BB" else {"nu": 0.25}
     p = O.point_params(om, 3.015 * dx, 2700.0, E=70e9, Gc=100.0, **kw)
     O.set_threads(threads)

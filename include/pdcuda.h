@@ -47,6 +47,10 @@ typedef int32_t pd_status;
 #define PD_CM_NEOHOOKE 1
 #define PD_CM_NEOHOOKE_PENALTY 2
 
+/* CMat zero-energy mode stabilisation (src/discretization/zem_stabilization.jl) */
+#define PD_ZEM_SILLING 0  /* ZEMSilling(Cs), zem_stabilization.jl:16-21 */
+#define PD_ZEM_WAN 1      /* ZEMWan(), zem_stabilization.jl:30-42 (stiffness C : K^-1 per point) */
+
 /* influence functions (src/discretization/kernels.jl:10-52) */
 #define PD_KERNEL_CONST_ONE 0
 #define PD_KERNEL_LINEAR 1
@@ -110,6 +114,7 @@ typedef struct {
     double zem_cs;                 /* ZEMSilling Cs (zem_stabilization.jl:16-21), default 0.5 */
     double maxdmg;                 /* CMaterial maxdmg (correspondence.jl:123-128), default 0.85 */
     int32_t device;                /* CUDA device ordinal */
+    int32_t zem;                   /* PD_ZEM_* (CMat); 0 (ZEMSilling with zem_cs) when zeroed */
 } pd_body_desc;
 
 /* One boundary condition on one point set and one dimension. */

@@ -21,6 +21,7 @@ _LIB = None
 BB, OSB, CMAT = 0, 1, 2
 SVK, NEOHOOKE, NHPENALTY = 0, 1, 2
 KERNEL_CONST_ONE, KERNEL_LINEAR, KERNEL_CUBIC_BSPLINE = 0, 1, 2
+ZEM_SILLING, ZEM_WAN = 0, 1
 
 
 class Params(C.Structure):
@@ -35,7 +36,7 @@ class Sys(C.Structure):
                 ("omega", C.c_void_p), ("pid", C.c_void_p), ("params", C.c_void_p),
                 ("n_params", C.c_int32), ("material", C.c_int32), ("cmodel", C.c_int32),
                 ("multi", C.c_int32), ("zem_cs", C.c_double), ("maxdmg", C.c_double),
-                ("scfactor", C.c_void_p)]
+                ("scfactor", C.c_void_p), ("zem", C.c_int32)]
 
 
 class State(C.Structure):
@@ -78,6 +79,7 @@ def lib():
         L.or_run_vv.argtypes = [vp, vp, vp, i32, i64, i64, dbl]
         L.or_first_piola_kirchhoff.argtypes = [i32, vp, vp, vp]
         L.or_inv3.argtypes = [vp, vp]
+        L.or_zem_wan_stiffness.argtypes = [vp, vp, vp]
         L.or_det3.restype = dbl
         L.or_det3.argtypes = [vp]
         L.or_point_params.restype = C.c_int
@@ -93,6 +95,15 @@ def lib():
 
 def _p(a):
     return None if a is None else a.ctypes.data
+
+
+def zem_wan_stiffness(params, Kinv):
+    """ZEMWan's C_1 = C : K^-1 (zem_stabilization.jl:32-42) for one parameter set and one
+    3x3 inverse shape tensor."""
+    k = np.asfortranarray(Kinv, dtype=np.float64)
+    out = np.zeros((3, 3), np.float64, order="F")
+    lib().or_zem_wan_stiffness(C.byref(params), k.ctypes.data, out.ctypes.data)
+    return out
 
 
 def point_params(material, horizon, rho, E=np.nan, nu=np.nan, G=np.nan, K=np.nan,
@@ -138,7 +149,7 @@ class OracleBody:
 
     def __init__(self, material, X, vol, params, pid=None, off=None, nbr=None, L=None,
                  fail_permit=None, kernel=KERNEL_LINEAR, cmodel=SVK, multi=None,
-                 zem_cs=0.5, maxdmg=0.85, fp_point=None, cracks=()):
+                 zem_cs=0.5, maxdmg=0.85, fp_point=None, cracks=(), zem=0):
         self.X = np.ascontiguousarray(X, dtype=np.float64).reshape(-1, 3)
         n = self.X.shape[0]
         self.n = n
@@ -165,7 +176,7 @@ class OracleBody:
         self.sys = Sys(n, B, _p(self.X), _p(self.vol), _p(self.off), _p(self.nbr), _p(self.L),
                        _p(self.fail_permit), _p(self.omega), _p(self.pid),
                        C.cast(self.params, C.c_void_p), len(params), material, cmodel, multi,
-                       zem_cs, maxdmg, None)
+                       zem_cs, maxdmg, None, int(zem))
         lib().or_kernels(C.byref(self.sys), kernel, _p(self.omega))
         z3 = lambda: np.zeros((n, 3), np.float64)
         self.pos, self.u, self.v, self.vh, self.a, self.b_int, self.b_ext = (z3() for _ in range(7))

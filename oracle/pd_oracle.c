@@ -513,7 +513,53 @@ void or_first_piola_kirchhoff(int32_t cmodel, const or_params *p, const double *
     matmul3(F, S, P);
 }
 
-/* CMaterial: correspondence.jl:183-251, 288-298; stress.jl:112-116 */
+/* Hooke tensor entry C[i,j,k,l] (0-based) as get_hooke_matrix builds it from the Voigt matrix
+ * (constitutive_models.jl:107-133): Voigt index of (i,j) in the order (1,1), (2,2), (3,3),
+ * (2,3), (1,3), (1,2); a = (1 - nu) lambda / nu on the diagonal of the normal block, lambda off
+ * it, mu on the diagonal of the shear block, zero elsewhere. */
+static int voigt_index(int i, int j) {
+    if (i == j) return i;
+    int m = i + j;  /* {1,2} -> 3, {0,2} -> 2, {0,1} -> 1 */
+    return m == 3 ? 3 : (m == 2 ? 4 : 5);
+}
+
+static double hooke_entry(const or_params *p, double a, int i, int j, int k, int l) {
+    int I = voigt_index(i, j), J = voigt_index(k, l);
+    if (I < 3 && J < 3) return I == J ? a : p->lambda;
+    if (I >= 3 && J >= 3) return I == J ? p->mu : 0.0;
+    return 0.0;
+}
+
+/* calc_zem_stiffness_tensor (zem_stabilization.jl:32-42): C_1[i,j] = sum over k (outer) and l
+ * (inner) of C[i,j,k,l] Kinv[k,l], every one of the 81 products summed as the reference does;
+ * column-major 3x3 result. */
+void or_zem_wan_stiffness(const or_params *p, const double *Kinv, double *C1) {
+    double a = (1 - p->nu) * p->lambda / p->nu;
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) {
+            double sum = 0.0;
+            for (int k = 0; k < 3; k++)
+                for (int l = 0; l < 3; l++) sum += hooke_entry(p, a, i, j, k, l) * Kinv[k + 3 * l];
+            C1[i + 3 * j] = sum;
+        }
+}
+
+/* the stabilisation term of bond b (c_force_density!, correspondence.jl:226-279):
+ * ZEMSilling (w beta) z with beta = Cs bc / delta, ZEMWan (w C_1) z */
+static inline void zem_term(const or_sys *sys, const or_params *p, const double *C1, double om,
+                            const double *z, double *tz) {
+    if (sys->zem == OR_ZEM_WAN) {
+        double W1[9];
+        for (int k = 0; k < 9; k++) W1[k] = om * C1[k];
+        matvec3(W1, z, tz);
+    } else {
+        double beta = sys->zem_cs * p->bc / p->delta;
+        double ob = om * beta;
+        for (int k = 0; k < 3; k++) tz[k] = ob * z[k];
+    }
+}
+
+/* CMaterial: correspondence.jl:183-279, 288-298; stress.jl:112-116 */
 static void c_force_point(const or_sys *sys, or_state *st, double *bsink, int64_t i) {
     const double *x = st->pos, *X = sys->X;
     const or_params *pi = P_of(sys, i);
@@ -546,20 +592,21 @@ static void c_force_point(const or_sys *sys, or_state *st, double *bsink, int64_
     for (int k = 0; k < 9; k++) Ps[k] = iJ * P[k];
     matmulT3(Ps, F, PF);
     memcpy(st->cauchy + 9 * i, PF, sizeof(PF));
-    double beta = sys->zem_cs * pi->bc / pi->delta;
+    double C1[9] = {0};
+    if (sys->zem == OR_ZEM_WAN) or_zem_wan_stiffness(pi, Kinv, C1);
     for (int64_t b = sys->off[i]; b < sys->off[i + 1]; b++) {
         int32_t j = sys->nbr[b];
         double D[3] = {X[3 * j] - X[3 * i], X[3 * j + 1] - X[3 * i + 1], X[3 * j + 2] - X[3 * i + 2]};
         double d[3] = {x[3 * j] - x[3 * i], x[3 * j + 1] - x[3 * i + 1], x[3 * j + 2] - x[3 * i + 2]};
         double om = sys->omega[b] * (st->bond_active[b] ? 1.0 : 0.0);
-        double FD[3], z[3], W[9], WD[3];
+        double FD[3], z[3], W[9], WD[3], tz[3];
         matvec3(F, D, FD);
         for (int k = 0; k < 3; k++) z[k] = d[k] - FD[k];
-        double ob = om * beta;
+        zem_term(sys, pi, C1, om, z, tz);
         for (int k = 0; k < 9; k++) W[k] = om * PKinv[k];
         matvec3(W, D, WD);
         for (int k = 0; k < 3; k++) {
-            double t = WD[k] + ob * z[k];
+            double t = WD[k] + tz[k];
             bsink[3 * i + k] += t * sys->vol[j];
             bsink[3 * j + k] += -t * sys->vol[i];
         }
@@ -678,6 +725,9 @@ static void gather_point(const or_sys *sys, or_state *st, int64_t i, const doubl
 /* CMat point state (correspondence.jl:183-224, 288-298): F and P K^-1 into FP (18 per point),
  * alive[i] = 0 when the point's bonds are killed; defgrad, cauchy and the kill as
  * c_force_point */
+/* per-point record of the serial-order gather: F (9), P K^-1 (9), ZEMWan's C_1 (9) */
+#define C_FPS 27
+
 static void c_state_point(const or_sys *sys, or_state *st, int64_t i, double *FP, unsigned char *alive) {
     const double *x = st->pos, *X = sys->X;
     const or_params *pi = P_of(sys, i);
@@ -712,8 +762,9 @@ static void c_state_point(const or_sys *sys, or_state *st, int64_t i, double *FP
     for (int k = 0; k < 9; k++) Ps[k] = iJ * P[k];
     matmulT3(Ps, F, PF);
     memcpy(st->cauchy + 9 * i, PF, sizeof(PF));
-    memcpy(FP + 18 * i, F, sizeof(F));
-    memcpy(FP + 18 * i + 9, PKinv, sizeof(PKinv));
+    memcpy(FP + C_FPS * i, F, sizeof(F));
+    memcpy(FP + C_FPS * i + 9, PKinv, sizeof(PKinv));
+    if (sys->zem == OR_ZEM_WAN) or_zem_wan_stiffness(pi, Kinv, FP + C_FPS * i + 18);
 }
 
 /* the force term t of bond b = (o -> q) of point o, as c_force_point computes it */
@@ -722,18 +773,17 @@ static inline void c_bond_term(const or_sys *sys, const or_state *st, int64_t o,
     const double *x = st->pos, *X = sys->X;
     const or_params *po = P_of(sys, o);
     int32_t q = sys->nbr[b];
-    const double *F = FP + 18 * o, *PKinv = FP + 18 * o + 9;
-    double beta = sys->zem_cs * po->bc / po->delta;
+    const double *F = FP + C_FPS * o, *PKinv = FP + C_FPS * o + 9, *C1 = FP + C_FPS * o + 18;
     double D[3] = {X[3 * q] - X[3 * o], X[3 * q + 1] - X[3 * o + 1], X[3 * q + 2] - X[3 * o + 2]};
     double d[3] = {x[3 * q] - x[3 * o], x[3 * q + 1] - x[3 * o + 1], x[3 * q + 2] - x[3 * o + 2]};
     double om = sys->omega[b] * (st->bond_active[b] ? 1.0 : 0.0);
-    double FD[3], z[3], W[9], WD[3];
+    double FD[3], z[3], W[9], WD[3], tz[3];
     matvec3(F, D, FD);
     for (int k = 0; k < 3; k++) z[k] = d[k] - FD[k];
-    double ob = om * beta;
+    zem_term(sys, po, C1, om, z, tz);
     for (int k = 0; k < 9; k++) W[k] = om * PKinv[k];
     matvec3(W, D, WD);
-    for (int k = 0; k < 3; k++) t[k] = WD[k] + ob * z[k];
+    for (int k = 0; k < 3; k++) t[k] = WD[k] + tz[k];
 }
 
 static void c_terms_point(const or_sys *sys, const or_state *st, int64_t i, const double *FP,
@@ -796,7 +846,7 @@ static void force_density_serial_order(const or_sys *sys, or_state *st) {
         }
         free(wd);
     } else {
-        double *FP = (double *)malloc(sizeof(double) * 18 * (size_t)n);
+        double *FP = (double *)calloc((size_t)C_FPS * (size_t)(n > 0 ? n : 1), sizeof(double));
 #pragma omp parallel for num_threads(g_threads) schedule(dynamic, 1024)
         for (int64_t i = 0; i < n; i++) {
             c_state_point(sys, st, i, FP, live);

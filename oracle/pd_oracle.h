@@ -33,6 +33,7 @@ typedef struct {
 enum { OR_BB = 0, OR_OSB = 1, OR_CMAT = 2 };
 enum { OR_SVK = 0, OR_NEOHOOKE = 1, OR_NHPENALTY = 2 };
 enum { OR_KERNEL_CONST_ONE = 0, OR_KERNEL_LINEAR = 1, OR_KERNEL_CUBIC_BSPLINE = 2 };
+enum { OR_ZEM_SILLING = 0, OR_ZEM_WAN = 1 };
 
 typedef struct {
     int64_t n, n_bonds;
@@ -52,6 +53,7 @@ typedef struct {
     double zem_cs;            /* ZEMSilling Cs */
     double maxdmg;            /* CMaterial maxdmg */
     const double *scfactor;   /* B surface correction factor per bond; NULL: NoCorrection */
+    int32_t zem;              /* CMat zero-energy mode stabilisation: OR_ZEM_SILLING, OR_ZEM_WAN */
 } or_sys;
 
 typedef struct {
@@ -88,6 +90,8 @@ double or_stable_timestep(const or_sys *sys, double safety_factor);
 int64_t or_run_vv(const or_sys *sys, or_state *st, const or_bc *bcs, int32_t n_bcs,
                   int64_t first_step, int64_t n_steps, double dt);
 void or_first_piola_kirchhoff(int32_t cmodel, const or_params *p, const double *F, double *P);
+/* ZEMWan's stiffness C_1 = C : K^-1 of one point (zem_stabilization.jl:32-42) */
+void or_zem_wan_stiffness(const or_params *p, const double *Kinv, double *C1);
 void or_inv3(const double *A, double *Ainv);
 double or_det3(const double *A);
 int or_point_params(int32_t material, double delta, double rho, double E, double nu, double G,

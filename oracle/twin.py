@@ -34,7 +34,8 @@ def oracle_body(body, cmodel=None):
     ob = O.OracleBody(MAT_ORACLE[type(mat)], body._pos, body.volume, params,
                       pid=body.params_map - 1, kernel=kernel, cmodel=cm,
                       zem_cs=getattr(getattr(mat, "zem", None), "Cs", 0.5), maxdmg=mat.maxdmg,
-                      fp_point=body.fail_permit.astype(np.uint8), cracks=cracks)
+                      fp_point=body.fail_permit.astype(np.uint8), cracks=cracks,
+                      zem=O.ZEM_WAN if isinstance(getattr(mat, "zem", None), pd.ZEMWan) else O.ZEM_SILLING)
     for a, b, filt in body.point_sets_precracks:
         if not filt:
             ob.break_bonds(body.point_sets[a], body.point_sets[b])

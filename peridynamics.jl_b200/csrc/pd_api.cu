@@ -70,10 +70,12 @@ static DevParam make_param(const pd_point_params& p, double cs) {
   q.delta = p.delta; q.rho = p.rho; q.bc = p.bc; q.epsc = p.epsilon_c; q.G = p.G; q.K = p.K;
   q.lambda = p.lambda; q.mu = p.mu;
   q.beta = cs * p.bc / p.delta;
+  q.zwa = (1 - p.nu) * p.lambda / p.nu;  // get_hooke_matrix_voigt, constitutive_models.jl:107-118
   q.dt = 0; q.dth = 0;
   q.deltaf = (float)p.delta; q.bcf = (float)p.bc; q.epscf = (float)p.epsilon_c;
   q.Gf = (float)p.G; q.Kf = (float)p.K; q.lambdaf = (float)p.lambda; q.muf = (float)p.mu;
   q.betaf = (float)q.beta;
+  q.zwaf = (float)q.zwa;
   q.inv_delta = (float)(1.0 / p.delta);
   q.vscale = (float)(1.0 / (p.delta * p.delta * p.delta));
   return q;
@@ -93,6 +95,8 @@ static pd_status validate_desc(const pd_body_desc* desc, bool need_bonds) {
     return fail(PD_ERR_ARG, "unknown precision");
   if (desc->kernel < PD_KERNEL_CONST_ONE || desc->kernel > PD_KERNEL_CUBIC_BSPLINE)
     return fail(PD_ERR_ARG, "unknown kernel");
+  if (desc->material == PD_MAT_CMAT && desc->zem != PD_ZEM_SILLING && desc->zem != PD_ZEM_WAN)
+    return fail(PD_ERR_ARG, "unknown zero-energy mode stabilisation");
   if (desc->cmodel < PD_CM_SVK || desc->cmodel > PD_CM_NEOHOOKE_PENALTY)
     return fail(PD_ERR_ARG, "unknown constitutive model");
   for (int k = 0; k < desc->n_params; k++) {
@@ -235,6 +239,10 @@ static pd_status finish_create(pd_handle* h, int* dnbr_csr, const double* dL, co
       PD_TRY(dalloc(h, &h->d.PK64, 9 * n));
       PD_CUDA(cudaMemsetAsync(h->d.F64, 0, sizeof(double) * 9 * n, h->stream));
       PD_CUDA(cudaMemsetAsync(h->d.PK64, 0, sizeof(double) * 9 * n, h->stream));
+      if (h->zem == PD_ZEM_WAN) {
+        PD_TRY(dalloc(h, &h->d.C164, 9 * n));
+        PD_CUDA(cudaMemsetAsync(h->d.C164, 0, sizeof(double) * 9 * n, h->stream));
+      }
     } else {
       PD_TRY(dalloc(h, &h->d.H32, 9 * n));
       PD_TRY(dalloc(h, &h->d.cst32, 3 * n));
@@ -242,6 +250,10 @@ static pd_status finish_create(pd_handle* h, int* dnbr_csr, const double* dL, co
       PD_CUDA(cudaMemsetAsync(h->d.H32, 0, sizeof(float) * 9 * n, h->stream));
       PD_CUDA(cudaMemsetAsync(h->d.cst32, 0, sizeof(float4) * 3 * n, h->stream));
       PD_CUDA(cudaMemsetAsync(h->d.K32, 0, sizeof(float) * 6 * n, h->stream));
+      if (h->zem == PD_ZEM_WAN) {
+        PD_TRY(dalloc(h, &h->d.zw32, 2 * n));
+        PD_CUDA(cudaMemsetAsync(h->d.zw32, 0, sizeof(float4) * 2 * n, h->stream));
+      }
     }
   }
   launch_count_active(h->d, h->stream);
@@ -335,6 +347,7 @@ static pd_status begin_create(const pd_body_desc* desc, pd_handle** out, pd_hand
   h->cmodel = desc->cmodel;
   h->precision = desc->precision;
   h->cs = desc->zem_cs;
+  h->zem = desc->material == PD_MAT_CMAT ? desc->zem : PD_ZEM_SILLING;
   h->maxdmg = desc->maxdmg;
   h->multi = desc->multi_params ? 1 : 0;
   PD_CUDA(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
@@ -372,6 +385,7 @@ static pd_status begin_create(const pd_body_desc* desc, pd_handle** out, pd_hand
   h->d.multi = h->multi;
   h->d.maxdmg = h->maxdmg;
   h->d.cs = h->cs;
+  h->d.zem = h->zem;
   h->d.sym = 1;
   h->cfg.group = 1;
   h->cfg.block = 256;

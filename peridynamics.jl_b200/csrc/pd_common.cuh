@@ -56,12 +56,15 @@ constexpr uint32_t META_HALO = 1u << 19;
 enum Material : int { MAT_BB = 0, MAT_OSB = 1, MAT_CMAT = 2 };
 enum CModel : int { CM_SVK = 0, CM_NEOHOOKE = 1, CM_NHPENALTY = 2 };
 enum Kernel : int { KER_CONST_ONE = 0, KER_LINEAR = 1, KER_CUBIC_BSPLINE = 2 };
+// CMat zero-energy mode stabilisation (zem_stabilization.jl)
+enum Zem : int { ZEM_SILLING = 0, ZEM_WAN = 1 };
 
 // One parameter set (StandardPointParameters) with the derived per-set constants.
 struct DevParam {
   double delta, rho, bc, epsc, G, K, lambda, mu, beta;  // beta = Cs * bc / delta
+  double zwa;                                           // (1 - nu) lambda / nu (Hooke diagonal)
   double dt, dth;                                       // integration step of the set
-  float deltaf, bcf, epscf, Gf, Kf, lambdaf, muf, betaf;
+  float deltaf, bcf, epscf, Gf, Kf, lambdaf, muf, betaf, zwaf;
   float inv_delta;  // 1 / delta (FP32 correspondence scaling)
   float vscale;     // 1 / delta^3 (FP32 correspondence scaling)
 };
@@ -103,6 +106,11 @@ struct DevBody {
   double* PK64;      // CMat FP64: P K^-1 (9 per point)
   float* H32;        // CMat FP32: displacement gradient H = F - I (9 per point)
   float4* cst32;     // CMat FP32: 3 float4 per point {A (9), beta~, 0, 0}
+  // CMat with ZEMWan: the stabilising stiffness C : K^-1 of every point (FP64: 9 per point,
+  // column-major; FP32: 2 float4 per point {S00, S11, S22, S01}, {S02, S12, 0, 0}); null with
+  // ZEMSilling
+  double* C164;
+  float4* zw32;
   float* K32;        // CMat FP32: the scaled shape tensor of every point {xx, yy, zz, xy, xz, yz}
   // EnergySurfaceCorrection (BB, OSB): the factor of every bond slot (FP64 / FP32 path) and
   // the per-point multiplication factors {x, y, z} it is made from; null without correction
@@ -110,7 +118,7 @@ struct DevBody {
   const float* sc32;
   double* mf;
   Ctrl* ctrl;
-  int material, kernel, cmodel, sym, multi;
+  int material, kernel, cmodel, sym, multi, zem;
   double maxdmg;
   double cs;
 };

@@ -600,6 +600,54 @@ __device__ void pk1_32(int cmodel, const DevParam& p, const float* H, float* P) 
 // -------------------------------------------------------------------------------------------
 // CMat phase A (correspondence.jl:193-224, 288-298; bond_system.jl:309-327)
 // -------------------------------------------------------------------------------------------
+// The phase-B state of a live point, from the scaled inverse shape tensor Kinv (the true
+// K^-1 = Kinv / delta^5), P K^-1 (scaled the same way) and H = F - I. The bond term
+// w (P K^-1 xi + S (dx - F xi)) is w (A xi + S du) with A = P K^-1 - S H, where S is the
+// stabilising stiffness: ZEMSilling beta I (c_force_density!, correspondence.jl:226-251; beta
+// in cst32), ZEMWan C : K^-1 (correspondence.jl:253-285, zem_stabilization.jl:32-42; the six
+// entries of the symmetric S in zw32, from the nonzero entries of the Hooke tensor: a = (1 - nu)
+// lambda / nu and lambda in the normal block, mu (both index orders) in the shear block).
+__device__ __forceinline__ void c_state_store32(const DevBody& d, const DevParam& P, long long i,
+                                                const float* PK, const float* Kinv, const float* H,
+                                                float id5) {
+  float A[9];
+  float4* cs = d.cst32 + 3 * i;
+  if (d.zem == ZEM_WAN) {
+    const float a = P.zwaf, l = P.lambdaf, m = P.muf;
+    const float S0 = (a * Kinv[0] + l * Kinv[4] + l * Kinv[8]) * id5;
+    const float S1 = (l * Kinv[0] + a * Kinv[4] + l * Kinv[8]) * id5;
+    const float S2 = (l * Kinv[0] + l * Kinv[4] + a * Kinv[8]) * id5;
+    const float S01 = m * (Kinv[3] + Kinv[1]) * id5;
+    const float S02 = m * (Kinv[6] + Kinv[2]) * id5;
+    const float S12 = m * (Kinv[7] + Kinv[5]) * id5;
+    const float Sm[9] = {S0, S01, S02, S01, S1, S12, S02, S12, S2};
+    float SH[9];
+    fmatmul(Sm, H, SH);
+#pragma unroll
+    for (int q = 0; q < 9; q++) A[q] = PK[q] * id5 - SH[q];
+    d.zw32[2 * i] = make_float4(S0, S1, S2, S01);
+    d.zw32[2 * i + 1] = make_float4(S02, S12, 0.f, 0.f);
+  } else {
+#pragma unroll
+    for (int q = 0; q < 9; q++) A[q] = PK[q] * id5 - P.betaf * H[q];
+  }
+  cs[0] = make_float4(A[0], A[1], A[2], A[3]);
+  cs[1] = make_float4(A[4], A[5], A[6], A[7]);
+  cs[2] = make_float4(A[8], d.zem == ZEM_WAN ? 0.f : P.betaf, 0.f, 0.f);
+}
+
+// a killed point's phase-B state: no term of its own, none for its neighbours
+__device__ __forceinline__ void c_state_clear32(const DevBody& d, long long i) {
+  float4* cs = d.cst32 + 3 * i;
+  cs[0] = make_float4(0.f, 0.f, 0.f, 0.f);
+  cs[1] = make_float4(0.f, 0.f, 0.f, 0.f);
+  cs[2] = make_float4(0.f, 0.f, 0.f, 0.f);
+  if (d.zem == ZEM_WAN) {
+    d.zw32[2 * i] = make_float4(0.f, 0.f, 0.f, 0.f);
+    d.zw32[2 * i + 1] = make_float4(0.f, 0.f, 0.f, 0.f);
+  }
+}
+
 // the correspondence phase A keeps 15 compensated 3x3 sums per point: it gets its own
 // occupancy bound (PD_MINB_CA resident blocks per SM). Measured on the 1M-point CMat block:
 // 1.50 / 1.44 / 1.49 ms at 2 / 3 / 4 blocks (109 / 80 / 64 registers).
@@ -717,22 +765,15 @@ __global__ void __launch_bounds__(256, FULLK ? PD_MINB_CA : PD_MINB_CAI) k_c_a32
       // a halo row sees only part of its bonds: its owner decides (the kill arrives with the
       // halo exchange of the phase-A state)
       killed = (meta & META_KILLED) || (!(meta & META_HALO) && (damage > d.maxdmg || hasnan));
-      float4* cs = d.cst32 + 3 * i;
       if (killed) {
         if (!(meta & META_KILLED)) d.meta[i] = meta | META_KILLED;
         na = 0;
-        cs[0] = make_float4(0.f, 0.f, 0.f, 0.f);
-        cs[1] = make_float4(0.f, 0.f, 0.f, 0.f);
-        cs[2] = make_float4(0.f, 0.f, 0.f, 0.f);
+        c_state_clear32(d, i);
       } else {
-        float Pm[9], PK[9], A[9];
+        float Pm[9], PK[9];
         pk1_32(d.cmodel, P, H, Pm);
         fmatmul(Pm, Kinv, PK);
-        const float id5 = id * id * id * id * id;
-        for (int q = 0; q < 9; q++) A[q] = PK[q] * id5 - P.betaf * H[q];
-        cs[0] = make_float4(A[0], A[1], A[2], A[3]);
-        cs[1] = make_float4(A[4], A[5], A[6], A[7]);
-        cs[2] = make_float4(A[8], P.betaf, 0.f, 0.f);
+        c_state_store32(d, P, i, PK, Kinv, H, id * id * id * id * id);
       }
       d.n_active[i] = na;
     }
@@ -747,9 +788,17 @@ __global__ void __launch_bounds__(256, FULLK ? PD_MINB_CA : PD_MINB_CAI) k_c_a32
 }
 
 // -------------------------------------------------------------------------------------------
-// CMat phase B (correspondence.jl:226-251): with A = P K^-1 - beta H,
-//   t_ij = w (A_i xi + beta_i du), and j's term -t_ji = w (A_j xi + beta_j du)
+// CMat phase B (correspondence.jl:226-279): with A = P K^-1 - S H (c_state_store32),
+//   t_ij = w (A_i xi + S_i du), and j's term -t_ji = w (A_j xi + S_j du);
+// S = beta I (ZEMSilling) or the symmetric C : K^-1 of the point (ZEMWan, template flag WAN)
 // -------------------------------------------------------------------------------------------
+// row q of S du for the symmetric S = {S00, S11, S22, S01, S02, S12}
+__device__ __forceinline__ float sym_row(const float* S, int q, const float* du) {
+  if (q == 0) return S[0] * du[0] + S[3] * du[1] + S[4] * du[2];
+  if (q == 1) return S[3] * du[0] + S[1] * du[1] + S[5] * du[2];
+  return S[4] * du[0] + S[5] * du[1] + S[2] * du[2];
+}
+
 // phase B with the next row's bond record in flight holds 80 registers at 3 resident blocks.
 // Measured on the 1M-point CMat block: 0.95 ms at 3 blocks; 1.21 ms at 4 (64 registers, 120 B
 // of spills); 1.12 ms for the kernel without the prefetch at 4.
@@ -758,7 +807,7 @@ __global__ void __launch_bounds__(256, FULLK ? PD_MINB_CA : PD_MINB_CAI) k_c_a32
 #endif
 // SYM: symmetric bond states (one bit serves both directions), dispatched from d.sym; the
 // variant without the reverse-bond lookup code took 1.1 % less time on the 1M-point block
-template <int G, bool SYM>
+template <int G, bool SYM, bool WAN>
 __global__ void __launch_bounds__(256, PD_MINB_CB) k_c_b32(DevBody d, int kstep) {
   if (d.ctrl->err) return;
   PD_SLICE_LOOP(G) {
@@ -773,6 +822,13 @@ __global__ void __launch_bounds__(256, PD_MINB_CB) k_c_b32(DevBody d, int kstep)
       Ai[0] = a0.x; Ai[1] = a0.y; Ai[2] = a0.z; Ai[3] = a0.w;
       Ai[4] = a1.x; Ai[5] = a1.y; Ai[6] = a1.z; Ai[7] = a1.w; Ai[8] = a2.x;
       bi = a2.y;
+    }
+    float Wi[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    if constexpr (WAN) {
+      if (valid) {
+        const float4 w0 = d.zw32[2 * i], w1 = d.zw32[2 * i + 1];
+        Wi[0] = w0.x; Wi[1] = w0.y; Wi[2] = w0.z; Wi[3] = w0.w; Wi[4] = w1.x; Wi[5] = w1.y;
+      }
     }
     // the bond record of row r + 1 is loaded while row r is processed (as k_osb_b32)
     const unsigned* wrow = d.bits + (sbase >> 5);
@@ -818,11 +874,18 @@ __global__ void __launch_bounds__(256, PD_MINB_CB) k_c_b32(DevBody d, int kstep)
       const float Aj[9] = {c0.x, c0.y, c0.z, c0.w, c1.x, c1.y, c1.z, c1.w, c2.x};
       const float bj = c2.y;
       const float V = hj.w;
+      float Wj[6];
+      if constexpr (WAN) {
+        const float4 w0 = __ldg(d.zw32 + 2 * (long long)j), w1 = __ldg(d.zw32 + 2 * (long long)j + 1);
+        Wj[0] = w0.x; Wj[1] = w0.y; Wj[2] = w0.z; Wj[3] = w0.w; Wj[4] = w1.x; Wj[5] = w1.y;
+      }
       float t[3];
 #pragma unroll
       for (int q = 0; q < 3; q++) {
-        const float ti = Ai[q] * g.x + Ai[q + 3] * g.y + Ai[q + 6] * g.z + bi * du[q];
-        const float tj = Aj[q] * g.x + Aj[q + 3] * g.y + Aj[q + 6] * g.z + bj * du[q];
+        const float si = WAN ? sym_row(Wi, q, du) : bi * du[q];
+        const float sj = WAN ? sym_row(Wj, q, du) : bj * du[q];
+        const float ti = Ai[q] * g.x + Ai[q + 3] * g.y + Ai[q + 6] * g.z + si;
+        const float tj = Aj[q] * g.x + Aj[q + 3] * g.y + Aj[q + 6] * g.z + sj;
         t[q] = (oi * ti + oj * tj) * V;
       }
       bx.add(t[0]); by.add(t[1]); bz.add(t[2]);
@@ -1004,22 +1067,15 @@ __global__ void __launch_bounds__(256, PD_MINB_CQA) k_c_a32q(DevBody d, int kste
       for (int q = 0; q < 9; q++) { d.H32[9 * i + q] = H[q]; hasnan |= isnan(H[q]); }
       const double damage = 1.0 - (double)na / (double)cnt;
       killed = (meta & META_KILLED) || (!(meta & META_HALO) && (damage > d.maxdmg || hasnan));
-      float4* cs = d.cst32 + 3 * i;
       if (killed) {
         if (!(meta & META_KILLED)) d.meta[i] = meta | META_KILLED;
         na = 0;
-        cs[0] = make_float4(0.f, 0.f, 0.f, 0.f);
-        cs[1] = make_float4(0.f, 0.f, 0.f, 0.f);
-        cs[2] = make_float4(0.f, 0.f, 0.f, 0.f);
+        c_state_clear32(d, i);
       } else {
-        float Pm[9], PK[9], A[9];
+        float Pm[9], PK[9];
         pk1_32(d.cmodel, P, H, Pm);
         fmatmul(Pm, Kinv, PK);
-        const float id5 = id * id * id * id * id;
-        for (int q = 0; q < 9; q++) A[q] = PK[q] * id5 - P.betaf * H[q];
-        cs[0] = make_float4(A[0], A[1], A[2], A[3]);
-        cs[1] = make_float4(A[4], A[5], A[6], A[7]);
-        cs[2] = make_float4(A[8], P.betaf, 0.f, 0.f);
+        c_state_store32(d, P, i, PK, Kinv, H, id * id * id * id * id);
       }
       d.n_active[i] = na;
     }
@@ -1123,10 +1179,12 @@ __global__ void __launch_bounds__(256, PD_MINB_CQB) k_c_b32q(DevBody d, int kste
 }
 
 // the packed correspondence kernels: one lane per point, one parameter set; phase B also needs
-// symmetric bond states
+// symmetric bond states and ZEMSilling. With ZEMWan the packed phase B (both points' stiffness
+// gathered with the next row pair in flight) spilled and took 1.37 ms on the 1M-point block
+// against 1.12 ms for k_c_b32, so ZEMWan's phase B is the one-row kernel.
 static bool cq_supported(const DevBody& d, int phase) {
   if (d.material != MAT_CMAT || d.lg != 1 || d.multi) return false;
-  if (phase == 2 && !d.sym) return false;
+  if (phase == 2 && (!d.sym || d.zem == ZEM_WAN)) return false;
   return true;
 }
 
@@ -1251,13 +1309,20 @@ int launch_force32(const DevBody& d, const LaunchCfg& c, int kstep, int phase, c
     }
     launches++;
   }
+  const bool wan = d.zem == ZEM_WAN;
   if (B && c.pipe == 5 && cq_supported(d, 2)) {
     if (lin) k_c_b32q<true><<<grid, c.block, 0, s>>>(d, kstep);
     else k_c_b32q<false><<<grid, c.block, 0, s>>>(d, kstep);
     launches++;
   } else if (B) {
-    if (d.sym) { PD_DISPATCH_G(G, (k_c_b32<GG, true><<<grid, c.block, 0, s>>>(d, kstep))); }
-    else { PD_DISPATCH_G(G, (k_c_b32<GG, false><<<grid, c.block, 0, s>>>(d, kstep))); }
+    if (wan) {
+      if (d.sym) { PD_DISPATCH_G(G, (k_c_b32<GG, true, true><<<grid, c.block, 0, s>>>(d, kstep))); }
+      else { PD_DISPATCH_G(G, (k_c_b32<GG, false, true><<<grid, c.block, 0, s>>>(d, kstep))); }
+    } else if (d.sym) {
+      PD_DISPATCH_G(G, (k_c_b32<GG, true, false><<<grid, c.block, 0, s>>>(d, kstep)));
+    } else {
+      PD_DISPATCH_G(G, (k_c_b32<GG, false, false><<<grid, c.block, 0, s>>>(d, kstep)));
+    }
     launches++;
   }
   return launches;

@@ -65,6 +65,32 @@ __device__ __forceinline__ void matvec3(const double* A, const double* v, double
   for (int r = 0; r < 3; r++) w[r] = (A[r] * v[0] + A[r + 3] * v[1]) + A[r + 6] * v[2];
 }
 
+// ZEMWan stiffness (zem_stabilization.jl:32-42): C_1[i,j] = sum over k (outer), l (inner) of
+// C[i,j,k,l] Kinv[k,l], all 81 products in that order, with C the Hooke tensor that
+// get_hooke_matrix builds from the Voigt matrix (constitutive_models.jl:107-133): Voigt index
+// of (i,j) in the order (1,1), (2,2), (3,3), (2,3), (1,3), (1,2); a = (1 - nu) lambda / nu on the
+// diagonal of the normal block, lambda off it, mu on the diagonal of the shear block.
+__device__ __forceinline__ int voigt_of(int i, int j) {
+  if (i == j) return i;
+  const int m = i + j;
+  return m == 3 ? 3 : (m == 2 ? 4 : 5);
+}
+__device__ __forceinline__ double hooke_of(const DevParam& p, int i, int j, int k, int l) {
+  const int I = voigt_of(i, j), J = voigt_of(k, l);
+  if (I < 3 && J < 3) return I == J ? p.zwa : p.lambda;
+  if (I >= 3 && J >= 3) return I == J ? p.mu : 0.0;
+  return 0.0;
+}
+__device__ void zem_wan64(const DevParam& p, const double* Kinv, double* C1) {
+  for (int i = 0; i < 3; i++)
+    for (int j = 0; j < 3; j++) {
+      double s = 0.0;
+      for (int k = 0; k < 3; k++)
+        for (int l = 0; l < 3; l++) s += hooke_of(p, i, j, k, l) * Kinv[k + 3 * l];
+      C1[i + 3 * j] = s;
+    }
+}
+
 // first_piola_kirchhoff (constitutive_models.jl:35-41, 169-176, 233-244)
 __device__ void pk1_64(int cmodel, const DevParam& p, const double* F, double* P) {
   double C[9], S[9];
@@ -458,6 +484,11 @@ __global__ void PD_LB64 k_c_a64(DevBody d, int kstep) {
         pk1_64(d.cmodel, P, F, Pm);
         matmul3(Pm, Kinv, PKinv);
         for (int q = 0; q < 9; q++) d.PK64[9 * i + q] = PKinv[q];
+        if (d.zem == ZEM_WAN) {
+          double C1[9];
+          zem_wan64(P, Kinv, C1);
+          for (int q = 0; q < 9; q++) d.C164[9 * i + q] = C1[q];
+        }
       }
       d.n_active[i] = na;
     }
@@ -472,18 +503,26 @@ __global__ void PD_LB64 k_c_a64(DevBody d, int kstep) {
 }
 
 // -------------------------------------------------------------------------------------------
-// CMat phase B: c_force_density!(::ZEMSilling) (correspondence.jl:226-251) in gather form
+// CMat phase B: c_force_density! (correspondence.jl:226-279) in gather form; the stabilisation
+// term is (w beta) z for ZEMSilling (C1 null) and (w C_1) z for ZEMWan
 // -------------------------------------------------------------------------------------------
-__device__ __forceinline__ void c_bond_t64(const double* F, const double* PK, double beta,
-                                           double om, const double* DX, const double* dx,
-                                           double* t) {
-  double FD[3], z[3], W[9], WD[3];
+__device__ __forceinline__ void c_bond_t64(const double* F, const double* PK, const double* C1,
+                                           double beta, double om, const double* DX,
+                                           const double* dx, double* t) {
+  double FD[3], z[3], W[9], WD[3], tz[3];
   matvec3(F, DX, FD);
   for (int q = 0; q < 3; q++) z[q] = dx[q] - FD[q];
-  const double ob = om * beta;
+  if (C1) {
+    double W1[9];
+    for (int q = 0; q < 9; q++) W1[q] = om * C1[q];
+    matvec3(W1, z, tz);
+  } else {
+    const double ob = om * beta;
+    for (int q = 0; q < 3; q++) tz[q] = ob * z[q];
+  }
   for (int q = 0; q < 9; q++) W[q] = om * PK[q];
   matvec3(W, DX, WD);
-  for (int q = 0; q < 3; q++) t[q] = WD[q] + ob * z[q];
+  for (int q = 0; q < 3; q++) t[q] = WD[q] + tz[q];
 }
 
 template <int G, bool EXACT>
@@ -497,10 +536,12 @@ __global__ void PD_LB64 k_c_b64(DevBody d, int kstep) {
     const unsigned mi = valid ? d.meta[i] : META_KILLED;
     const DevParam& Pi = d.params[mi & META_PID_MASK];
     const bool own = !(mi & META_KILLED);
-    double Fi[9], PKi[9];
+    const bool wan = d.zem == ZEM_WAN;
+    double Fi[9], PKi[9], Ci[9];
     for (int q = 0; q < 9; q++) {
       Fi[q] = own ? d.F64[9 * i + q] : 0.0;
       PKi[q] = own ? d.PK64[9 * i + q] : 0.0;
+      Ci[q] = own && wan ? d.C164[9 * i + q] : 0.0;
     }
     auto own_term = [&](long long b) {
       const int j = __ldg(d.nbr + b);
@@ -511,7 +552,7 @@ __global__ void PD_LB64 k_c_b64(DevBody d, int kstep) {
       const bool act = bond_bit(d.bits, b);
       const double om = act ? omega_of(d.kernel, Pi.delta, L) : 0.0;
       double t[3];
-      c_bond_t64(Fi, PKi, Pi.beta, om, DX, dx, t);
+      c_bond_t64(Fi, PKi, wan ? Ci : nullptr, Pi.beta, om, DX, dx, t);
       bx += t[0] * xj.w; by += t[1] * xj.w; bz += t[2] * xj.w;
     };
     auto nbr_term = [&](long long b) {
@@ -525,9 +566,11 @@ __global__ void PD_LB64 k_c_b64(DevBody d, int kstep) {
       const double DX[3] = {Xi.x - Xj.x, Xi.y - Xj.y, Xi.z - Xj.z};
       const double dx[3] = {xi.x - xj.x, xi.y - xj.y, xi.z - xj.z};
       const double om = act ? omega_of(d.kernel, Pj.delta, L) : 0.0;
-      double Fj[9], PKj[9], t[3];
+      double Fj[9], PKj[9], Cj[9], t[3];
       for (int q = 0; q < 9; q++) { Fj[q] = d.F64[9 * (long long)j + q]; PKj[q] = d.PK64[9 * (long long)j + q]; }
-      c_bond_t64(Fj, PKj, Pj.beta, om, DX, dx, t);
+      if (wan)
+        for (int q = 0; q < 9; q++) Cj[q] = d.C164[9 * (long long)j + q];
+      c_bond_t64(Fj, PKj, wan ? Cj : nullptr, Pj.beta, om, DX, dx, t);
       bx += -t[0] * xj.w; by += -t[1] * xj.w; bz += -t[2] * xj.w;
     };
     if (EXACT) {

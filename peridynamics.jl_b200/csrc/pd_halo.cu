@@ -57,8 +57,10 @@ static HaloKind halo_kind(const pd_handle* h, int kind) {
     if (h->precision == PD_PREC_FP64) {
       add(d.F64, 18, 0);
       add(d.PK64, 18, 0);
+      if (d.C164) add(d.C164, 18, 0);
     } else {
       add(d.cst32, 12, 0);
+      if (d.zw32) add(d.zw32, 8, 0);
     }
     add(d.meta, 1, 1);
   }

@@ -55,7 +55,7 @@ struct pd_handle {
   cudaStream_t stream = nullptr;      // the stream all work is issued on
   cudaStream_t own_stream = nullptr;  // the stream the handle created (destroyed with it)
   long long n = 0, nb = 0;
-  int material = 0, kernel = 1, cmodel = 0, precision = 0, multi = 0;
+  int material = 0, kernel = 1, cmodel = 0, precision = 0, multi = 0, zem = 0;
   double cs = 0.5, maxdmg = 0.85;
   std::vector<DevParam> hp;
   std::vector<unsigned> hmeta;

@@ -7,7 +7,7 @@ Verlet update run as CUDA kernels; there is no CPU fallback.
 """
 from ._lib import NaNError, PDCudaError, lib, LIB_PATH, EXPORTS
 from .materials import (BBMaterial, OSBMaterial, CMaterial, SaintVenantKirchhoff, NeoHooke,
-                        NeoHookePenalty, ZEMSilling, CriticalStretch, NoCorrection,
+                        NeoHookePenalty, ZEMSilling, ZEMWan, CriticalStretch, NoCorrection,
                         EnergySurfaceCorrection,
                         const_one_kernel, linear_kernel, cubic_b_spline_kernel,
                         point_parameters, PointParameters)

@@ -20,6 +20,7 @@ _LIB = None
 # materials, models, kernels, precision
 MAT_BB, MAT_OSB, MAT_CMAT = 0, 1, 2
 CM_SVK, CM_NEOHOOKE, CM_NEOHOOKE_PENALTY = 0, 1, 2
+ZEM_SILLING, ZEM_WAN = 0, 1
 KERNEL_CONST_ONE, KERNEL_LINEAR, KERNEL_CUBIC_BSPLINE = 0, 1, 2
 PREC_FP64, PREC_FP32_KAHAN = 0, 1
 # fields
@@ -66,7 +67,7 @@ class BodyDesc(C.Structure):
                 ("param_id", C.c_void_p), ("n_params", C.c_int32), ("params", C.c_void_p),
                 ("material", C.c_int32), ("kernel", C.c_int32), ("cmodel", C.c_int32),
                 ("precision", C.c_int32), ("multi_params", C.c_int32), ("zem_cs", C.c_double),
-                ("maxdmg", C.c_double), ("device", C.c_int32)]
+                ("maxdmg", C.c_double), ("device", C.c_int32), ("zem", C.c_int32)]
 
 
 class BCDesc(C.Structure):

@@ -67,6 +67,17 @@ class NeoHookePenalty:
 class ZEMSilling:
     """Zero-energy mode stabilisation of Silling (zem_stabilization.jl:16-21)."""
     Cs: float = 0.5
+    id = L.ZEM_SILLING
+
+
+class ZEMWan:
+    """Zero-energy mode stabilisation of Wan et al. (2019) (zem_stabilization.jl:23-42): the
+    stabilising stiffness of every point is C : K^-1, the Hooke tensor of its parameter set
+    contracted with its inverse shape tensor; no stabilisation parameter."""
+    id = L.ZEM_WAN
+
+    def __repr__(self):
+        return "ZEMWan()"
 
 
 # ----------------------------------------------------------------------------------------
@@ -141,20 +152,21 @@ class OSBMaterial(AbstractMaterial):
 
 
 class CMaterial(AbstractMaterial):
-    """Correspondence formulation (correspondence.jl:111-128) with ZEMSilling."""
+    """Correspondence formulation (correspondence.jl:111-128) with ZEMSilling or ZEMWan."""
     material_id = L.MAT_CMAT
 
     def __init__(self, kernel=linear_kernel, model=None, zem=None, dmgmodel=None, maxdmg=0.85):
         self.kernel = kernel
         self.model = model if model is not None else SaintVenantKirchhoff()
         self.zem = zem if zem is not None else ZEMSilling()
-        if not isinstance(self.zem, ZEMSilling):
-            raise ValueError("only ZEMSilling stabilisation is available on the device")
+        if not isinstance(self.zem, (ZEMSilling, ZEMWan)):
+            raise ValueError("zem must be ZEMSilling(Cs) or ZEMWan()")
         self.dmgmodel = dmgmodel or CriticalStretch()
         self.maxdmg = float(maxdmg)
 
     def __repr__(self):
-        return f"CMaterial(model={type(self.model).__name__}, maxdmg={self.maxdmg})"
+        return (f"CMaterial(model={type(self.model).__name__}, zem={self.zem!r}, "
+                f"maxdmg={self.maxdmg})")
 
 
 # ----------------------------------------------------------------------------------------

@@ -111,7 +111,8 @@ class DeviceBody:
         # several parameter sets: the reference's ParameterHandler semantics (bond-averaged
         # parameters), unless every bonded pair shares its set (independent specimens)
         desc.multi_params = 1 if (len(body.point_params) > 1 and not independent_params) else 0
-        desc.zem_cs = mat.zem.Cs if isinstance(mat, CMaterial) else 0.5
+        desc.zem_cs = getattr(mat.zem, "Cs", 0.5) if isinstance(mat, CMaterial) else 0.5
+        desc.zem = mat.zem.id if isinstance(mat, CMaterial) else L.ZEM_SILLING
         desc.maxdmg = mat.maxdmg
         desc.device = device
         filt = [c for c in body.point_sets_precracks if c[2]]

@@ -17,6 +17,7 @@ MATS = {
     "BB": (pd.BBMaterial, None),
     "OSB": (pd.OSBMaterial, 0.25),
     "C": (lambda: pd.CMaterial(maxdmg=0.3), 0.25),
+    "C-Wan": (lambda: pd.CMaterial(zem=pd.ZEMWan(), maxdmg=0.3), 0.25),
 }
 
 
@@ -61,7 +62,7 @@ def assert_same(dev, pb):
     assert np.array_equal(pb.field("bond_active"), dev.field("bond_active"))
 
 
-@pytest.mark.parametrize("name", ["BB", "OSB", "C"])
+@pytest.mark.parametrize("name", ["BB", "OSB", "C", "C-Wan"])
 @pytest.mark.parametrize("prec,mapping,how", [("fp64", (0,), "index"), ("fp32", (8,), "index"),
                                               ("fp64", (4,), "slabs"), ("fp32", (1,), "slabs")])
 def test_partitions_step_like_the_body(name, prec, mapping, how):
@@ -80,14 +81,14 @@ def test_partitions_step_like_the_body(name, prec, mapping, how):
     dev.close()
 
 
-@pytest.mark.parametrize("name", ["OSB", "C"])
+@pytest.mark.parametrize("name", ["OSB", "C", "C-Wan"])
 def test_directed_bond_states(name):
     body = make_plate(name, two_sets=True)
     dev, dt = run_body(body, "fp64", (0,), 100)
     assert dev.info()[2] == 0      # directed states: reverse-bond lookups
     pb, _ = run_parts(body, 2, "fp64", (0,), 100)
     assert_same(dev, pb)
-    if name == "C":
+    if name.startswith("C"):
         # points were killed (damage above maxdmg), on both sides of the cut
         assert (dev.field("damage") == 1.0).any()
     pb.close()

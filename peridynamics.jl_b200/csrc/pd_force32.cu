@@ -1205,7 +1205,8 @@ static int grid_for32(long long nslices, int block) {
   long long warps = nslices;
   long long blocks = (warps + block / 32 - 1) / (block / 32);
   if (blocks < 1) blocks = 1;
-  if (blocks > 148LL * 64) blocks = 148LL * 64;
+  if (PD_GRID_BLOCKS_PER_SM > 0 && blocks > 148LL * PD_GRID_BLOCKS_PER_SM)
+    blocks = 148LL * PD_GRID_BLOCKS_PER_SM;
   return (int)blocks;
 }
 

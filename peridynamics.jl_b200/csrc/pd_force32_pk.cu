@@ -275,7 +275,8 @@ bool pk_supported(const DevBody& d, int phase) {
 static int grid_pk(long long nslices, int block) {
   long long blocks = (nslices + block / 32 - 1) / (block / 32);
   if (blocks < 1) blocks = 1;
-  if (blocks > 148LL * 64) blocks = 148LL * 64;
+  if (PD_GRID_BLOCKS_PER_SM > 0 && blocks > 148LL * PD_GRID_BLOCKS_PER_SM)
+    blocks = 148LL * PD_GRID_BLOCKS_PER_SM;
   return (int)blocks;
 }
 

@@ -3,6 +3,13 @@
 #include <cuda_runtime.h>
 #include "pd_common.cuh"
 
+// Upper bound of a force kernel's grid in blocks per SM (148 SMs; 0: one block per group of
+// slices, no bound). Every warp loops over slices with the grid's stride, so a grid below the
+// slice count gives each warp several slices.
+#ifndef PD_GRID_BLOCKS_PER_SM
+#define PD_GRID_BLOCKS_PER_SM 64
+#endif
+
 namespace pd {
 
 struct LaunchCfg {

@@ -3,11 +3,14 @@
 #include <cuda_runtime.h>
 #include "pd_common.cuh"
 
-// Upper bound of a force kernel's grid in blocks per SM (148 SMs; 0: one block per group of
-// slices, no bound). Every warp loops over slices with the grid's stride, so a grid below the
-// slice count gives each warp several slices.
+// Upper bound of a force kernel's grid in blocks per SM (148 SMs; 0: no bound, one warp per
+// slice). Every warp loops over slices with the grid's stride, so a bounded grid gives each warp
+// several slices. Measured on the 8M-point OSB block (packed kernels, blocks of 128 threads, one
+// B200): bound 64 (9,472 blocks): step 8.76 ms, phase A 4.15 ms, phase B 4.46 ms; no bound
+// (62,500 blocks): 8.18 ms, 3.92 ms, 4.12 ms at a lower SM clock; bounds 32, 16 and 8: 8.81,
+// 9.15 and 10.26 ms (phase B 4.51, 5.04 and 6.26 ms).
 #ifndef PD_GRID_BLOCKS_PER_SM
-#define PD_GRID_BLOCKS_PER_SM 64
+#define PD_GRID_BLOCKS_PER_SM 0
 #endif
 
 namespace pd {

@@ -484,7 +484,8 @@ static void nk_k0(pd_handle* h, const double* v, double* out) {
   k_pack4<<<nk_grid(h->n, 256), 256, 0, h->stream>>>(S->kx, v, h->n);
   long long blocks = (h->d.nslices + 7) / 8;
   if (blocks < 1) blocks = 1;
-  if (blocks > 148LL * 64) blocks = 148LL * 64;
+  if (PD_GRID_BLOCKS_PER_SM > 0 && blocks > 148LL * PD_GRID_BLOCKS_PER_SM)
+    blocks = 148LL * PD_GRID_BLOCKS_PER_SM;
   const int grid = (int)blocks;
   switch (h->d.lg) {
     case 1: k_k0<1><<<grid, 256, 0, h->stream>>>(h->d, S->kx, S->cmask, out); break;

@@ -1249,8 +1249,8 @@ def main():
             "roofline": {"bound": "hbm", "kernel": f"{mat.lower()} force {dom}",
                          "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
-                         "traffic_source": "profiles/traffic.json (ncu DRAM counters; phase B "
-                                           "captured on the 8M-point block, per bond)",
+                         "traffic_source": "profiles/traffic.json (ncu DRAM counters of both "
+                                           "phases captured on the 8M-point block, per bond)",
                          "alg_bytes_per_launch": alg_bytes, "ms_per_launch": dom_ms},
             "roofline_step": {"achieved": step_achieved, "peak": peak, "frac": step_achieved / peak,
                               "alg_bytes_per_step": step_bytes,

@@ -15,7 +15,7 @@ import pytest
 
 import oracle as O
 import pdcuda as pd
-from helpers import cube_body, deform, oracle_body, plate_body
+from helpers import cube_body, deform, oracle_bcs, oracle_body, plate_body
 
 
 def rel_err(a, b):
@@ -233,7 +233,6 @@ def test_fracturing_plate_trajectory():
     mk = lambda: pd.CMaterial(zem=pd.ZEMWan())
     body = plate_body(mk(), nx=24, ny=12, nz=3, nu=0.25)
     ob = oracle_body(body)
-    from helpers import oracle_bcs
     sf = SAFETY_FACTOR_WAN_PLATE
     dt = ob.stable_timestep(sf)
     ob.force_density(0.0, dt)

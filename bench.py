@@ -62,6 +62,8 @@ B_DR_POINT = {"fp64": 304.0, "fp32": 280.0}
 B_BOND = {"fp32": 20.125, "fp64": 36.125}
 B_POINT = {"fp32": 140.0, "fp64": 184.0}
 B_POINT_EXTRA = {"BB": 0.0, "OSB": 8.0, "C": 72.0, "CW": 96.0}
+# steps of the legs beside the timed run (per-kernel events, end to end): at most this many
+EAGER_STEPS = 500
 
 
 def pinned(*shape):
@@ -981,7 +983,9 @@ def jfnk_cpu_baseline(force_evals, budget_s=20.0):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--steps", type=int, default=None,
+                    help="timed steps (default: 5000 for osb8m, the 5000-step run of that "
+                         "workload; 200 otherwise)")
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="osb8m", choices=list(CONFIGS))
@@ -1021,6 +1025,8 @@ def main():
                     help="lane mappings per arm (the first is reported, the others give the spread)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
+    if args.steps is None:
+        args.steps = 5000 if args.config == "osb8m" and args.impl == "ours" else 200
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -1143,10 +1149,11 @@ def main():
         ms_total = dev.run_timed(step, args.steps, dt, phases=False)
         step += args.steps
         launches = dev.launch_count() - launches0
-        # per-kernel durations for the roofline: the same number of steps again, issued eagerly
-        # with events around every kernel on the handle's stream
-        _, ms_a, ms_b, ms_int = dev.run_timed(step, args.steps, dt)
-        step += args.steps
+        # per-kernel durations for the roofline: the following steps (at most EAGER_STEPS),
+        # issued eagerly with events around every kernel on the handle's stream
+        n_launch = min(args.steps, EAGER_STEPS)
+        _, ms_a, ms_b, ms_int = dev.run_timed(step, n_launch, dt)
+        step += n_launch
     barrier()
     ms_max = max_over_ranks(ms_total)
     value = n_bonds * args.steps * world / (ms_max / 1e3)
@@ -1154,7 +1161,6 @@ def main():
 
     # roofline of the dominant kernel (per launch, algorithmic bytes)
     prec = args.precision
-    n_launch = args.steps
     per_kernel = {"phase_a": ms_a / n_launch, "phase_b": ms_b / n_launch}
     dom = max(per_kernel, key=per_kernel.get) if mat != "BB" else "phase_a"
     dom_ms = per_kernel[dom]
@@ -1183,7 +1189,7 @@ def main():
 
     # FP64 comparison on the same workload
     fp64 = None
-    f64_steps = args.fp64_steps if args.fp64_steps >= 0 else max(args.steps // 4, 10)
+    f64_steps = args.fp64_steps if args.fp64_steps >= 0 else min(max(args.steps // 4, 10), 250)
     if prec == "fp32" and f64_steps > 0:
         dev.close()
         _, d64, dt64 = build("fp64")
@@ -1210,16 +1216,17 @@ def main():
     dev.run(1, max(args.warmup, 3, gsteps), dt)
     dev.field("displacement", out=out_u)
     barrier()
+    e2e_steps = min(args.steps, EAGER_STEPS)
     t0 = time.perf_counter()
     dev.set_state(displacement=h_u, velocity=h_v)
-    dev.run(1, args.steps, dt)
+    dev.run(1, e2e_steps, dt)
     dev.field("displacement", out=out_u)
     dev.field("damage", out=out_d)
     e2e_s = time.perf_counter() - t0
     e2e_s = max_over_ranks(e2e_s)
-    h2d = (h_u.nbytes + h_v.nbytes) / args.steps
-    d2h = (out_u.nbytes + out_d.nbytes) / args.steps
-    e2e = n_bonds * args.steps * world / e2e_s
+    h2d = (h_u.nbytes + h_v.nbytes) / e2e_steps
+    d2h = (out_u.nbytes + out_d.nbytes) / e2e_steps
+    e2e = n_bonds * e2e_steps * world / e2e_s
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -1257,13 +1264,15 @@ def main():
                               "ms": {"phase_a": ms_a / n_launch, "phase_b": ms_b / n_launch,
                                      "integrate": ms_int / n_launch}},
             "fp64_value": fp64, "fp32_over_fp64": (value / fp64) if fp64 else None,
-            "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                    "steps": e2e_steps},
             "gpu_launches": launches, "clocks": clocks, "cpu_baseline": cpu,
             "jfnk": jfnk,
-            "timing": ("value: the timed steps as CUDA graphs of graph_steps steps between two "
-                       "events; roofline: the same number of steps issued eagerly with events "
-                       "around every kernel" if gsteps else
-                       "value and roofline: eager launches with events around every kernel"),
+            "timing": (f"value: the timed steps as CUDA graphs of graph_steps steps between two "
+                       f"events; roofline: the next {n_launch} steps issued eagerly with events "
+                       f"around every kernel" if gsteps else
+                       f"value: eager launches between two events; roofline: the next {n_launch} "
+                       f"steps with events around every kernel"),
         }
         print(json.dumps(line), flush=True)
     if dist:

@@ -984,8 +984,8 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=None,
-                    help="timed steps (default: 5000 for osb8m, the 5000-step run of that "
-                         "workload; 200 otherwise)")
+                    help="timed steps (default: the workload's own run, 5000 for osb8m and 500 "
+                         "for plate3200; 200 otherwise)")
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="osb8m", choices=list(CONFIGS))
@@ -1026,7 +1026,8 @@ def main():
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
     if args.steps is None:
-        args.steps = 5000 if args.config == "osb8m" and args.impl == "ours" else 200
+        own = {"osb8m": 5000, "plate3200": 500}
+        args.steps = own.get(args.config, 200) if args.impl == "ours" else 200
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

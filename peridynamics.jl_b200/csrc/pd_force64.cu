@@ -418,6 +418,143 @@ __global__ void PD_LB64 k_osb_b64(DevBody d, int kstep) {
 }
 
 // -------------------------------------------------------------------------------------------
+// OSB phases for the mappings other than the serial order: two rows per iteration (two
+// neighbour gathers in flight per lane), the weighted volume from the stored bond length
+// (L^2 for |X_j - X_i|^2, equal to a few units in the last place), and in phase B the point's
+// own term and its neighbour's term of a bond summed before one division by l. The failure
+// test keeps the reference's eps = (l - L) / L. Results differ from the serial order by a few
+// units in the last place, as the lane-group sums already do.
+// -------------------------------------------------------------------------------------------
+template <int G, bool ESC>
+__global__ void __launch_bounds__(256, 3) k_osb_a64f(DevBody d, int kstep) {
+  if (d.ctrl->err) return;
+  PD_SLICE_LOOP(G) {
+    PD_SLICE_SETUP
+    double wvol = 0.0, sdil = 0.0;
+    int na = 0;
+    const DevParam& P = d.params[valid ? (d.meta[i] & META_PID_MASK) : 0];
+    const double4 xi = valid ? ld4(d.cur + i) : make_double4(0, 0, 0, 0);
+    const int self = valid ? (int)i : 0;
+    for (int r = 0; r < rows; r += 2) {
+      const bool two = r + 1 < rows;
+      const long long wi = (sbase >> 5) + r;
+      const unsigned w0 = d.bits[wi], w1 = two ? d.bits[wi + 1] : 0u;
+      const int k0 = r * G + gl, k1 = k0 + G;
+      const bool h0 = k0 < cnt, h1 = two && k1 < cnt;
+      const long long b0 = sbase + (long long)r * 32 + lane, b1 = b0 + 32;
+      const int j0 = h0 ? __ldg(d.nbr + b0) : self, j1 = h1 ? __ldg(d.nbr + b1) : self;
+      const double Ls0 = h0 ? __ldg(d.len64 + b0) : 1.0, Ls1 = h1 ? __ldg(d.len64 + b1) : 1.0;
+      const double4 x0 = ld4(d.cur + j0), x1 = ld4(d.cur + j1);
+      bool act0 = false, act1 = false;
+#pragma unroll
+      for (int u = 0; u < 2; u++) {
+        if (!(u ? h1 : h0)) continue;
+        const double4 xj = u ? x1 : x0;
+        const double Ls = u ? Ls1 : Ls0;
+        const double L = fabs(Ls);
+        const double dx = xj.x - xi.x, dy = xj.y - xi.y, dz = xj.z - xi.z;
+        const double l = sqrt((dx * dx + dy * dy) + dz * dz);
+        const double eps = (l - L) / L;
+        const bool act = (((u ? w1 : w0) >> lane) & 1u) && !(eps > P.epsc && Ls > 0);
+        if (act) {
+          const double bet = ESC ? __ldg(d.sc64 + (u ? b1 : b0)) : 1.0;
+          const double t = omega_of(d.kernel, P.delta, L) * bet * xj.w;
+          wvol += t * (L * L);
+          sdil += t * L * (l - L);
+        }
+        if (u) act1 = act; else act0 = act;
+      }
+      na += act0 + act1;
+      commit_row64(d.bits, wi, w0, act0, lane);
+      if (two) commit_row64(d.bits, wi + 1, w1, act1, lane);
+    }
+    if (G > 1) {
+      wvol = group_sum<G>(wvol); sdil = group_sum<G>(sdil); na = group_sum<G>(na);
+    }
+    if (valid && gl == 0) {
+      double c1 = 0.0, c2 = 0.0, dil = 0.0;
+      if (wvol != 0.0) {
+        dil = 3.0 / wvol * sdil;
+        c1 = 15.0 * P.G / wvol;
+        c2 = dil * (3.0 * P.K / wvol - c1 / 3.0);
+      }
+      d.coef64[i] = make_double4(c1, c2, wvol, dil);
+      d.n_active[i] = na;
+    }
+  }
+}
+
+// omega beta (c2 L + c1 (l - L)) of a bond owner o with partner q: osb_s64 before its division
+template <bool MULTI>
+__device__ __forceinline__ double osb_num64(const double4& co, const DevParam& Po, const DevParam& Pq,
+                                            double om, double bet, double L, double l) {
+  double c1, c2;
+  if (MULTI) {
+    c1 = 15.0 * (Po.G + Pq.G) / (2 * co.z);
+    c2 = co.w * (3.0 * (Po.K + Pq.K) / (2 * co.z) - c1 / 3.0);
+  } else {
+    c1 = co.x;
+    c2 = co.y;
+  }
+  return om * bet * (c2 * L + c1 * (l - L));
+}
+
+template <int G, bool MULTI, bool ESC>
+__global__ void __launch_bounds__(256, 2) k_osb_b64f(DevBody d, int kstep) {
+  if (d.ctrl->err) return;
+  PD_SLICE_LOOP(G) {
+    PD_SLICE_SETUP
+    double bx = 0.0, by = 0.0, bz = 0.0;
+    const DevParam& Pi = d.params[valid ? (d.meta[i] & META_PID_MASK) : 0];
+    const double4 xi = valid ? ld4(d.cur + i) : make_double4(0, 0, 0, 0);
+    const double4 ci = valid ? d.coef64[i] : make_double4(0, 0, 0, 0);
+    const bool own = ci.z != 0.0;
+    const int self = valid ? (int)i : 0;
+    for (int r = 0; r < rows; r += 2) {
+      const bool two = r + 1 < rows;
+      const long long wi = (sbase >> 5) + r;
+      const unsigned w0 = __ldg(d.bits + wi), w1 = two ? __ldg(d.bits + wi + 1) : 0u;
+      const int k0 = r * G + gl, k1 = k0 + G;
+      const bool h0 = k0 < cnt, h1 = two && k1 < cnt;
+      const long long b0 = sbase + (long long)r * 32 + lane, b1 = b0 + 32;
+      const int j0 = h0 ? __ldg(d.nbr + b0) : self, j1 = h1 ? __ldg(d.nbr + b1) : self;
+      const double Ls0 = h0 ? __ldg(d.len64 + b0) : 1.0, Ls1 = h1 ? __ldg(d.len64 + b1) : 1.0;
+      const double4 x0 = ld4(d.cur + j0), x1 = ld4(d.cur + j1);
+      const double4 c0 = d.coef64[j0], c1 = d.coef64[j1];
+#pragma unroll
+      for (int u = 0; u < 2; u++) {
+        if (!(u ? h1 : h0)) continue;
+        const double4 xj = u ? x1 : x0;
+        const double4 cj = u ? c1 : c0;
+        const int j = u ? j1 : j0;
+        const long long b = u ? b1 : b0;
+        const double L = fabs(u ? Ls1 : Ls0);
+        const double dx = xj.x - xi.x, dy = xj.y - xi.y, dz = xj.z - xi.z;
+        const double l = sqrt((dx * dx + dy * dy) + dz * dz);
+        const bool ai = ((u ? w1 : w0) >> lane) & 1u;
+        const bool aj = d.sym ? ai : bond_bit(d.bits, rev_slot(d, b, j));
+        const DevParam& Pj = d.params[d.meta[j] & META_PID_MASK];
+        const double bet = ESC ? __ldg(d.sc64 + b) : 1.0;
+        double num = 0.0;
+        if (own && ai) num += osb_num64<MULTI>(ci, Pi, Pj, omega_of(d.kernel, Pi.delta, L), bet, L, l);
+        // j returned early for a zero weighted volume (iszero(wvol))
+        if (cj.z != 0.0 && aj)
+          num += osb_num64<MULTI>(cj, Pj, Pi, omega_of(d.kernel, Pj.delta, L), bet, L, l);
+        const double sc = num / l * xj.w;
+        bx += sc * dx;
+        by += sc * dy;
+        bz += sc * dz;
+      }
+    }
+    if (G > 1) { bx = group_sum<G>(bx); by = group_sum<G>(by); bz = group_sum<G>(bz); }
+    if (valid && gl == 0) {
+      d.b64[3 * i] = bx; d.b64[3 * i + 1] = by; d.b64[3 * i + 2] = bz;
+      flag_nan(d, kstep, bx, by, bz);
+    }
+  }
+}
+
+// -------------------------------------------------------------------------------------------
 // CMat phase A: calc_failure! (bond_system.jl:309-327), calc_damage!,
 // calc_deformation_gradient! (correspondence.jl:193-214), too_much_damage! (:288-298),
 // calc_first_piola_kirchhoff! (:216-224)
@@ -662,7 +799,7 @@ static int launch_osb64(const DevBody& d, const LaunchCfg& c, int G, int grid, i
   int launches = 0;
   if (A) {
     if (c.exact) k_osb_a64<1, true, ESC><<<grid, c.block, 0, s>>>(d, kstep);
-    else { PD_DISPATCH_G(G, (k_osb_a64<GG, false, ESC><<<grid, c.block, 0, s>>>(d, kstep))); }
+    else { PD_DISPATCH_G(G, (k_osb_a64f<GG, ESC><<<grid, c.block, 0, s>>>(d, kstep))); }
     launches++;
   }
   if (B) {
@@ -670,9 +807,9 @@ static int launch_osb64(const DevBody& d, const LaunchCfg& c, int G, int grid, i
       if (d.multi) k_osb_b64<1, true, true, ESC><<<grid, c.block, 0, s>>>(d, kstep);
       else k_osb_b64<1, true, false, ESC><<<grid, c.block, 0, s>>>(d, kstep);
     } else if (d.multi) {
-      PD_DISPATCH_G(G, (k_osb_b64<GG, false, true, ESC><<<grid, c.block, 0, s>>>(d, kstep)));
+      PD_DISPATCH_G(G, (k_osb_b64f<GG, true, ESC><<<grid, c.block, 0, s>>>(d, kstep)));
     } else {
-      PD_DISPATCH_G(G, (k_osb_b64<GG, false, false, ESC><<<grid, c.block, 0, s>>>(d, kstep)));
+      PD_DISPATCH_G(G, (k_osb_b64f<GG, false, ESC><<<grid, c.block, 0, s>>>(d, kstep)));
     }
     launches++;
   }

@@ -256,6 +256,14 @@ def test_asymmetric_bond_states_use_reverse_bonds():
     ob.force_density()
     dev.force()
     assert np.array_equal(dev.field("b_int").T, ob.b_int)
+    for group in (1, 4, 32):   # the two-row kernels of the lane-group mappings
+        dg = pd.DeviceBody(body, precision="fp64")
+        dg.set_mapping(group)
+        dg.set_state(bond_active=ba, position=ob.pos)
+        dg.force()
+        assert rel_err(dg.field("b_int").T, ob.b_int) < 1e-12, group
+        assert np.array_equal(dg.field("n_active_bonds"), ob.n_active), group
+        dg.close()
     dev32 = pd.DeviceBody(body, precision="fp32")
     dev32.set_state(bond_active=ba, displacement=ob.pos - body._pos)
     dev32.force()

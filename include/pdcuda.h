@@ -280,12 +280,13 @@ pd_status pd_set_mapping(pd_handle *h, int32_t group, int32_t block);
  * the sliced bond arrays staged in shared memory by TMA bulk copies (4 rows x 3 stages,
  * 4 rows x 4 stages, 8 rows x 3 stages per warp; one lane per point, BB or OSB); 4 = direct
  * loads two rows at a time, all their neighbour gathers in flight together (BB, OSB; results
- * identical to 0); 5 = OSB and CMat with the x and y components of every bond vector and
+ * identical to 0); 5 = BB, OSB and CMat with the x and y components of every bond vector and
  * 3x3 row in packed FP32 pairs, the bond states selecting instead of branching, and the next
  * row pair's bond stream loaded (as streaming loads) while the current pair is computed (one
- * lane per point and one parameter set; phase B needs symmetric bond states, OSB phase A no
- * surface correction; where they do not apply the phase runs as 4, CMat as 0; same FP32 form,
- * roundings differ in the order of a few operations). pd_autotune times all that apply. */
+ * lane per point and one parameter set; phase B needs symmetric bond states and, for CMat,
+ * ZEMSilling; BB and OSB need no surface correction; where they do not apply the phase runs
+ * as 4, CMat as 0; same FP32 form, roundings differ in the order of a few operations).
+ * pd_autotune times all that apply. */
 pd_status pd_set_pipeline(pd_handle *h, int32_t pipe);
 
 /* The current mapping (group 0 = serial order), block size and bond-stream variant. */

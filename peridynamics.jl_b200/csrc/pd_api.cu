@@ -1559,8 +1559,8 @@ extern "C" pd_status pd_set_pipeline(pd_handle* h, int32_t pipe) {
   if (pipe < 0 || pipe > 5) return fail(PD_ERR_ARG, "pipe must be 0 to 5");
   if (pipe == 4 && (h->precision != PD_PREC_FP32_KAHAN || h->material == PD_MAT_CMAT))
     return fail(PD_ERR_ARG, "the two-row kernels are the FP32 BB and OSB ones");
-  if (pipe == 5 && (h->precision != PD_PREC_FP32_KAHAN || h->material == PD_MAT_BB))
-    return fail(PD_ERR_ARG, "the packed-pair kernels are the FP32 OSB and CMat ones");
+  if (pipe == 5 && h->precision != PD_PREC_FP32_KAHAN)
+    return fail(PD_ERR_ARG, "the packed-pair kernels are FP32 ones");
   if (pipe >= 1 && pipe <= 3 && (h->precision != PD_PREC_FP32_KAHAN || !tma_supported(h->d)))
     return fail(PD_ERR_ARG, "the staged bond stream needs the FP32 path, one lane per point and BB or OSB");
   h->cfg.pipe = pipe;

@@ -1268,8 +1268,11 @@ int launch_force32(const DevBody& d, const LaunchCfg& c, int kstep, int phase, c
   int launches = 0;
   if (d.material == MAT_BB) {
     if (!A) return 0;
-    if (d.sc32) launch_bb32<true>(d, c, G, grid, kstep, s);
-    else launch_bb32<false>(d, c, G, grid, kstep, s);
+    if (c.pipe == 5 && pk_supported(d, 1)) return launch_force32_pk(d, c, kstep, 1, s);
+    LaunchCfg c4 = c;
+    if (c.pipe == 5) c4.pipe = 4;   // the two-row kernel where the packed one does not apply
+    if (d.sc32) launch_bb32<true>(d, c4, G, grid, kstep, s);
+    else launch_bb32<false>(d, c4, G, grid, kstep, s);
     return 1;
   }
   if (d.material == MAT_OSB) {

@@ -264,10 +264,101 @@ __global__ void __launch_bounds__(256, PD_MINB_QA) k_osb_a32q(DevBody d, int kst
   }
 }
 
-// the packed kernels serve one lane per point, OSB without surface correction and with one
-// parameter set; phase B also needs symmetric bond states
+// BB (calc_failure! and force_density_point!, bond_based.jl:125-161) in one sweep with packed
+// pairs and the next row pair's stream in flight, as the OSB phases above: f = bc eps V_j eta / l
+// for the bonds that stay active, the failure test on eps = e / L.
+#ifndef PD_MINB_QBB
+#define PD_MINB_QBB 4
+#endif
+__global__ void __launch_bounds__(256, PD_MINB_QBB) k_bb32q(DevBody d, int kstep) {
+  if (d.ctrl->err) return;
+  const int lane = threadIdx.x & 31;
+  const long long warp0 = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+  for (long long s = warp0; s < d.nslices; s += nwarps) {
+    const long long i = s * 32 + lane;
+    const bool valid = i < d.n;
+    const int self = valid ? (int)i : 0;
+    const long long sbase = d.soff[s];
+    const int rows = (int)((d.soff[s + 1] - sbase) >> 5);
+    const DevParam& P = d.params[d.meta[self] & META_PID_MASK];
+    const float epsc = P.epscf, bc = P.bcf;
+    const float4 hi = d.uhi[self], lo = d.ulo[self];
+    const float2 nhi = make_float2(-hi.x, -hi.y), nlo = make_float2(-lo.x, -lo.y);
+    const float nhz = -hi.z, nlz = -lo.z;
+    const int* pn = d.nbr + sbase + lane;
+    const float4* pg = d.geo + sbase + lane;
+    unsigned* pw = d.bits + (sbase >> 5);
+    KSum2 bxy;
+    KSum1 bz;
+    int na = 0;
+    int nj0 = self, nj1 = self;
+    float4 ng0 = make_float4(0.f, 0.f, 0.f, 1.f), ng1 = ng0;
+    unsigned nw0 = 0u, nw1 = 0u;
+    // the state words are plain loads: this warp owns them and rewrites them below
+    auto load_pair = [&](int r) {
+      const bool two = r + 1 < rows;
+      nw0 = pw[r];
+      nw1 = two ? pw[r + 1] : 0u;
+      nj0 = ld_stream(pn + 32 * r);
+      ng0 = ld_stream(pg + 32 * r);
+      if (two) { nj1 = ld_stream(pn + 32 * r + 32); ng1 = ld_stream(pg + 32 * r + 32); }
+      else { nj1 = self; ng1 = make_float4(0.f, 0.f, 0.f, 1.f); }
+    };
+    if (rows > 0) load_pair(0);
+    for (int r = 0; r < rows; r += 2) {
+      const bool two = r + 1 < rows;
+      const unsigned w0 = nw0, w1 = nw1;
+      const bool a0 = (w0 >> lane) & 1u, a1 = (w1 >> lane) & 1u;
+      const int j0 = a0 ? nj0 : self, j1 = a1 ? nj1 : self;
+      const float4 g0 = ng0, g1 = ng1;
+      const float4 hj0 = __ldg(d.uhi + j0), lj0 = __ldg(d.ulo + j0);
+      const float4 hj1 = __ldg(d.uhi + j1), lj1 = __ldg(d.ulo + j1);
+      if (r + 2 < rows) load_pair(r + 2);
+      bool act0, act1;
+#pragma unroll
+      for (int u = 0; u < 2; u++) {
+        const float4& g = u ? g1 : g0;
+        const float4& hj = u ? hj1 : hj0;
+        const bool a = u ? a1 : a0;
+        BondP B;
+        bond_pk(g, hj, u ? lj1 : lj0, nhi, nhz, nlo, nlz, B);
+        const float eps = B.e * B.rL;
+        const bool act = a && !(eps > epsc && g.w > 0.f);
+        const float sc = act ? bc * eps * hj.w * B.rl : 0.f;
+        bxy.add(mul2(make_float2(sc, sc), B.exy));
+        bz.add(sc * B.ez);
+        if (u) act1 = act; else act0 = act;
+      }
+      na += (int)act0 + (int)act1;
+      const unsigned c0 = __ballot_sync(0xffffffffu, act0);
+      const unsigned c1 = __ballot_sync(0xffffffffu, act1);
+      if (lane == 0) {
+        if (c0 != w0) pw[r] = c0;
+        if (two && c1 != w1) pw[r + 1] = c1;
+      }
+    }
+    if (valid) {
+      const float2 v = bxy.value();
+      const float z = bz.value();
+      d.b32[3 * i] = v.x;
+      d.b32[3 * i + 1] = v.y;
+      d.b32[3 * i + 2] = z;
+      d.n_active[i] = na;
+      if (isnan(v.x) || isnan(v.y) || isnan(z)) {
+        const long long step = d.ctrl->base + kstep;
+        if (atomicExch(&d.ctrl->err, 1) == 0) d.ctrl->err_step = step;
+        else atomicMin(&d.ctrl->err_step, step);
+      }
+    }
+  }
+}
+
+// the packed kernels serve one lane per point, BB and OSB without surface correction and with
+// one parameter set; OSB's phase B also needs symmetric bond states
 bool pk_supported(const DevBody& d, int phase) {
-  if (d.material != MAT_OSB || d.lg != 1 || d.sc32 != nullptr || d.multi) return false;
+  if (d.material == MAT_CMAT || d.lg != 1 || d.sc32 != nullptr || d.multi) return false;
+  if (d.material == MAT_BB) return phase == 1;
   if (phase == 2 && !d.sym) return false;
   return true;
 }
@@ -284,6 +375,11 @@ int launch_force32_pk(const DevBody& d, const LaunchCfg& c, int kstep, int phase
   const int grid = grid_pk(d.nslices, c.block);
   const bool lin = d.kernel == KER_LINEAR;
   int launches = 0;
+  if (d.material == MAT_BB) {
+    if (phase == 2) return 0;
+    k_bb32q<<<grid, c.block, 0, s>>>(d, kstep);
+    return 1;
+  }
   if (phase != 2) {
     if (c.fullk) {
       if (lin) k_osb_a32q<true, true><<<grid, c.block, 0, s>>>(d, kstep);

@@ -495,3 +495,27 @@ def test_packed_cmat_kernels_against_oracle(model):
     broken_ref = np.count_nonzero(ob.bond_active[:ob.n_bonds] == 0)
     broken = np.count_nonzero(five["bond_active_run"] == 0)
     assert abs(broken - broken_ref) <= max(2, 0.01 * broken_ref)
+
+
+def test_packed_bb_kernel_against_oracle():
+    """The packed BB kernel (pipe 5): force density on a deformed cube with fracture within the
+    FP32 tolerance of the oracle and 1e-6 of the two-row kernel with the same failure decisions;
+    a 150-step fracturing plate within 1e-5 of the oracle."""
+    body = cube_body(pd.BBMaterial(), n=9, fracture=True)
+    u = deform(body._pos, amplitude=0.002)
+    ob = oracle_body(body)
+    ob.pos[:] = body._pos + u
+    ob.force_density()
+    for block in (128, 256):
+        four, five = packed_and_two_row(body, u, block=block)
+        assert rel_err(five["b_int"].T, ob.b_int) < 2e-5
+        assert rel_err(five["b_int"], four["b_int"]) < 1e-6
+        for f in ("n_active_bonds", "bond_active", "damage"):
+            assert np.array_equal(five[f], four[f]), f
+    body = plate_body(pd.BBMaterial(), nx=24, ny=12, nz=3)
+    ob, _ = run_pair(body, 150, "fp64", mapping=0)
+    four, five = packed_and_two_row(body, steps=150)
+    assert rel_err(five["displacement"].T, ob.u) < 1e-5
+    broken_ref = np.count_nonzero(ob.bond_active[:ob.n_bonds] == 0)
+    broken = np.count_nonzero(five["bond_active_run"] == 0)
+    assert broken_ref > 0 and abs(broken - broken_ref) <= max(2, 0.01 * broken_ref)

@@ -903,7 +903,8 @@ __global__ void __launch_bounds__(256, PD_MINB_CB) k_c_b32(DevBody d, int kstep)
 // CMat phases with packed pairs and the next row pair's bond stream in flight (bond-stream
 // variant 5; one lane per point, one parameter set; phase B for symmetric bond states). The
 // per-bond sums are those of k_c_a32 / k_c_b32: the x and y rows of every 3x3 sum are one
-// packed compensated pair, z is scalar; bond states select the contributions (inactive bonds
+// packed pair, z is scalar (the shape-tensor and force sums compensated, the
+// displacement-gradient sums of phase A plain); bond states select the contributions (inactive bonds
 // and padding slots gather their own point and add zero). The per-point epilogue of phase A is
 // k_c_a32's. Phase B: with one influence value for both directions, t_ij + the term of j is
 // w V_j ((A_i + A_j) xi + (beta_i + beta_j) du).
@@ -970,8 +971,12 @@ __global__ void __launch_bounds__(256, PD_MINB_CQA) k_c_a32q(DevBody d, int kste
     const float4* pg = d.geo + sbase + lane;
     unsigned* pw = d.bits + (sbase >> 5);
     KSum2 K01, K23, K45;        // FULLK: (xx, yy), (zz, xy), (xz, yz)
-    KSum2 Hxy[3];               // rows x, y of column c of the displacement-gradient sum
-    KSum1 Hz[3];
+    // rows x, y of column c of the displacement-gradient sum, and row z: plain FP32 sums (with
+    // compensated sums phase A took 0.648 against 0.594 ms on the 1M-point CMat block, and the
+    // FP32 displacement after 250 steps was within 1.33e-7 of FP64 against 1.37e-7 here, RMS
+    // 7.85e-8 both: the error of the form comes from elsewhere)
+    float2 Hxy[3] = {make_float2(0.f, 0.f), make_float2(0.f, 0.f), make_float2(0.f, 0.f)};
+    float Hz[3] = {0.f, 0.f, 0.f};
     float dK[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
     int na = 0;
     int nj0 = self, nj1 = self;
@@ -1011,9 +1016,9 @@ __global__ void __launch_bounds__(256, PD_MINB_CQA) k_c_a32q(DevBody d, int kste
         const float Xz = g.z * id;
         const float2 tU = mul2(make_float2(t, t), mul2(B.dxy, id2));
         const float tUz = t * (B.dz * id);
-        Hxy[0].add(mul2(tU, make_float2(X.x, X.x))); Hz[0].add(tUz * X.x);
-        Hxy[1].add(mul2(tU, make_float2(X.y, X.y))); Hz[1].add(tUz * X.y);
-        Hxy[2].add(mul2(tU, make_float2(Xz, Xz)));   Hz[2].add(tUz * Xz);
+        Hxy[0] = add2(Hxy[0], mul2(tU, make_float2(X.x, X.x))); Hz[0] += tUz * X.x;
+        Hxy[1] = add2(Hxy[1], mul2(tU, make_float2(X.y, X.y))); Hz[1] += tUz * X.y;
+        Hxy[2] = add2(Hxy[2], mul2(tU, make_float2(Xz, Xz)));   Hz[2] += tUz * Xz;
         if constexpr (FULLK) {
           const float2 tX = mul2(make_float2(t, t), X);
           const float tXz = t * Xz;
@@ -1059,8 +1064,7 @@ __global__ void __launch_bounds__(256, PD_MINB_CQA) k_c_a32q(DevBody d, int kste
       finv3(Km, Kinv);
 #pragma unroll
       for (int c = 0; c < 3; c++) {
-        const float2 v = Hxy[c].value();
-        Hm[3 * c] = v.x; Hm[3 * c + 1] = v.y; Hm[3 * c + 2] = Hz[c].value();
+        Hm[3 * c] = Hxy[c].x; Hm[3 * c + 1] = Hxy[c].y; Hm[3 * c + 2] = Hz[c];
       }
       fmatmul(Hm, Kinv, H);
       bool hasnan = false;

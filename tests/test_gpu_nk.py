@@ -21,8 +21,9 @@ def rel(a, b):
     return np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300)
 
 
-def test_uniform_tension_bar_device_matches_oracle_and_analytic():
-    body = tension_bar(1 / 30)
+@pytest.mark.parametrize("zem", ["silling", "wan"])
+def test_uniform_tension_bar_device_matches_oracle_and_analytic(zem):
+    body = tension_bar(1 / 30, pd.ZEMWan() if zem == "wan" else None)
     nk = pd.NewtonKrylov(steps=5, tol=1e-3, maxiter=50)
     dev = pd.submit(pd.Job(body, nk))
     u = dev.field("displacement").T

@@ -82,11 +82,12 @@ def test_validation_rejects_time_conditions_and_fracture():
 LBAR, WBAR, HBAR, FBAR, EBAR = 1.0, 0.1, 0.1, 2e6, 200e9
 
 
-def tension_bar(dx):
-    """`newton_bar` of test_analytic_solutions.jl: CMaterial with ZEMSilling(Cs=0.5), left end
-    fixed by displacement conditions, the force F spread over the right layer as b_ext."""
+def tension_bar(dx, zem=None):
+    """`newton_bar` of test_analytic_solutions.jl: CMaterial with ZEMSilling(Cs=0.5) (or the
+    given stabilisation), left end fixed by displacement conditions, the force F spread over the
+    right layer as b_ext."""
     pos, vol = pd.uniform_box(LBAR + 3 * dx, WBAR, HBAR, dx, center=(-1.5 * dx, 0, 0))
-    body = pd.Body(pd.CMaterial(zem=pd.ZEMSilling(Cs=0.5)), pos, vol)
+    body = pd.Body(pd.CMaterial(zem=zem if zem is not None else pd.ZEMSilling(Cs=0.5)), pos, vol)
     pd.material(body, horizon=3.015 * dx, rho=7850.0, E=EBAR, nu=0.25)
     pd.point_set(body, "left", where=lambda p: p[0] < -LBAR / 2)
     pd.point_set(body, "right", where=lambda p: p[0] > LBAR / 2 - dx)
@@ -105,8 +106,9 @@ def nk_conditions(body):
     return out
 
 
-def test_oracle_uniform_tension_matches_analytic_band():
-    body = tension_bar(1 / 30)
+@pytest.mark.parametrize("zem", ["silling", "wan"])
+def test_oracle_uniform_tension_matches_analytic_band(zem):
+    body = tension_bar(1 / 30, pd.ZEMWan() if zem == "wan" else None)
     assert body.n_points == 297
     ob = oracle_body(body)
     nk = OracleNK(ob, nk_conditions(body))
@@ -116,8 +118,14 @@ def test_oracle_uniform_tension_matches_analytic_band():
     right = body.point_sets["right"]
     elong = ob.u[right, 0].mean()
     exact = FBAR / (EBAR * WBAR * HBAR) * LBAR
-    # the reference's band: measured 0.5 %, asserted < 2 %
-    assert abs(elong - exact) / exact < 0.02
+    if zem == "silling":
+        # the reference's band: measured 0.5 %, asserted < 2 %
+        assert abs(elong - exact) / exact < 0.02
+    else:
+        # the reference asserts its band for ZEMSilling only; ZEMWan's stiffness C : K^-1 acts
+        # on the non-affine part of the motion near the clamped and the loaded ends of this
+        # bar, three spacings thick: 3.05 % shorter than the closed form
+        assert abs(elong - exact) / exact < 0.05
 
 
 def small_beam(nx=24, ny=6, nz=4, dx=1e-3, load=-0.05e-3):

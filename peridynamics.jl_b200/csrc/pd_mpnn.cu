@@ -11,9 +11,8 @@
 //   x_i  16 features (k_feat_*)            h0 = relu(W0 x + b0)                     64
 //   m_l = mean_j h_{l-1,j};  h_l = h_{l-1} + relu(W_l [h_{l-1}; m_l] + b_l),  l = 1, 2
 //   A_i = Wo h2 + bo (3x3, column-major);  D_i = s I,  s = mean_j tr(A_j) / 3 (body readout)
-// The dense layers are BF16 tensor-core products (mma.sync m16n8k16, FP32 accumulation) with
-// the weights staged in shared memory; activations are stored as BF16, the aggregation sums
-// in FP32. Training minimises, over unit sample vectors r (recorded Krylov residual
+// The dense layers are BF16 tcgen05 products with FP32 accumulators in tensor memory (k_dense);
+// activations are stored as BF16, the aggregation sums in FP32. Training minimises, over unit sample vectors r (recorded Krylov residual
 // directions and random probes),
 //   L = sum_s w_s || (I - alpha_s K0 B)^2 r_s ||^2 / S,
 // the residual after one application of the block polynomial M = B (2 I - K0 B) with the
@@ -25,13 +24,14 @@
 // sample; the backward pass runs the same products transposed and reduces the weight gradients over the
 // points per block, then in a fixed order (deterministic). Adam updates FP32 master weights.
 //
-// The dense layers move 16-128 BF16 values per point against 64 outputs: at 500k points a
+// The dense layers move 16-128 BF16 values per point against 16-128 outputs: at 500k points a
 // layer is ~8 GFLOP, microseconds on the tensor cores; the network's time goes to the
-// neighbour gathers of the aggregation, which is why mma.sync fragments loaded straight from
-// shared memory are used here rather than a TMEM-resident tcgen05 pipeline.
+// neighbour gathers of the aggregation. The weight gradients (sums over all points, split over
+// blocks) use mma.sync m16n8k16 fragments.
 #include <cuda_bf16.h>
 
 #include <cmath>
+#include <cstddef>
 #include <cstring>
 #include <vector>
 
@@ -131,8 +131,15 @@ __global__ void k_feat_fin(long long n, const float* __restrict__ raw,
 }
 
 // ------------------------------------------------------------------------------------------
-// dense layers: Y[rows x NOUT] = [in0 | in1][rows x KIN] W^T, W row-major [NOUT][KIN] (BF16)
-// one warp = 16 rows; MODE selects the epilogue
+// dense layers: Y[rows x NOUT] = [in0 | in1][rows x KIN] W^T, W row-major [NOUT][KIN] (BF16),
+// on the 5th-generation tensor cores: a CTA of 128 threads takes tiles of 128 rows; the rows
+// and W sit in shared memory in the canonical K-major layout without swizzle (core matrices
+// of 8 rows x 16 bytes, the K-neighbour 128 bytes on, the row-neighbour KIN / 8 x 128 bytes
+// on); one thread issues the tcgen05.mma of every K step of 16 into an FP32 accumulator in
+// tensor memory (128 lanes x NOUT columns) and commits them to an mbarrier; each warp then
+// reads its 32 lanes (rows) back with tcgen05.ld and applies the MODE epilogue, one row per
+// thread. The wait on the mbarrier is bounded: on expiry the kernel records error 3 in
+// ctrl->err (a bounded wait gave up) and writes nothing for the tile.
 // ------------------------------------------------------------------------------------------
 enum { D_RELU = 0, D_RESID = 1, D_OUT = 2, D_BWD = 3, D_BWD_OUT = 4 };
 
@@ -148,80 +155,168 @@ struct DenseArgs {
   float* out_f;                 // D_OUT: D [n x 9]; D_BWD*: dh accumulate [n x 64]
   float* out_s;                 // D_BWD: s = dm / n_i [n x 64]
   const float* cnt;             // D_BWD: active bonds per point
+  int* err;                     // the body's error word (ctrl->err)
 };
 
-template <int KIN>
-__device__ __forceinline__ uint32_t lda(const DenseArgs& a, long long row, int col) {
-  if (row >= a.n) return 0u;
-  if (col < a.ld0) return *reinterpret_cast<const uint32_t*>(a.in0 + row * a.ld0 + col);
-  return *reinterpret_cast<const uint32_t*>(a.in1 + row * (KIN - a.ld0) + (col - a.ld0));
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
 }
+
+// SM100 shared-memory matrix descriptor: K-major, no swizzle, version 1
+__device__ __forceinline__ uint64_t umma_sdesc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+  return (uint64_t)((addr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+         ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | ((uint64_t)1 << 46);
+}
+
+template <int KIN, int NOUT>
+constexpr int dense_smem() { return (128 + NOUT) * KIN * 2 + 16; }
 
 template <int KIN, int NOUT, int MODE>
 __global__ void __launch_bounds__(128) k_dense(DenseArgs a) {
-  __shared__ __align__(16) bf16 Ws[NOUT * KIN];
-  for (int q = threadIdx.x; q < NOUT * KIN / 2; q += blockDim.x)
-    reinterpret_cast<uint32_t*>(Ws)[q] = reinterpret_cast<const uint32_t*>(a.W)[q];
+  static_assert(KIN % 16 == 0 && NOUT % 16 == 0 && NOUT <= 256, "UMMA shape M=128, N%16, K%16");
+  constexpr int TCOLS = NOUT < 32 ? 32 : NOUT;   // tensor-memory columns: a power of two >= 32
+  constexpr int CM = KIN / 8;                    // core matrices along K
+  extern __shared__ __align__(1024) unsigned char dsm[];
+  unsigned char* As = dsm;                       // 128 x KIN
+  unsigned char* Bs = dsm + 128 * KIN * 2;       // NOUT x KIN
+  uint64_t* bar = reinterpret_cast<uint64_t*>(dsm + (128 + NOUT) * KIN * 2);
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(bar + 1);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  auto put = [&](unsigned char* base, int row, int c, uint4 v) {
+    *reinterpret_cast<uint4*>(base + ((row >> 3) * CM + c) * 128 + (row & 7) * 16) = v;
+  };
+  for (int q = tid; q < NOUT * CM; q += 128)
+    put(Bs, q / CM, q % CM, *reinterpret_cast<const uint4*>(a.W + (size_t)(q / CM) * KIN + 8 * (q % CM)));
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                 :: "r"(smem_u32(tslot)), "r"(TCOLS));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  if (tid == 0) asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_u32(bar)));
+  asm volatile("tcgen05.fence::before_thread_sync;");
   __syncthreads();
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
-  for (long long tile = (long long)blockIdx.x * 4 + warp; tile * 16 < a.n;
-       tile += (long long)gridDim.x * 4) {
-    const long long r0 = tile * 16;
-    float acc[NOUT / 8][4];
+  asm volatile("tcgen05.fence::after_thread_sync;");
+  const uint32_t tmem = *tslot;
+  const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) |      // F32 <- BF16 x BF16
+                         ((uint32_t)(NOUT >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
+  uint32_t phase = 0;
+  for (long long tile = blockIdx.x; tile * 128 < a.n; tile += gridDim.x) {
+    const long long r0 = tile * 128;
+    {
+      const long long row = r0 + tid;
 #pragma unroll
-    for (int nt = 0; nt < NOUT / 8; nt++) acc[nt][0] = acc[nt][1] = acc[nt][2] = acc[nt][3] = 0.f;
-#pragma unroll
-    for (int k0 = 0; k0 < KIN; k0 += 16) {
-      uint32_t af[4];
-      af[0] = lda<KIN>(a, r0 + g, k0 + 2 * t);
-      af[1] = lda<KIN>(a, r0 + g + 8, k0 + 2 * t);
-      af[2] = lda<KIN>(a, r0 + g, k0 + 2 * t + 8);
-      af[3] = lda<KIN>(a, r0 + g + 8, k0 + 2 * t + 8);
-#pragma unroll
-      for (int nt = 0; nt < NOUT / 8; nt++) {
-        uint32_t bfm[2];
-        bfm[0] = *reinterpret_cast<const uint32_t*>(Ws + (nt * 8 + g) * KIN + k0 + 2 * t);
-        bfm[1] = *reinterpret_cast<const uint32_t*>(Ws + (nt * 8 + g) * KIN + k0 + 2 * t + 8);
-        mma16816(acc[nt], af, bfm);
+      for (int c = 0; c < CM; c++) {
+        uint4 v = make_uint4(0u, 0u, 0u, 0u);
+        if (row < a.n) {
+          const int col = 8 * c;
+          const bf16* src = col < a.ld0 ? a.in0 + row * a.ld0 + col
+                                        : a.in1 + row * (KIN - a.ld0) + (col - a.ld0);
+          v = *reinterpret_cast<const uint4*>(src);
+        }
+        put(As, tid, c, v);
       }
     }
+    asm volatile("fence.proxy.async.shared::cta;");
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    if (tid == 0) {
 #pragma unroll
-    for (int nt = 0; nt < NOUT / 8; nt++) {
-      const int c = nt * 8 + 2 * t;
+      for (int ks = 0; ks < KIN / 16; ks++) {
+        const uint64_t ad = umma_sdesc(smem_u32(As) + ks * 256, 128, CM * 128);
+        const uint64_t bd = umma_sdesc(smem_u32(Bs) + ks * 256, 128, CM * 128);
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n"
+            :: "r"(tmem), "l"(ad), "l"(bd), "r"(idesc), "r"(ks > 0 ? 1u : 0u));
+      }
+      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                   :: "r"(smem_u32(bar)) : "memory");
+    }
+    bool done = false;
+    for (int it = 0; it < (1 << 22) && !done; it++) {
+      uint32_t ok;
+      asm volatile(
+          "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+          "selp.u32 %0, 1, 0, p;\n\t}\n"
+          : "=r"(ok) : "r"(smem_u32(bar)), "r"(phase) : "memory");
+      done = ok != 0u;
+    }
+    if (!done && tid == 0) atomicExch(a.err, 3);
+    phase ^= 1u;
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    const long long row = r0 + 32 * warp + lane;
+    const bool live = row < a.n && done;
 #pragma unroll
-      for (int hf = 0; hf < 2; hf++) {
-        const long long row = r0 + g + 8 * hf;
-        if (row >= a.n) continue;
-        const float z0 = acc[nt][2 * hf], z1 = acc[nt][2 * hf + 1];
-        if (MODE == D_RELU) {
+    for (int c0 = 0; c0 < NOUT; c0 += 16) {
+      uint32_t v[16];
+      asm volatile(
+          "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+          : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
+            "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]),
+            "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+          : "r"(tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)c0));
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+      if (!live) continue;
+      float z[16];
+#pragma unroll
+      for (int q = 0; q < 16; q++) z[q] = __uint_as_float(v[q]);
+      if (MODE == D_RELU || MODE == D_RESID) {
+        uint32_t oh[8], oa[8];
+#pragma unroll
+        for (int q = 0; q < 8; q++) {
+          const int c = c0 + 2 * q;
           const float b0 = a.bias[c], b1 = a.bias[c + 1];
-          *reinterpret_cast<uint32_t*>(a.out_h + row * NOUT + c) =
-              pack2(fmaxf(z0 + b0, 0.f), fmaxf(z1 + b1, 0.f));
-        } else if (MODE == D_RESID) {
-          const float b0 = a.bias[c], b1 = a.bias[c + 1];
-          const float a0 = bfr(fmaxf(z0 + b0, 0.f)), a1 = bfr(fmaxf(z1 + b1, 0.f));
-          const float2 hp = unpack2(*reinterpret_cast<const uint32_t*>(a.resid + row * NOUT + c));
-          *reinterpret_cast<uint32_t*>(a.out_a + row * NOUT + c) = pack2(a0, a1);
-          *reinterpret_cast<uint32_t*>(a.out_h + row * NOUT + c) = pack2(hp.x + a0, hp.y + a1);
-        } else if (MODE == D_OUT) {
-          if (c < NO) a.out_f[row * NO + c] = z0 + a.bias[c];
-          if (c + 1 < NO) a.out_f[row * NO + c + 1] = z1 + a.bias[c + 1];
-        } else if (MODE == D_BWD_OUT) {
-          a.out_f[row * HID + c] = z0;
-          a.out_f[row * HID + c + 1] = z1;
-        } else {  // D_BWD: columns [0, 64) add to dh, [64, 128) become s = dm / n
-          if (c < HID) {
-            a.out_f[row * HID + c] += z0;
-            a.out_f[row * HID + c + 1] += z1;
+          if (MODE == D_RELU) {
+            oh[q] = pack2(fmaxf(z[2 * q] + b0, 0.f), fmaxf(z[2 * q + 1] + b1, 0.f));
           } else {
-            const float nn = a.cnt[row];
-            a.out_s[row * HID + c - HID] = nn > 0 ? z0 / nn : 0.f;
-            a.out_s[row * HID + c - HID + 1] = nn > 0 ? z1 / nn : 0.f;
+            const float a0 = bfr(fmaxf(z[2 * q] + b0, 0.f)), a1 = bfr(fmaxf(z[2 * q + 1] + b1, 0.f));
+            const float2 hp = unpack2(*reinterpret_cast<const uint32_t*>(a.resid + row * NOUT + c));
+            oa[q] = pack2(a0, a1);
+            oh[q] = pack2(hp.x + a0, hp.y + a1);
           }
+        }
+        uint4* dh = reinterpret_cast<uint4*>(a.out_h + row * NOUT + c0);
+        dh[0] = make_uint4(oh[0], oh[1], oh[2], oh[3]);
+        dh[1] = make_uint4(oh[4], oh[5], oh[6], oh[7]);
+        if (MODE == D_RESID) {
+          uint4* da = reinterpret_cast<uint4*>(a.out_a + row * NOUT + c0);
+          da[0] = make_uint4(oa[0], oa[1], oa[2], oa[3]);
+          da[1] = make_uint4(oa[4], oa[5], oa[6], oa[7]);
+        }
+      } else if (MODE == D_OUT) {
+#pragma unroll
+        for (int q = 0; q < 16; q++)
+          if (c0 + q < NO) a.out_f[row * NO + c0 + q] = z[q] + a.bias[c0 + q];
+      } else if (MODE == D_BWD_OUT) {
+        float4* o = reinterpret_cast<float4*>(a.out_f + row * HID + c0);
+#pragma unroll
+        for (int q = 0; q < 4; q++) o[q] = make_float4(z[4 * q], z[4 * q + 1], z[4 * q + 2], z[4 * q + 3]);
+      } else {  // D_BWD: columns [0, 64) add to dh, [64, 128) become s = dm / n
+        if (c0 < HID) {
+          float4* o = reinterpret_cast<float4*>(a.out_f + row * HID + c0);
+#pragma unroll
+          for (int q = 0; q < 4; q++) {
+            float4 t = o[q];
+            t.x += z[4 * q]; t.y += z[4 * q + 1]; t.z += z[4 * q + 2]; t.w += z[4 * q + 3];
+            o[q] = t;
+          }
+        } else {
+          const float nn = a.cnt[row];
+          float4* o = reinterpret_cast<float4*>(a.out_s + row * HID + c0 - HID);
+#pragma unroll
+          for (int q = 0; q < 4; q++)
+            o[q] = nn > 0 ? make_float4(z[4 * q] / nn, z[4 * q + 1] / nn, z[4 * q + 2] / nn,
+                                        z[4 * q + 3] / nn)
+                          : make_float4(0.f, 0.f, 0.f, 0.f);
         }
       }
     }
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();
   }
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" :: "r"(tmem), "r"(TCOLS));
 }
 
 // ------------------------------------------------------------------------------------------
@@ -596,11 +691,24 @@ static void refresh_weights(pd_mpnn* net, cudaStream_t s) {
   net->weights_dirty = false;
 }
 
-static int dense_grid(long long n) {
-  long long tiles = (n + 15) / 16;
-  long long b = (tiles + 3) / 4;
-  if (b > 148LL * 8) b = 148LL * 8;
-  return (int)(b < 1 ? 1 : b);
+// the body's error word (ctrl->err) as a device address
+static int* ctrl_err(pd_handle* h) {
+  return reinterpret_cast<int*>(reinterpret_cast<char*>(h->d.ctrl) + offsetof(Ctrl, err));
+}
+
+// a dense layer on the tensor cores: tiles of 128 rows, at most two CTAs per SM's worth of
+// grid (each CTA loops over tiles)
+template <int KIN, int NOUT, int MODE>
+static void launch_dense(const DenseArgs& a, cudaStream_t s) {
+  constexpr int smem = dense_smem<KIN, NOUT>();
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(k_dense<KIN, NOUT, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    attr = true;
+  }
+  long long tiles = (a.n + 127) / 128;
+  if (tiles > 296) tiles = 296;
+  k_dense<KIN, NOUT, MODE><<<(int)(tiles < 1 ? 1 : tiles), 128, smem, s>>>(a);
 }
 
 // features and forward pass on body h; D in net->Dv
@@ -616,7 +724,8 @@ static pd_status net_forward(pd_mpnn* net, pd_handle* h) {
   DenseArgs a{};
   a.n = n;
   a.in0 = net->x; a.ld0 = NF; a.W = net->W0; a.bias = th + O_B0; a.out_h = net->h0;
-  k_dense<NF, HID, D_RELU><<<dense_grid(n), 128, 0, s>>>(a);
+  a.err = ctrl_err(h);
+  launch_dense<NF, HID, D_RELU>(a, s);
   const int ag = grid1(n * 32, 256);
   bf16* hp = net->h0;
   bf16* ms[2] = {net->m1, net->m2};
@@ -628,13 +737,14 @@ static pd_status net_forward(pd_mpnn* net, pd_handle* h) {
     k_agg_mean<<<ag, 256, 0, s>>>(h->d, hp, net->cnt, ms[l]);
     DenseArgs b{};
     b.n = n; b.in0 = hp; b.ld0 = HID; b.in1 = ms[l]; b.W = Ws[l]; b.bias = th + ob[l];
-    b.resid = hp; b.out_a = as[l]; b.out_h = hs[l];
-    k_dense<2 * HID, HID, D_RESID><<<dense_grid(n), 128, 0, s>>>(b);
+    b.resid = hp; b.out_a = as[l]; b.out_h = hs[l]; b.err = ctrl_err(h);
+    launch_dense<2 * HID, HID, D_RESID>(b, s);
     hp = hs[l];
   }
   DenseArgs o{};
   o.n = n; o.in0 = net->h2; o.ld0 = HID; o.W = net->Wo; o.bias = th + O_BO; o.out_f = net->Dv;
-  k_dense<HID, NOP, D_OUT><<<dense_grid(n), 128, 0, s>>>(o);
+  o.err = ctrl_err(h);
+  launch_dense<HID, NOP, D_OUT>(o, s);
   k_trace_part<<<ISO_BLOCKS, 256, 0, s>>>(n, net->Dv, net->red + 4);
   k_iso_write<<<ISO_BLOCKS, 256, 0, s>>>(n, net->red + 4, ISO_BLOCKS, 1.0 / (3.0 * n), net->Dv, nullptr);
   h->launches += 11;
@@ -654,7 +764,8 @@ static pd_status net_backward(pd_mpnn* net, pd_handle* h) {
   k_wgrad_reduce<<<1, 64, 0, s>>>(net->cpart, WG_BLOCKS, NO, NO, net->grad + O_BO);
   DenseArgs o{};
   o.n = n; o.in0 = net->dDb; o.ld0 = NOP; o.W = net->WoT; o.out_f = net->dh;
-  k_dense<NOP, HID, D_BWD_OUT><<<dense_grid(n), 128, 0, s>>>(o);
+  o.err = ctrl_err(h);
+  launch_dense<NOP, HID, D_BWD_OUT>(o, s);
   const bf16* hprev[2] = {net->h0, net->h1};
   const bf16* ms[2] = {net->m1, net->m2};
   const bf16* as[2] = {net->a1, net->a2};
@@ -670,8 +781,8 @@ static pd_status net_backward(pd_mpnn* net, pd_handle* h) {
     k_wgrad_reduce<<<1, 64, 0, s>>>(net->cpart, WG_BLOCKS, HID, HID, net->grad + ob[l]);
     DenseArgs b{};
     b.n = n; b.in0 = net->dz; b.ld0 = HID; b.W = WT[l]; b.out_f = net->dh; b.out_s = net->sbuf;
-    b.cnt = net->cnt;
-    k_dense<HID, 2 * HID, D_BWD><<<dense_grid(n), 128, 0, s>>>(b);
+    b.cnt = net->cnt; b.err = ctrl_err(h);
+    launch_dense<HID, 2 * HID, D_BWD>(b, s);
     k_agg_adj<<<ag, 256, 0, s>>>(h->d, net->sbuf, net->dh);
   }
   k_relu_grad<<<eg, 256, 0, s>>>(n, net->dh, net->h0, net->dz);

@@ -696,18 +696,22 @@ static int* ctrl_err(pd_handle* h) {
   return reinterpret_cast<int*>(reinterpret_cast<char*>(h->d.ctrl) + offsetof(Ctrl, err));
 }
 
-// a dense layer on the tensor cores: tiles of 128 rows, at most two CTAs per SM's worth of
-// grid (each CTA loops over tiles)
+// a dense layer on the tensor cores: tiles of 128 rows; the grid holds as many CTAs per SM as
+// shared memory and the 512 tensor-memory columns of an SM allow (at most 8), each CTA looping
+// over tiles
 template <int KIN, int NOUT, int MODE>
 static void launch_dense(const DenseArgs& a, cudaStream_t s) {
   constexpr int smem = dense_smem<KIN, NOUT>();
+  constexpr int tcols = NOUT < 32 ? 32 : NOUT;
+  constexpr int by_smem = (227 * 1024) / smem, by_tmem = 512 / tcols;
+  constexpr int per_sm = by_smem < by_tmem ? (by_smem < 8 ? by_smem : 8) : (by_tmem < 8 ? by_tmem : 8);
   static bool attr = false;
   if (!attr) {
     cudaFuncSetAttribute(k_dense<KIN, NOUT, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     attr = true;
   }
   long long tiles = (a.n + 127) / 128;
-  if (tiles > 296) tiles = 296;
+  if (tiles > 148LL * per_sm) tiles = 148LL * per_sm;
   k_dense<KIN, NOUT, MODE><<<(int)(tiles < 1 ? 1 : tiles), 128, smem, s>>>(a);
 }
 

@@ -27,7 +27,7 @@
 // The dense layers move 16-128 BF16 values per point against 16-128 outputs: at 500k points a
 // layer is ~8 GFLOP, microseconds on the tensor cores; the network's time goes to the
 // neighbour gathers of the aggregation. The weight gradients (sums over all points, split over
-// blocks) use mma.sync m16n8k16 fragments.
+// blocks) are tcgen05 products too, the points being their contraction dimension (k_wgrad).
 #include <cuda_bf16.h>
 
 #include <cmath>
@@ -47,14 +47,6 @@ constexpr int O_W0 = 0, O_B0 = O_W0 + HID * NF, O_W1 = O_B0 + HID, O_B1 = O_W1 +
 constexpr int WG_BLOCKS = 296;  // blocks of the weight-gradient reductions (148 SMs x 2)
 
 using bf16 = __nv_bfloat16;
-
-__device__ __forceinline__ void mma16816(float* c, const uint32_t* a, const uint32_t* b) {
-  asm volatile(
-      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, "
-      "{%8,%9}, {%0,%1,%2,%3};\n"
-      : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
-      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
-}
 
 __device__ __forceinline__ uint32_t pack2(float lo, float hi) {
   __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
@@ -375,79 +367,232 @@ __global__ void k_relu_grad(long long n, const float* __restrict__ dh, const bf1
 }
 
 // ------------------------------------------------------------------------------------------
-// weight gradients: part[block][MO x KIN] = sum over the block's rows of dz^T X (tensor cores)
-// X = [in0 | in1] as in DenseArgs; dz row-major [rows x MO]
+// weight gradients G[o][k] = sum_i dz[i][o] x[i][k] of one dense layer (dz row-major
+// [rows x MO], x = [in0 | in1] as in DenseArgs) on the tensor cores, the points being the
+// contraction dimension. A CTA takes chunks of WG_P = 128 points with the grid's stride and
+// accumulates them in tensor memory: A = dz^T (MO rows, padded to 128 with rows of zeros
+// written once), B = x^T (KIN rows), eight tcgen05 products of K = 16 per chunk. With BIAS, B
+// carries 16 more rows written once, the first all ones and the rest zero: column KIN of the
+// product is then the bias gradient sum_i dz[i][o]. Each thread stages 8 x 8 blocks (8 points
+// x 8 features, one 16-byte load per point), transposed in registers, into the canonical
+// K-major layout. The CTA writes its partial sums to part[block][MO][KIN] (and bpart[block][MO]);
+// k_wgrad_reduce adds the blocks in a fixed order. The wait on each chunk's products is
+// bounded: on expiry the CTA records error 3 and writes zeros.
 // ------------------------------------------------------------------------------------------
-template <int MO, int KIN>
-__global__ void __launch_bounds__(256) k_wgrad(long long n, const bf16* __restrict__ dz,
+constexpr int WG_P = 128;
+
+template <int KIN, bool BIAS>
+__host__ __device__ constexpr int wgrad_n() { return BIAS ? KIN + 16 : KIN; }
+template <int KIN, bool BIAS>
+__host__ __device__ constexpr int wgrad_tcols() {
+  return wgrad_n<KIN, BIAS>() <= 32 ? 32 : wgrad_n<KIN, BIAS>() <= 64 ? 64
+       : wgrad_n<KIN, BIAS>() <= 128 ? 128 : 256;
+}
+template <int MO, int KIN, bool BIAS>
+constexpr int wgrad_smem() { return (128 + wgrad_n<KIN, BIAS>()) * WG_P * 2 + 16; }
+
+// 8 x 8 BF16 transpose: r[p] holds features 0..7 of point p; t[f] gets points 0..7 of feature f
+__device__ __forceinline__ void transpose8(const uint4 (&r)[8], uint4 (&t)[8]) {
+  uint32_t w[8][4];
+#pragma unroll
+  for (int p = 0; p < 8; p++) { w[p][0] = r[p].x; w[p][1] = r[p].y; w[p][2] = r[p].z; w[p][3] = r[p].w; }
+#pragma unroll
+  for (int f = 0; f < 8; f++) {
+    const int word = f >> 1, sel = (f & 1) ? 0x7632 : 0x5410;   // high or low halves
+    uint32_t o[4];
+#pragma unroll
+    for (int q = 0; q < 4; q++) o[q] = __byte_perm(w[2 * q][word], w[2 * q + 1][word], sel);
+    t[f] = make_uint4(o[0], o[1], o[2], o[3]);
+  }
+}
+
+template <int MO, int KIN, bool BIAS>
+__global__ void __launch_bounds__(128, 1) k_wgrad(long long n, const bf16* __restrict__ dz,
                                               const bf16* __restrict__ in0, int ld0,
                                               const bf16* __restrict__ in1,
-                                              float* __restrict__ part) {
-  __shared__ __align__(16) bf16 dzT[MO * 16];
-  __shared__ __align__(16) bf16 xT[KIN * 16];
-  constexpr int NT = KIN / 8, TILES = (MO / 16) * NT, PER = TILES / 8;
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
-  float acc[PER][4];
-#pragma unroll
-  for (int q = 0; q < PER; q++) acc[q][0] = acc[q][1] = acc[q][2] = acc[q][3] = 0.f;
-  const bf16 zero = __float2bfloat16_rn(0.f);
-  for (long long r0 = (long long)blockIdx.x * 16; r0 < n; r0 += (long long)gridDim.x * 16) {
-    for (int e = threadIdx.x; e < 16 * MO; e += blockDim.x) {
-      const int rr = e / MO, o = e % MO;
-      dzT[o * 16 + rr] = r0 + rr < n ? dz[(r0 + rr) * MO + o] : zero;
+                                              float* __restrict__ part, float* __restrict__ bpart,
+                                              int* err) {
+  constexpr int NB = wgrad_n<KIN, BIAS>();       // rows of B, the product's columns
+  static_assert(MO % 8 == 0 && MO <= 128 && KIN % 16 == 0 && NB <= 256, "UMMA shape M=128, N%16");
+  constexpr int CMK = WG_P / 8;                  // core matrices along K (points)
+  constexpr int TCOLS = wgrad_tcols<KIN, BIAS>();  // tensor-memory columns: a power of two >= 32
+  constexpr int FA = MO / 8, FB = KIN / 8;       // 8-feature groups of dz and x
+  extern __shared__ __align__(1024) unsigned char wsm[];
+  unsigned char* As = wsm;                       // 128 x WG_P (rows: o)
+  unsigned char* Bs = wsm + 128 * WG_P * 2;      // NB x WG_P (rows: k)
+  uint64_t* bar = reinterpret_cast<uint64_t*>(wsm + (128 + NB) * WG_P * 2);
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(bar + 1);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  // core matrix (row group, point group) at (rg * CMK + pg) * 128 B, row (row & 7) at 16 B
+  auto core = [&](unsigned char* base, int rg, int pg) { return base + (rg * CMK + pg) * 128; };
+  for (int q = tid; q < (128 - MO) * WG_P / 8; q += 128)   // rows MO..127 of A: zero
+    *reinterpret_cast<uint4*>(As + MO * WG_P * 2 + q * 16) = make_uint4(0u, 0u, 0u, 0u);
+  if (BIAS)   // rows KIN..KIN+15 of B: row KIN ones (BF16 1.0 = 0x3F80), the rest zero
+    for (int q = tid; q < 16 * WG_P / 8; q += 128) {
+      const uint32_t one = q / 8 < CMK && q % 8 == 0 ? 0x3F803F80u : 0u;
+      *reinterpret_cast<uint4*>(Bs + KIN * WG_P * 2 + q * 16) = make_uint4(one, one, one, one);
     }
-    for (int e = threadIdx.x; e < 16 * KIN; e += blockDim.x) {
-      const int rr = e / KIN, k = e % KIN;
-      bf16 v = zero;
-      if (r0 + rr < n) v = k < ld0 ? in0[(r0 + rr) * ld0 + k] : in1[(r0 + rr) * (KIN - ld0) + k - ld0];
-      xT[k * 16 + rr] = v;
-    }
-    __syncthreads();
-#pragma unroll
-    for (int q = 0; q < PER; q++) {
-      const int tile = warp * PER + q, mt = tile / NT, nt = tile % NT;
-      uint32_t af[4], bfm[2];
-      af[0] = *reinterpret_cast<const uint32_t*>(dzT + (mt * 16 + g) * 16 + 2 * t);
-      af[1] = *reinterpret_cast<const uint32_t*>(dzT + (mt * 16 + g + 8) * 16 + 2 * t);
-      af[2] = *reinterpret_cast<const uint32_t*>(dzT + (mt * 16 + g) * 16 + 2 * t + 8);
-      af[3] = *reinterpret_cast<const uint32_t*>(dzT + (mt * 16 + g + 8) * 16 + 2 * t + 8);
-      bfm[0] = *reinterpret_cast<const uint32_t*>(xT + (nt * 8 + g) * 16 + 2 * t);
-      bfm[1] = *reinterpret_cast<const uint32_t*>(xT + (nt * 8 + g) * 16 + 2 * t + 8);
-      mma16816(acc[q], af, bfm);
-    }
-    __syncthreads();
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                 :: "r"(smem_u32(tslot)), "r"(TCOLS));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
+  if (tid == 0) asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_u32(bar)));
+  asm volatile("tcgen05.fence::before_thread_sync;");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;");
+  const uint32_t tmem = *tslot;
+  const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) |      // F32 <- BF16 x BF16
+                         ((uint32_t)(NB >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
+  uint32_t phase = 0;
+  int chunks = 0;
+  bool bad = false;
+  for (long long c0 = (long long)blockIdx.x * WG_P; c0 < n; c0 += (long long)gridDim.x * WG_P) {
+    for (int u = tid; u < CMK * FA; u += 128) {
+      const int f = u % FA, pg = u / FA;
+      uint4 r[8], t[8];
+#pragma unroll
+      for (int p = 0; p < 8; p++) {
+        const long long i = c0 + 8 * pg + p;
+        r[p] = i < n ? *reinterpret_cast<const uint4*>(dz + i * MO + 8 * f) : make_uint4(0u, 0u, 0u, 0u);
+      }
+      transpose8(r, t);
+      unsigned char* dst = core(As, f, pg);
+#pragma unroll
+      for (int q = 0; q < 8; q++) *reinterpret_cast<uint4*>(dst + q * 16) = t[q];
+    }
+    for (int u = tid; u < CMK * FB; u += 128) {
+      const int f = u % FB, pg = u / FB, col = 8 * f;
+      uint4 r[8], t[8];
+#pragma unroll
+      for (int p = 0; p < 8; p++) {
+        const long long i = c0 + 8 * pg + p;
+        uint4 v = make_uint4(0u, 0u, 0u, 0u);
+        if (i < n) {
+          const bf16* src = col < ld0 ? in0 + i * ld0 + col : in1 + i * (KIN - ld0) + (col - ld0);
+          v = *reinterpret_cast<const uint4*>(src);
+        }
+        r[p] = v;
+      }
+      transpose8(r, t);
+      unsigned char* dst = core(Bs, f, pg);
+#pragma unroll
+      for (int q = 0; q < 8; q++) *reinterpret_cast<uint4*>(dst + q * 16) = t[q];
+    }
+    asm volatile("fence.proxy.async.shared::cta;");
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    if (tid == 0) {
+#pragma unroll
+      for (int ks = 0; ks < WG_P / 16; ks++) {
+        const uint64_t ad = umma_sdesc(smem_u32(As) + ks * 256, 128, CMK * 128);
+        const uint64_t bd = umma_sdesc(smem_u32(Bs) + ks * 256, 128, CMK * 128);
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n"
+            :: "r"(tmem), "l"(ad), "l"(bd), "r"(idesc), "r"((chunks > 0 || ks > 0) ? 1u : 0u));
+      }
+      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                   :: "r"(smem_u32(bar)) : "memory");
+    }
+    bool done = false;
+    for (int it = 0; it < (1 << 22) && !done; it++) {
+      uint32_t ok;
+      asm volatile(
+          "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+          "selp.u32 %0, 1, 0, p;\n\t}\n"
+          : "=r"(ok) : "r"(smem_u32(bar)), "r"(phase) : "memory");
+      done = ok != 0u;
+    }
+    phase ^= 1u;
+    chunks++;
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    // every thread has seen the products complete before shared memory is staged again
+    if (__syncthreads_or(!done)) { bad = true; break; }
+  }
+  if (bad && tid == 0) atomicExch(err, 3);
   float* out = part + (long long)blockIdx.x * MO * KIN;
+  if (32 * warp < MO) {
+    const int o = 32 * warp + lane;
 #pragma unroll
-  for (int q = 0; q < PER; q++) {
-    const int tile = warp * PER + q, mt = tile / NT, nt = tile % NT;
-    const int r = mt * 16 + g, c = nt * 8 + 2 * t;
-    out[r * KIN + c] = acc[q][0];
-    out[r * KIN + c + 1] = acc[q][1];
-    out[(r + 8) * KIN + c] = acc[q][2];
-    out[(r + 8) * KIN + c + 1] = acc[q][3];
+    for (int k0 = 0; k0 < NB; k0 += 16) {
+      uint32_t v[16];
+      if (chunks > 0 && !bad) {
+        asm volatile(
+            "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+            : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
+              "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]),
+              "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+            : "r"(tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)k0));
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+      } else {
+#pragma unroll
+        for (int q = 0; q < 16; q++) v[q] = 0u;
+      }
+      if (o < MO && k0 == KIN) {   // the bias column
+        bpart[(long long)blockIdx.x * MO + o] = __uint_as_float(v[0]);
+      } else if (o < MO) {
+        float4* dst = reinterpret_cast<float4*>(out + o * KIN + k0);
+#pragma unroll
+        for (int q = 0; q < 4; q++)
+          dst[q] = make_float4(__uint_as_float(v[4 * q]), __uint_as_float(v[4 * q + 1]),
+                               __uint_as_float(v[4 * q + 2]), __uint_as_float(v[4 * q + 3]));
+      }
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;");
+  __syncthreads();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" :: "r"(tmem), "r"(TCOLS));
+}
+
+// grad[e] += sum_b part[b][e] for e < used, in a fixed order: a block of 256 threads takes 32
+// elements; its eight warps each sum a contiguous eighth of the nb partials (lanes reading
+// consecutive elements), then warp 0 adds the eight sums in order
+__global__ void __launch_bounds__(256) k_wgrad_reduce(const float* __restrict__ part, int nb,
+                                                      int size, int used, float* __restrict__ grad) {
+  __shared__ float ps[8][32];
+  const int lane = threadIdx.x & 31, sl = threadIdx.x >> 5, e = blockIdx.x * 32 + lane;
+  float s = 0.f;
+  if (e < used)
+    for (int b = sl * nb / 8; b < (sl + 1) * nb / 8; b++) s += part[(long long)b * size + e];
+  ps[sl][lane] = s;
+  __syncthreads();
+  if (sl == 0 && e < used) {
+    float t = ps[0][lane];
+#pragma unroll
+    for (int k = 1; k < 8; k++) t += ps[k][lane];
+    grad[e] += t;
   }
 }
 
-// grad[off + e] += sum_b part[b][e] for e < rows_used * KIN (fixed order)
-__global__ void k_wgrad_reduce(const float* __restrict__ part, int nb, int size, int used,
-                               float* __restrict__ grad) {
-  const int e = blockIdx.x * blockDim.x + threadIdx.x;
-  if (e >= used) return;
+// column sums of v [n x COLS] (FP32), per block: block b takes a contiguous range of rows and
+// its 32 * COLS threads read the range's values with stride 32 * COLS, so that thread t always
+// meets column t % COLS and neighbouring threads read neighbouring words; the 32 sums of a
+// column are then added in a fixed order into part[b][c]
+template <int COLS>
+__global__ void __launch_bounds__(32 * COLS) k_colsum(long long n, const float* __restrict__ v,
+                                                      float* __restrict__ part) {
+  constexpr int T = 32 * COLS;
+  __shared__ float ps[T];
+  const long long rows = (n + gridDim.x - 1) / gridDim.x;
+  const long long r0 = (long long)blockIdx.x * rows;
+  const long long r1 = r0 + rows < n ? r0 + rows : n;
   float s = 0.f;
-  for (int b = 0; b < nb; b++) s += part[(long long)b * size + e];
-  grad[e] += s;
-}
-
-// column sums of dz (bf16 values) or of dD (fp32): per-block partials, then reduced
-template <typename T>
-__global__ void k_colsum(long long n, int cols, const T* __restrict__ v, float* __restrict__ part) {
-  // block b sums rows b, b + nb, ...; thread c < cols owns column c
-  const int c = threadIdx.x;
-  if (c >= cols) return;
-  float s = 0.f;
-  for (long long r = blockIdx.x; r < n; r += gridDim.x) s += (float)v[r * cols + c];
-  part[(long long)blockIdx.x * cols + c] = s;
+  if (r0 < r1) {
+    const float* src = v + r0 * COLS;
+    const long long m = (r1 - r0) * COLS;
+#pragma unroll 4
+    for (long long e = threadIdx.x; e < m; e += T) s += src[e];
+  }
+  ps[threadIdx.x] = s;
+  __syncthreads();
+  if (threadIdx.x < COLS) {
+    float t = 0.f;
+    for (int j = 0; j < 32; j++) t += ps[threadIdx.x + COLS * j];
+    part[(long long)blockIdx.x * COLS + threadIdx.x] = t;
+  }
 }
 
 // ------------------------------------------------------------------------------------------
@@ -715,6 +860,25 @@ static void launch_dense(const DenseArgs& a, cudaStream_t s) {
   k_dense<KIN, NOUT, MODE><<<(int)(tiles < 1 ? 1 : tiles), 128, smem, s>>>(a);
 }
 
+// grad[e] += the sum over the WG_BLOCKS partials part[b][e] (row stride size), e < used
+static void reduce_blocks(const float* part, int nb, int size, int used, float* grad, cudaStream_t s) {
+  k_wgrad_reduce<<<(used + 31) / 32, 256, 0, s>>>(part, nb, size, used, grad);
+}
+
+// the weight (and with BIAS the bias) gradients of one layer: WG_BLOCKS CTAs over the points,
+// partial sums per CTA
+template <int MO, int KIN, bool BIAS>
+static void launch_wgrad(long long n, const bf16* dz, const bf16* in0, int ld0, const bf16* in1,
+                         float* part, float* bpart, int* err, cudaStream_t s) {
+  constexpr int smem = wgrad_smem<MO, KIN, BIAS>();
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(k_wgrad<MO, KIN, BIAS>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    attr = true;
+  }
+  k_wgrad<MO, KIN, BIAS><<<WG_BLOCKS, 128, smem, s>>>(n, dz, in0, ld0, in1, part, bpart, err);
+}
+
 // features and forward pass on body h; D in net->Dv
 static pd_status net_forward(pd_mpnn* net, pd_handle* h) {
   const long long n = h->n;
@@ -760,12 +924,12 @@ static pd_status net_forward(pd_mpnn* net, pd_handle* h) {
 static pd_status net_backward(pd_mpnn* net, pd_handle* h) {
   const long long n = h->n;
   cudaStream_t s = h->stream;
-  // output layer: dWo = dDb^T h2 (16 x 64, rows 0..8 used), dbo = colsum dD, dh2 = dDb Wo
-  k_wgrad<NOP, HID><<<WG_BLOCKS, 256, 0, s>>>(n, net->dDb, net->h2, HID, nullptr, net->wpart);
-  k_wgrad_reduce<<<grid1(NO * HID, 256), 256, 0, s>>>(net->wpart, WG_BLOCKS, NOP * HID, NO * HID,
-                                                     net->grad + O_WO);
-  k_colsum<float><<<WG_BLOCKS, 32, 0, s>>>(n, NO, net->dD, net->cpart);
-  k_wgrad_reduce<<<1, 64, 0, s>>>(net->cpart, WG_BLOCKS, NO, NO, net->grad + O_BO);
+  // output layer: dWo = dDb^T h2 (16 x 64, rows 0..8 used), dbo = colsum dD (FP32), dh2 = dDb Wo;
+  // hidden layers: dW and db = colsum dz (BF16) from one k_wgrad
+  launch_wgrad<NOP, HID, false>(n, net->dDb, net->h2, HID, nullptr, net->wpart, nullptr, ctrl_err(h), s);
+  reduce_blocks(net->wpart, WG_BLOCKS, NOP * HID, NO * HID, net->grad + O_WO, s);
+  k_colsum<NO><<<WG_BLOCKS, 32 * NO, 0, s>>>(n, net->dD, net->cpart);
+  reduce_blocks(net->cpart, WG_BLOCKS, NO, NO, net->grad + O_BO, s);
   DenseArgs o{};
   o.n = n; o.in0 = net->dDb; o.ld0 = NOP; o.W = net->WoT; o.out_f = net->dh;
   o.err = ctrl_err(h);
@@ -778,11 +942,10 @@ static pd_status net_backward(pd_mpnn* net, pd_handle* h) {
   const int eg = grid1(n * HID, 256), ag = grid1(n * 32, 256);
   for (int l = 1; l >= 0; l--) {
     k_relu_grad<<<eg, 256, 0, s>>>(n, net->dh, as[l], net->dz);
-    k_wgrad<HID, 2 * HID><<<WG_BLOCKS, 256, 0, s>>>(n, net->dz, hprev[l], HID, ms[l], net->wpart);
-    k_wgrad_reduce<<<grid1(HID * 2 * HID, 256), 256, 0, s>>>(net->wpart, WG_BLOCKS, HID * 2 * HID,
-                                                            HID * 2 * HID, net->grad + ow[l]);
-    k_colsum<bf16><<<WG_BLOCKS, 64, 0, s>>>(n, HID, net->dz, net->cpart);
-    k_wgrad_reduce<<<1, 64, 0, s>>>(net->cpart, WG_BLOCKS, HID, HID, net->grad + ob[l]);
+    launch_wgrad<HID, 2 * HID, true>(n, net->dz, hprev[l], HID, ms[l], net->wpart, net->cpart,
+                                     ctrl_err(h), s);
+    reduce_blocks(net->wpart, WG_BLOCKS, HID * 2 * HID, HID * 2 * HID, net->grad + ow[l], s);
+    reduce_blocks(net->cpart, WG_BLOCKS, HID, HID, net->grad + ob[l], s);
     DenseArgs b{};
     b.n = n; b.in0 = net->dz; b.ld0 = HID; b.W = WT[l]; b.out_f = net->dh; b.out_s = net->sbuf;
     b.cnt = net->cnt; b.err = ctrl_err(h);
@@ -790,12 +953,10 @@ static pd_status net_backward(pd_mpnn* net, pd_handle* h) {
     k_agg_adj<<<ag, 256, 0, s>>>(h->d, net->sbuf, net->dh);
   }
   k_relu_grad<<<eg, 256, 0, s>>>(n, net->dh, net->h0, net->dz);
-  k_wgrad<HID, NF><<<WG_BLOCKS, 256, 0, s>>>(n, net->dz, net->x, NF, nullptr, net->wpart);
-  k_wgrad_reduce<<<grid1(HID * NF, 256), 256, 0, s>>>(net->wpart, WG_BLOCKS, HID * NF, HID * NF,
-                                                     net->grad + O_W0);
-  k_colsum<bf16><<<WG_BLOCKS, 64, 0, s>>>(n, HID, net->dz, net->cpart);
-  k_wgrad_reduce<<<1, 64, 0, s>>>(net->cpart, WG_BLOCKS, HID, HID, net->grad + O_B0);
-  h->launches += 26;
+  launch_wgrad<HID, NF, true>(n, net->dz, net->x, NF, nullptr, net->wpart, net->cpart, ctrl_err(h), s);
+  reduce_blocks(net->wpart, WG_BLOCKS, HID * NF, HID * NF, net->grad + O_W0, s);
+  reduce_blocks(net->cpart, WG_BLOCKS, HID, HID, net->grad + O_B0, s);
+  h->launches += 21;
   PD_CUDA(cudaGetLastError());
   return PD_OK;
 }

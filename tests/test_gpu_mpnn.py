@@ -69,6 +69,26 @@ def test_loss_and_gradient_match_oracle():
         o += k
 
 
+def test_gradient_with_several_point_chunks_per_block_matches_oracle():
+    """45,600 points: more 128-point chunks (357, the last one ragged) than the 296 blocks of
+    the weight-gradient kernels, so blocks accumulate two chunks in tensor memory."""
+    body, dev, onk, theta = setup_pair(nx=100, ny=24, nz=19, seed=5)
+    net = P.BlockPreconditionerNet(theta)
+    rng = np.random.default_rng(6)
+    samples = P.random_probes(onk.cmask, 2, rng)
+    loss, grad = net.loss_grad(dev, (), samples, alpha=0.6, weight=1.0)
+    P_blocks = onk.bj_blocks().astype(np.float32).astype(np.float64)
+    Lo, go = M.loss_grad(theta, onk, P_blocks, [s.astype(np.float64) for s in samples],
+                         alphas=[0.6] * len(samples))
+    assert abs(loss - Lo) <= 1e-3 * Lo
+    assert rel(grad, go) <= 3e-2
+    o = 0
+    for name, s in M.SHAPES:
+        k = int(np.prod(s))
+        assert rel(grad[o:o + k], go[o:o + k]) <= 6e-2, name
+        o += k
+
+
 def test_spectral_gradient_matches_oracle():
     body, dev, onk, theta = setup_pair(seed=2)
     plain = pd.NewtonKrylov(steps=1, tol=1e-8, tol_mode="relative", frechet="forward",

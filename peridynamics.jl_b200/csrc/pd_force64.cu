@@ -150,8 +150,15 @@ __device__ __forceinline__ void commit_row64(unsigned int* bits, long long word_
 // forces differ from the serial order by a few units in the last place, as the lane-group sums
 // already do. The failure decision keeps the reference's expression.
 // ESC: the bond's surface correction factor multiplies its force (bond_based.jl:156, 175)
+// rows of neighbour gathers in flight per lane in the FAST loop. Measured on the 500k-point
+// bending beam at 4 lanes per point (first two load increments, identical Krylov steps): 2 rows
+// (80 registers, three blocks of 256 per SM) block Jacobi 6.59 s / block polynomial 3.00 s; 3 rows
+// 7.37 / 3.26 s; 4 rows (116 registers, two blocks per SM) 7.02 / 3.13 s.
+#ifndef PD_BB64_ROWS
+#define PD_BB64_ROWS 2
+#endif
 template <int G, bool MULTI, bool FAST, bool ESC>
-__global__ void __launch_bounds__(256, FAST ? 3 : 2) k_bb64(DevBody d, int kstep) {
+__global__ void __launch_bounds__(256, FAST && PD_BB64_ROWS <= 2 ? 3 : 2) k_bb64(DevBody d, int kstep) {
   if (d.ctrl->err) return;
   PD_SLICE_LOOP(G) {
     PD_SLICE_SETUP
@@ -160,44 +167,54 @@ __global__ void __launch_bounds__(256, FAST ? 3 : 2) k_bb64(DevBody d, int kstep
     const double4 xi = valid ? ld4(d.cur + i) : make_double4(0, 0, 0, 0);
     const DevParam& P = d.params[valid ? (d.meta[i] & META_PID_MASK) : 0];
     if (FAST) {
-      // two rows per iteration: two independent neighbour gathers in flight per lane
+      // PD_BB64_ROWS rows per iteration: as many independent neighbour gathers in flight per
+      // lane; the bonds are still added row by row
+      constexpr int RU = PD_BB64_ROWS;
       const int self = valid ? (int)i : 0;
-      for (int r = 0; r < rows; r += 2) {
-        const bool two = r + 1 < rows;
+      for (int r = 0; r < rows; r += RU) {
         const long long wi = (sbase >> 5) + r;
-        const unsigned w0 = d.bits[wi], w1 = two ? d.bits[wi + 1] : 0u;
-        const int k0 = r * G + gl, k1 = k0 + G;
-        const bool h0 = k0 < cnt, h1 = two && k1 < cnt;
-        const long long b0 = sbase + (long long)r * 32 + lane, b1 = b0 + 32;
-        const int j0 = h0 ? __ldg(d.nbr + b0) : self, j1 = h1 ? __ldg(d.nbr + b1) : self;
-        const double Ls0 = h0 ? __ldg(d.len64 + b0) : 1.0, Ls1 = h1 ? __ldg(d.len64 + b1) : 1.0;
-        const double4 x0 = ld4(d.cur + j0), x1 = ld4(d.cur + j1);
-        bool act0 = false, act1 = false;
+        unsigned w[RU];
+        int j[RU];
+        double Lsv[RU];
+        bool hv[RU], act[RU];
+        double4 xv[RU];
 #pragma unroll
-        for (int u = 0; u < 2; u++) {
-          const bool h = u ? h1 : h0;
-          if (!h) continue;
-          const double4 xj = u ? x1 : x0;
-          const double Ls = u ? Ls1 : Ls0;
+        for (int u = 0; u < RU; u++) {
+          const bool in = r + u < rows;
+          w[u] = in ? d.bits[wi + u] : 0u;
+          hv[u] = in && (r + u) * G + gl < cnt;
+          const long long b = sbase + (long long)(r + u) * 32 + lane;
+          j[u] = hv[u] ? __ldg(d.nbr + b) : self;
+          Lsv[u] = hv[u] ? __ldg(d.len64 + b) : 1.0;
+        }
+#pragma unroll
+        for (int u = 0; u < RU; u++) xv[u] = ld4(d.cur + j[u]);
+#pragma unroll
+        for (int u = 0; u < RU; u++) {
+          act[u] = false;
+          if (!hv[u]) continue;
+          const double4 xj = xv[u];
+          const double Ls = Lsv[u];
           const double L = fabs(Ls);
           const double dx = xj.x - xi.x, dy = xj.y - xi.y, dz = xj.z - xi.z;
           const double l = sqrt((dx * dx + dy * dy) + dz * dz);
           // the failure test keeps the reference's eps = (l - L) / L (bonds that may fail only)
           const bool brk = Ls > 0 && (l - L) / L > P.epsc;
-          const bool act = (((u ? w1 : w0) >> lane) & 1u) && !brk;
+          act[u] = ((w[u] >> lane) & 1u) && !brk;
           const double q = (l - L) / (L * l);  // eps / l
           const double bcb =
-              MULTI ? 0.5 * (P.bc + d.params[d.meta[u ? j1 : j0] & META_PID_MASK].bc) : P.bc;
-          const double bet = ESC ? __ldg(d.sc64 + (u ? b1 : b0)) : 1.0;
-          const double sc = act ? bet * bcb * q * xj.w : 0.0;
+              MULTI ? 0.5 * (P.bc + d.params[d.meta[j[u]] & META_PID_MASK].bc) : P.bc;
+          const double bet = ESC ? __ldg(d.sc64 + sbase + (long long)(r + u) * 32 + lane) : 1.0;
+          const double sc = act[u] ? bet * bcb * q * xj.w : 0.0;
           bx += sc * dx;
           by += sc * dy;
           bz += sc * dz;
-          if (u) act1 = act; else act0 = act;
         }
-        na += act0 + act1;
-        commit_row64(d.bits, wi, w0, act0, lane);
-        if (two) commit_row64(d.bits, wi + 1, w1, act1, lane);
+#pragma unroll
+        for (int u = 0; u < RU; u++) {
+          na += act[u];
+          if (r + u < rows) commit_row64(d.bits, wi + u, w[u], act[u], lane);
+        }
       }
     } else
     for (int r = 0; r < rows; r++) {

@@ -34,13 +34,17 @@ def jittered_cube(n, seed=1):
     return pos, vol, dx
 
 
-def test_bond_search_matches_oracle():
+# horizons (in dx) whose longest bond list on the jittered 12^3 cube takes each branch of the
+# bond-list sort: 1.5 (18 bonds: lists of up to 32), 2.2 (44: 64), 3.015 (118: 128), 3.6
+# (193: 256), 4.2 (313: 512), 6.0 (911: 1024) and 7.5 (1461: the library's segmented sort)
+@pytest.mark.parametrize("h", [1.5, 2.2, 3.015, 3.6, 4.2, 6.0, 7.5])
+def test_bond_search_matches_oracle(h):
     pos, vol, dx = jittered_cube(12)
     X = np.ascontiguousarray(pos.T)
-    delta = np.full(len(vol), 3.015 * dx)
+    delta = np.full(len(vol), h * dx)
     off, nbr, L, fp = O.find_bonds(X, delta)
     body = pd.Body(pd.OSBMaterial(), pos, vol)
-    pd.material(body, horizon=3.015 * dx, rho=1, E=1, nu=0.25, Gc=1)
+    pd.material(body, horizon=h * dx, rho=1, E=1, nu=0.25, Gc=1)
     ob = oracle_body(body)
     dev = pd.DeviceBody(body)
     assert dev.n_bonds == len(nbr)

@@ -218,11 +218,12 @@ void launch_count_active(const DevBody& d, cudaStream_t s) {
 }
 
 // reverse bonds on the CSR lists: position k' of i in the list of j (binary search in the
-// common sorted case, linear search otherwise); flags[0] = 1 if a bond has no reverse
+// common sorted case, linear search otherwise); flags[0] = 1 if a bond has no reverse. One warp
+// per point, its lanes taking consecutive bonds (coalesced reads of nbr, writes of revk).
 __global__ void k_reverse(long long n, const long long* off, const int* nbr, int* revk, int* flags) {
-  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long i = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   if (i >= n) return;
-  for (long long b = off[i]; b < off[i + 1]; b++) {
+  for (long long b = off[i] + (threadIdx.x & 31); b < off[i + 1]; b += 32) {
     const int j = nbr[b];
     const long long lo = off[j], hi = off[j + 1];
     long long found = -1, a = lo, z = hi;
@@ -240,7 +241,7 @@ __global__ void k_reverse(long long n, const long long* off, const int* nbr, int
 }
 
 void launch_reverse(long long n, const long long* off, const int* nbr, int* revk, int* flags, cudaStream_t s) {
-  k_reverse<<<blocks_for(n, 256), 256, 0, s>>>(n, off, nbr, revk, flags);
+  k_reverse<<<blocks_for(n * 32, 256), 256, 0, s>>>(n, off, nbr, revk, flags);
 }
 
 // flags[1] = 1 if a bond and its reverse differ in state; flags[2] = 1 if a fail-permitted

@@ -850,11 +850,8 @@ static void launch_dense(const DenseArgs& a, cudaStream_t s) {
   constexpr int tcols = NOUT < 32 ? 32 : NOUT;
   constexpr int by_smem = (227 * 1024) / smem, by_tmem = 512 / tcols;
   constexpr int per_sm = by_smem < by_tmem ? (by_smem < 8 ? by_smem : 8) : (by_tmem < 8 ? by_tmem : 8);
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(k_dense<KIN, NOUT, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    attr = true;
-  }
+  // the attribute belongs to the current device's context: set on every launch (cheap)
+  cudaFuncSetAttribute(k_dense<KIN, NOUT, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
   long long tiles = (a.n + 127) / 128;
   if (tiles > 148LL * per_sm) tiles = 148LL * per_sm;
   k_dense<KIN, NOUT, MODE><<<(int)(tiles < 1 ? 1 : tiles), 128, smem, s>>>(a);
@@ -871,11 +868,8 @@ template <int MO, int KIN, bool BIAS>
 static void launch_wgrad(long long n, const bf16* dz, const bf16* in0, int ld0, const bf16* in1,
                          float* part, float* bpart, int* err, cudaStream_t s) {
   constexpr int smem = wgrad_smem<MO, KIN, BIAS>();
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(k_wgrad<MO, KIN, BIAS>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    attr = true;
-  }
+  // the attribute belongs to the current device's context: set on every launch (cheap)
+  cudaFuncSetAttribute(k_wgrad<MO, KIN, BIAS>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
   k_wgrad<MO, KIN, BIAS><<<WG_BLOCKS, 128, smem, s>>>(n, dz, in0, ld0, in1, part, bpart, err);
 }
 
